@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark of the Q2 log-conductivity assembly + Hessian-action path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 64]
+
+Workload (one step): the linearization point of the 64^3 Q2 configuration in FP64 --
+pointwise data of (u, m, p) and one fused assembly of the full block set (A = K, its
+adjoint A^T = A, C = dr/dm, W_um, W_mm) with the assembled vectors (residual, dR/dm,
+dR/du) into the diagonal-first CSR pattern, eliminated on the boundary.  ``value`` is
+Q2 elements assembled per second (whole job), device-timed with inputs resident.
+After the timed steps, Hessian actions (misfit 4096 pointwise observations, two
+matrix-free Jacobi-PCG solves at rtol 1e-12 each) are timed for H-applies/s and their
+p50/p99 latency.  ``e2e`` repeats the step through the public API with the fields copied
+from pinned host memory and the gradient dR/dm copied back, inside the timed region.
+
+Under torchrun (N > 1) every rank runs an independent replica of the workload (the
+path does not shard: one GPU per request stream); value = all ranks' elements / the
+slowest rank's time.  ``--impl reference`` times the reference's algorithm on the host
+cores instead (element blocks by forward-over-reverse AD in 2048-element windows and a
+bincount scatter, restated in oracle/; rank 0 only).
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Q2 elems/s, H-applies/s at 64^3 vs plain FP64; p50/p99 batched-solve latency"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--happly", type=int, default=5, help="timed Hessian actions")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, smax, power, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [c.strip() for c in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU baselines
+def cpu_port_baseline(budget_s=12.0):
+    """The oracle's closed-form assembly of every block (oracle/q2.py) on a 16^3 sample
+    of the per-element work, bincount scatter and elimination included."""
+    from oracle import q2
+
+    try:
+        from threadpoolctl import threadpool_info
+        cores = max([i.get("num_threads", 1) for i in threadpool_info()] + [1])
+    except Exception:                                     # noqa: BLE001
+        cores = os.cpu_count() or 1
+    mesh = q2.Lattice(16)
+    E = mesh.edofs()
+    rng = np.random.default_rng(0)
+    u, m, p = (rng.standard_normal(mesh.ndof) for _ in range(3))
+    ess = np.zeros(mesh.ndof, bool)
+    ess[mesh.boundary_dofs()] = True
+    pat = q2.build_tables(E, E, mesh.ndof, mesh.ndof, True)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s or done == 0:
+        blk = q2.element_blocks(mesh, E, u, 0.1 * m, p)
+        for k in blk:
+            q2.assemble_block(k, pat, blk[k], ess)
+        q2.element_vectors(mesh, E, u, 0.1 * m, p)
+        done += mesh.ne
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "elements/s", "cores": int(cores), "kind": "port",
+            "sample": "oracle closed-form assembly of A, C, Wum, Wmm + vectors on 16^3 "
+                      "(4096 elements) repeated for %.1f s" % dt}
+
+
+def reference_step_fn(n_sample=16):
+    """One step of the reference's host algorithm on a 16^3 sample: blocks by AD in
+    2048-element windows (oracle/ad.py) + bincount scatter + folded elimination."""
+    from oracle import ad, q2
+
+    mesh = q2.Lattice(n_sample)
+    E = mesh.edofs()
+    rng = np.random.default_rng(0)
+    u, m, p = (rng.standard_normal(mesh.ndof) for _ in range(3))
+    ess = np.zeros(mesh.ndof, bool)
+    ess[mesh.boundary_dofs()] = True
+    pat = q2.build_tables(E, E, mesh.ndof, mesh.ndof, True)
+
+    def step():
+        blk = ad.element_blocks(mesh, E, u, 0.1 * m, p)
+        for k in blk:
+            q2.assemble_block(k, pat, blk[k], ess)
+        ad.element_vectors(mesh, E, u, 0.1 * m, p)
+        return mesh.ne
+    return step
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    step = reference_step_fn()
+    for _ in range(a.warmup):
+        step()
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(a.steps):
+        done += step()
+    dt = time.perf_counter() - t0
+    v = done / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "elements/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1000.0 * dt / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "Q2 hex linearization-point assembly (A, C, Wum, Wmm + "
+                                   "vectors), reference algorithm on the host",
+                       "mesh": "16^3 sample of the 64^3 per-element work", "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": "elements/s", "cores": torch.get_num_threads(),
+                             "kind": "port",
+                             "sample": "16^3 (4096 elements) per step: torch.func "
+                                       "forward-over-reverse AD in 2048-element windows "
+                                       "+ bincount scatter + elimination"},
+            "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------- ours
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import hippymfem_b200 as hm
+    from hippymfem_b200 import _lib
+    from hippymfem_b200._lib import check, lib, ptr, stream_ptr
+    from hippymfem_b200.synthetic import interior_points, log_conductivity, normal_vector
+
+    dev = torch.device("cuda", local)
+    n = a.n
+    mesh = hm.BoxMesh(n, device=dev)
+    V = hm.Q2Space(mesh)
+    bc = hm.DirichletBC(V)
+    pat = hm.LatticePattern(mesh)
+    ne, nd, nnz = mesh.ne, mesh.ndof, mesh.nnz
+    coords = mesh.node_coords()
+    m_h = log_conductivity(coords, seed=0)
+    rng = np.random.default_rng(11)
+    u_h, p_h = rng.standard_normal(nd), rng.standard_normal(nd)
+    u, m, p = (torch.as_tensor(x, device=dev) for x in (u_h, m_h, p_h))
+    quad = torch.empty(mesh.quad_bytes() // 8, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    vals = [torch.empty(nnz, dtype=torch.float64, device=dev) for _ in range(4)]
+    vecs = [torch.empty(nd, dtype=torch.float64, device=dev) for _ in range(3)]
+    marker = bc.marker
+    stream = torch.cuda.current_stream()
+    sp = stream_ptr(stream)
+    ev_k0 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ev_k1 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+
+    def step(i=None):
+        check(lib.hm_lattice_quadrature(mesh.handle, ptr(u), ptr(m), ptr(p), _lib.HM_FP64,
+                                        ptr(quad), ptr(status), sp))
+        if i is not None:
+            ev_k0[i].record(stream)
+        check(lib.hm_lattice_assemble(mesh.handle, ptr(quad), _lib.HM_FP64, ptr(pat.indptr),
+                                      ptr(marker), 1.0, *(ptr(v) for v in vals),
+                                      *(ptr(v) for v in vecs), 0, sp))
+        if i is not None:
+            ev_k1[i].record(stream)
+
+    launches_per_step = 2
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for i in range(a.steps):
+        step(i)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    k_ms = statistics.mean(ev_k0[i].elapsed_time(ev_k1[i]) for i in range(a.steps))
+    if world > 1:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    assert int(status.item()) == 0, "non-finite values in the benchmark fields"
+    value = world * ne * a.steps / (ms / 1000.0)
+
+    # roofline of the fused assembly kernel: bytes it must move per launch
+    alg_bytes = 8 * nnz * 4 + 8 * nd * 3 + 8 * 216 * ne + 4 * (nd + 1) + nd
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (k_ms / 1000.0) / 1e9
+    step_bytes = 8 * nnz * 4 + 8 * nd * 5            # survey's B_asm without the slot map
+
+    # ------------------------------------------------------------ e2e (public API)
+    pin = [torch.empty(nd, dtype=torch.float64).pin_memory() for _ in range(3)]
+    for h, src in zip(pin, (u_h, m_h, p_h)):
+        h.copy_(torch.as_tensor(src))
+    gpin = torch.empty(nd, dtype=torch.float64).pin_memory()
+    prob = hm.PDEVariationalProblem([V, V, V], f=1.0, bc=bc, check_finite=False)
+    prob._pattern = pat
+    du, dm, dp = (torch.empty(nd, dtype=torch.float64, device=dev) for _ in range(3))
+    g = torch.empty(nd, dtype=torch.float64, device=dev)
+
+    def e2e_step():
+        du.copy_(pin[0], non_blocking=True)
+        dm.copy_(pin[1], non_blocking=True)
+        dp.copy_(pin[2], non_blocking=True)
+        prob._jac_cache = None                     # a new point: the Jacobian too
+        prob.setLinearizationPoint([du, dm, dp])
+        prob.evalGradientParameter([du, dm, dp], g)
+        gpin.copy_(g, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(3, a.steps // 2)
+    e0.record(stream)
+    for _ in range(e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e_ms = float(tt.item())
+    e2e_value = world * ne * e_steps / (e_ms / 1000.0)
+    del prob
+    torch.cuda.empty_cache()
+
+    # ------------------------------------------------------ Hessian actions
+    prob = hm.PDEVariationalProblem([V, V, V], f=1.0, bc=bc, matrix_free_solves=True,
+                                    check_finite=False, solver_tolerance=1e-12)
+    prob._pattern = pat
+    pts = interior_points(4096, seed=2)
+    misfit = hm.PointwiseStateObservation(V, pts, data=np.zeros(4096), noise_variance=1.0)
+    model = hm.Model(prob, None, misfit)
+    mt = torch.as_tensor(log_conductivity(coords, seed=1), device=dev)
+    ut = V.vector()
+    model.solveFwd(ut, [ut, mt, None])
+    Bu = misfit.Bh @ ut.cpu().numpy()
+    noise = 0.01 * float(ut.abs().max())
+    misfit.d.copy_(torch.as_tensor(Bu + noise * np.random.default_rng(5).standard_normal(4096)))
+    misfit.noise_variance = noise ** 2
+    uu, pp = V.vector(), V.vector()
+    x = [uu, m, pp]
+    model.solveFwd(uu, x)
+    model.solveAdj(pp, x)
+    model.setPointForHessianEvaluations(x)
+    H = hm.ReducedHessian(model)
+    v = torch.as_tensor(normal_vector(nd, seed=4), device=dev)
+    y = V.vector()
+    H.mult(v, y)
+    torch.cuda.synchronize()
+    lat = []
+    H.iterations.clear()
+    for _ in range(a.happly):
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        H.mult(v, y)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        lat.append(h0.elapsed_time(h1))
+    iters = list(H.iterations)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_port_baseline()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "Q2 hex %d^3 linearization-point assembly: A(=K=A^T), C, "
+                                   "Wum, Wmm + residual, dR/dm, dR/du, FP64, boundary "
+                                   "eliminated" % n,
+                       "elements": ne, "dofs": nd, "nnz_per_block": nnz,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs and outputs larger than L2 (4.3 GB written per step)"},
+            "dofs_per_s": world * nd * a.steps / (ms / 1000.0),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "kernel": "k_tile_assemble<double>", "kernel_ms": k_ms,
+                         "alg_bytes_per_launch": alg_bytes,
+                         "step_alg_bytes": step_bytes,
+                         "step_frac": step_bytes / (ms / a.steps / 1000.0) / 1e9 / peak},
+            "h_applies_per_s": world * 1000.0 / statistics.mean(lat),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "what": "one Hessian action (2 matrix-free Jacobi-PCG solves, "
+                                   "rtol 1e-12)"},
+            "pcg_iterations": iters,
+            "e2e": {"value": e2e_value, "unit": "elements/s",
+                    "h2d_bytes_per_step": 3 * 8 * nd, "d2h_bytes_per_step": 8 * nd,
+                    "steps": e_steps},
+            "clocks": ck,
+            "gpu_launches": launches_per_step * a.steps,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,24 @@
+// Launchers shared between the translation units of libhippymfem_b200.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/hippymfem_b200.h"
+
+namespace hm {
+struct Lattice;
+}
+
+int hm_launch_pattern(const hm::Lattice& L, int32_t* indptr, int32_t* indices, int32_t* slot,
+                      void* stream);
+int hm_launch_tpos(const hm::Lattice& L, const int32_t* indptr, int32_t* tpos, void* stream);
+int hm_launch_quad(const hm::Lattice& L, const double* u, const double* m, const double* p,
+                   int precision, void* quad, uint32_t* status, void* stream);
+int hm_launch_assemble(const hm::Lattice& L, const void* quad, int precision,
+                       const int32_t* indptr, const uint8_t* ess, double f, double* vA,
+                       double* vC, double* vWum, double* vWmm, double* vs, double* vp,
+                       double* va, int zero_ess, void* stream);
+int hm_launch_apply_A(const hm::Lattice& L, const void* quad, int precision,
+                      const uint8_t* ess, const double* x, double* y, void* stream);
+int hm_launch_diag_A(const hm::Lattice& L, const void* quad, int precision,
+                     const uint8_t* ess, double* diag, void* stream);

@@ -1,0 +1,878 @@
+// Structured-lattice kernels of the Q2 log-conductivity path (sm_100a).
+//
+//   k_pattern_*     the CSR graph (diagonal first), the entry->slot map and the
+//                   transpose map of a Q2 x Q2 block, arithmetically
+//   k_quad          pointwise data D, E = D grad u, F = D grad p, W = D grad u.grad p
+//   k_tile_assemble the fused assembly: every CSR value of A, C, Wum, Wmm and the
+//                   three assembled vectors, each written exactly once
+//   k_tile_apply_A  the matrix-free Jacobian apply
+//
+// The assembly is output-stationary.  On a uniform lattice every block is a sum of
+// separable terms over the global quadrature lattice, e.g.
+//     A(n, j) = sum_g D(g) sum_d  T_d,x(g_x; n_x, j_x) T_d,y(...) T_d,z(...)
+// with 1D pair tables T (B B, B' B', B' B) that vanish unless the row and column
+// nodes share an element.  A CTA owns a 4 x 4 x 4 tile of node rows, stages the
+// pointwise data of the 3 x 3 x 3 elements around it in shared memory, contracts the
+// three axes one after the other (sum factorisation over the tile's 16 ordered 1D
+// pairs per axis) and streams the finished rows out in CSR order.  No atomics, no
+// colouring, no slot map: every value is summed in registers in a fixed order and
+// stored once, so the assembly is bit-reproducible by construction.
+#include <cstdio>
+
+#include "hm_common.cuh"
+#include "hm_internal.h"
+
+namespace hm {
+
+// =============================================================== pattern kernels
+__device__ __forceinline__ void node_of(int64_t n, const Lattice& L, int& i, int& j, int& k) {
+  i = (int)(n % L.Nx);
+  const int64_t t = n / L.Nx;
+  j = (int)(t % L.Ny);
+  k = (int)(t / L.Ny);
+}
+
+__device__ __forceinline__ int64_t row_start(const Lattice& L, int i, int j, int k) {
+  const int64_t T1 = stencil_prefix(L.Nx, L.Nx), T2 = stencil_prefix(L.Ny, L.Ny);
+  return stencil_prefix(k, L.Nz) * T1 * T2 +
+         (int64_t)stencil_n(k, L.Nz) *
+             (stencil_prefix(j, L.Ny) * T1 + (int64_t)stencil_n(j, L.Ny) * stencil_prefix(i, L.Nx));
+}
+
+// CSR position of column (ci, cj, ck) within row (i, j, k): diagonal first, the rest
+// ascending (ascending lexicographic node number = z, then y, then x rank)
+__device__ __forceinline__ int pos_in_row(const Lattice& L, int i, int j, int k, int ci,
+                                          int cj, int ck) {
+  const int n1 = stencil_n(i, L.Nx), n2 = stencil_n(j, L.Ny);
+  const int rank = ((ck - stencil_lo(k)) * n2 + (cj - stencil_lo(j))) * n1 + (ci - stencil_lo(i));
+  const int kd = ((k - stencil_lo(k)) * n2 + (j - stencil_lo(j))) * n1 + (i - stencil_lo(i));
+  return rank == kd ? 0 : (rank < kd ? rank + 1 : rank);
+}
+
+__global__ void k_pattern_indptr(Lattice L, int32_t* __restrict__ indptr) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n > L.ndof) return;
+  if (n == L.ndof) {
+    indptr[n] = (int32_t)(stencil_prefix(L.Nx, L.Nx) * stencil_prefix(L.Ny, L.Ny) *
+                          stencil_prefix(L.Nz, L.Nz));
+    return;
+  }
+  int i, j, k;
+  node_of(n, L, i, j, k);
+  indptr[n] = (int32_t)row_start(L, i, j, k);
+}
+
+// one warp per row: the row's columns in CSR order
+__global__ void k_pattern_indices(Lattice L, const int32_t* __restrict__ indptr,
+                                  int32_t* __restrict__ indices) {
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= L.ndof) return;
+  int i, j, k;
+  node_of(row, L, i, j, k);
+  const int n1 = stencil_n(i, L.Nx), n2 = stencil_n(j, L.Ny), n3 = stencil_n(k, L.Nz);
+  const int lo1 = stencil_lo(i), lo2 = stencil_lo(j), lo3 = stencil_lo(k);
+  const int kd = ((k - lo3) * n2 + (j - lo2)) * n1 + (i - lo1);
+  const int len = n1 * n2 * n3;
+  const int64_t base = indptr[row];
+  for (int pos = lane; pos < len; pos += 32) {
+    const int rank = pos == 0 ? kd : (pos <= kd ? pos - 1 : pos);
+    const int k1 = rank % n1, t = rank / n1, k2 = t % n2, k3 = t / n2;
+    indices[base + pos] = (int32_t)((lo1 + k1) + (int64_t)L.Nx * ((lo2 + k2) + (int64_t)L.Ny * (lo3 + k3)));
+  }
+}
+
+// entry k = (e*27 + a)*27 + b -> CSR position (patternbuild.build_tables' slot)
+__global__ void k_pattern_slot(Lattice L, int32_t* __restrict__ slot) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= L.ne * 729) return;
+  const int b = (int)(k % 27);
+  const int a = (int)((k / 27) % 27);
+  const int64_t e = k / 729;
+  const int ex = (int)(e % L.nx), ey = (int)((e / L.nx) % L.ny), ez = (int)(e / ((int64_t)L.nx * L.ny));
+  const int i = 2 * ex + a % 3, j = 2 * ey + (a / 3) % 3, kk = 2 * ez + a / 9;
+  const int ci = 2 * ex + b % 3, cj = 2 * ey + (b / 3) % 3, ck = 2 * ez + b / 9;
+  slot[k] = (int32_t)(row_start(L, i, j, kk) + pos_in_row(L, i, j, kk, ci, cj, ck));
+}
+
+// tpos[s] = CSR position of (col, row) for entry s = (row, col)
+__global__ void k_pattern_tpos(Lattice L, const int32_t* __restrict__ indptr,
+                               int32_t* __restrict__ tpos) {
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= L.ndof) return;
+  int i, j, k;
+  node_of(row, L, i, j, k);
+  const int n1 = stencil_n(i, L.Nx), n2 = stencil_n(j, L.Ny), n3 = stencil_n(k, L.Nz);
+  const int lo1 = stencil_lo(i), lo2 = stencil_lo(j), lo3 = stencil_lo(k);
+  const int kd = ((k - lo3) * n2 + (j - lo2)) * n1 + (i - lo1);
+  const int len = n1 * n2 * n3;
+  const int64_t base = indptr[row];
+  for (int pos = lane; pos < len; pos += 32) {
+    const int rank = pos == 0 ? kd : (pos <= kd ? pos - 1 : pos);
+    const int k1 = rank % n1, t = rank / n1, k2 = t % n2, k3 = t / n2;
+    const int ci = lo1 + k1, cj = lo2 + k2, ck = lo3 + k3;
+    tpos[base + pos] = (int32_t)(row_start(L, ci, cj, ck) + pos_in_row(L, ci, cj, ck, i, j, k));
+  }
+}
+
+// ============================================================ quadrature data
+// One thread per (element, Gauss point), 8 elements per 216-thread block.  Layout:
+// quad[e][c][q], c = 0 D, 1-3 E, 4-6 F, 7 W (each element's 216 values contiguous).
+template <typename real>
+__global__ void __launch_bounds__(216) k_quad(Lattice L, const double* __restrict__ u,
+                                              const double* __restrict__ m,
+                                              const double* __restrict__ p,
+                                              real* __restrict__ quad,
+                                              uint32_t* __restrict__ status) {
+  __shared__ real sv[8][3][27];
+  const int le = threadIdx.x / 27, q = threadIdx.x % 27;
+  const int64_t e = blockIdx.x * 8LL + le;
+  const bool live = e < L.ne;
+  if (live) {
+    const int ex = (int)(e % L.nx), ey = (int)((e / L.nx) % L.ny), ez = (int)(e / ((int64_t)L.nx * L.ny));
+    const int a = q;
+    const int64_t node = (2 * ex + a % 3) + (int64_t)L.Nx * ((2 * ey + (a / 3) % 3) + (int64_t)L.Ny * (2 * ez + a / 9));
+    sv[le][0][a] = (real)u[node];
+    sv[le][1][a] = (real)m[node];
+    sv[le][2][a] = (real)p[node];
+  }
+  __syncthreads();
+  if (!live) return;
+  const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
+  real b1[3], b2[3], b3[3], d1[3], d2[3], d3[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    b1[a] = (real)bq(q1, a); b2[a] = (real)bq(q2, a); b3[a] = (real)bq(q3, a);
+    d1[a] = (real)dbq(q1, a); d2[a] = (real)dbq(q2, a); d3[a] = (real)dbq(q3, a);
+  }
+  real val[3], gx[3], gy[3], gz[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const real* x = sv[le][f];
+    real vb = 0, vx = 0, vy = 0, vz = 0;
+#pragma unroll
+    for (int a3 = 0; a3 < 3; ++a3) {
+      real sbb = 0, sdb = 0, sbd = 0;
+#pragma unroll
+      for (int a2 = 0; a2 < 3; ++a2) {
+        real xb = 0, xd = 0;
+#pragma unroll
+        for (int a1 = 0; a1 < 3; ++a1) {
+          xb = fma(b1[a1], x[a1 + 3 * a2 + 9 * a3], xb);
+          xd = fma(d1[a1], x[a1 + 3 * a2 + 9 * a3], xd);
+        }
+        sbb = fma(b2[a2], xb, sbb);
+        sdb = fma(b2[a2], xd, sdb);
+        sbd = fma(d2[a2], xb, sbd);
+      }
+      vb = fma(b3[a3], sbb, vb);
+      vx = fma(b3[a3], sdb, vx);
+      vy = fma(b3[a3], sbd, vy);
+      vz = fma(d3[a3], sbb, vz);
+    }
+    val[f] = vb;
+    gx[f] = vx / (real)L.hx;
+    gy[f] = vy / (real)L.hy;
+    gz[f] = vz / (real)L.hz;
+  }
+  const real wdet = (real)(wq(q1) * wq(q2) * wq(q3) * L.hx * L.hy * L.hz);
+  const real D = wdet * exp(val[1]);
+  const real E[3] = {D * gx[0], D * gy[0], D * gz[0]};
+  const real F[3] = {D * gx[2], D * gy[2], D * gz[2]};
+  const real W = D * (gx[0] * gx[2] + gy[0] * gy[2] + gz[0] * gz[2]);
+  real* out = quad + e * 216;
+  out[q] = D;
+  out[27 + q] = E[0]; out[54 + q] = E[1]; out[81 + q] = E[2];
+  out[108 + q] = F[0]; out[135 + q] = F[1]; out[162 + q] = F[2];
+  out[189 + q] = W;
+  const bool finite = isfinite(D) && isfinite(E[0]) && isfinite(E[1]) && isfinite(E[2]) &&
+                      isfinite(F[0]) && isfinite(F[1]) && isfinite(F[2]) && isfinite(W);
+  if (!finite) atomicOr(status, HM_STATUS_NONFINITE);
+}
+
+// ================================================================ tile assembly
+template <typename real>
+struct TileSmem {
+  real W[8][9][9][9];      // pointwise data on the tile's 9^3 local Gauss lattice
+  real T1[16][9][9];       // after the z contraction: [p3][g2][g1]
+  real T2[16][16][9];      // after the y contraction: [p3][p2][g1]
+  real V[16][16][17];      // finished values [p3][p2][p1] (padded: conflict-free)
+  uint8_t ess[7][7][7];    // Dirichlet markers of the halo'd nodes [s3][s2][s1]
+  int32_t rowptr[4][4][4]; // CSR offsets of the owned rows [r3][r2][r1]
+};
+
+struct TileCtx {
+  int t1, t2, t3;      // tile coordinates
+  int vl[3];           // bit l set: halo'd element l is inside the mesh, per axis
+};
+
+// stage 1: contract the z axis of weight c with table TZ -> T1[p3][g2][g1]
+template <int TZ, typename real>
+__device__ __forceinline__ void stage1(const real* __restrict__ Wc, real* __restrict__ T1) {
+  for (int task = threadIdx.x; task < 81; task += blockDim.x) {
+    const int g1 = task % 9, g2 = task / 9;
+    real w[9];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) w[l] = Wc[(l * 9 + g2) * 9 + g1];
+#pragma unroll
+    for (int p = 0; p < 16; ++p) {
+      real acc = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t < pair_cnt(p)) acc = fma((real)pair_coef(TZ, p, t), w[pair_g0(p) + t], acc);
+      T1[(p * 9 + g2) * 9 + g1] = acc;
+    }
+  }
+}
+
+// stage 2: contract the y axis with table TY -> T2[p3][p2][g1] (= or +=) scale * ...
+template <int TY, bool ACC, typename real>
+__device__ __forceinline__ void stage2(const real* __restrict__ T1, real* __restrict__ T2,
+                                       real scale) {
+  for (int task = threadIdx.x; task < 144; task += blockDim.x) {
+    const int g1 = task % 9, p3 = task / 9;
+    real w[9];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) w[l] = T1[(p3 * 9 + l) * 9 + g1];
+#pragma unroll
+    for (int p = 0; p < 16; ++p) {
+      real acc = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t < pair_cnt(p)) acc = fma((real)pair_coef(TY, p, t), w[pair_g0(p) + t], acc);
+      const int idx = (p3 * 16 + p) * 9 + g1;
+      T2[idx] = ACC ? fma(scale, acc, T2[idx]) : scale * acc;
+    }
+  }
+}
+
+// stage 3: contract the x axis with table TX -> V[p3][p2][p1] (= or +=)
+template <int TX, bool ACC, typename real>
+__device__ __forceinline__ void stage3(const real* __restrict__ T2, real* __restrict__ V) {
+  for (int task = threadIdx.x; task < 256; task += blockDim.x) {
+    const int p2 = task % 16, p3 = task / 16;
+    real w[9];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) w[l] = T2[(p3 * 16 + p2) * 9 + l];
+    real* out = V + (p3 * 16 + p2) * 17;
+#pragma unroll
+    for (int p = 0; p < 16; ++p) {
+      real acc = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t < pair_cnt(p)) acc = fma((real)pair_coef(TX, p, t), w[pair_g0(p) + t], acc);
+      out[p] = ACC ? out[p] + acc : acc;
+    }
+  }
+}
+
+enum BlockKind { BK_A = 0, BK_C = 1, BK_WUM = 2, BK_WMM = 3 };
+
+// The separable terms of each block; terms that share the x table form one stage-3
+// group, and each group's y/z partial sums are added before the x contraction:
+//   A   = K.M.M/hx^2 (D)  +  M.[K.M/hy^2 + M.K/hz^2] (D)
+//   C   = R.M.M/hx (Ex)   +  M.[R.M/hy (Ey) + M.R/hz (Ez)]
+//   Wum = C with F in place of E
+//   Wmm = M.M.M (W)
+// (tables as x.y.z; the weights carry w|J| and the physical gradients)
+template <int BLK, typename real>
+__device__ __forceinline__ void tile_block(TileSmem<real>& S, const Lattice& L) {
+  real* T1 = &S.T1[0][0][0];
+  real* T2 = &S.T2[0][0][0];
+  real* V = &S.V[0][0][0];
+  if (BLK == BK_A) {
+    const real* D = &S.W[0][0][0][0];
+    stage1<TM>(D, T1); __syncthreads();
+    stage2<TM, false>(T1, T2, (real)(1.0 / (L.hx * L.hx))); __syncthreads();
+    stage3<TK, false>(T2, V); __syncthreads();
+    stage2<TK, false>(T1, T2, (real)(1.0 / (L.hy * L.hy))); __syncthreads();
+    stage1<TK>(D, T1); __syncthreads();
+    stage2<TM, true>(T1, T2, (real)(1.0 / (L.hz * L.hz))); __syncthreads();
+    stage3<TM, true>(T2, V); __syncthreads();
+  } else if (BLK == BK_C || BLK == BK_WUM) {
+    const int c0 = BLK == BK_C ? 1 : 4;
+    const real* Gx = &S.W[c0][0][0][0];
+    const real* Gy = &S.W[c0 + 1][0][0][0];
+    const real* Gz = &S.W[c0 + 2][0][0][0];
+    stage1<TM>(Gx, T1); __syncthreads();
+    stage2<TM, false>(T1, T2, (real)(1.0 / L.hx)); __syncthreads();
+    stage3<TR, false>(T2, V); __syncthreads();
+    stage1<TM>(Gy, T1); __syncthreads();
+    stage2<TR, false>(T1, T2, (real)(1.0 / L.hy)); __syncthreads();
+    stage1<TR>(Gz, T1); __syncthreads();
+    stage2<TM, true>(T1, T2, (real)(1.0 / L.hz)); __syncthreads();
+    stage3<TM, true>(T2, V); __syncthreads();
+  } else {
+    const real* Wq = &S.W[7][0][0][0];
+    stage1<TM>(Wq, T1); __syncthreads();
+    stage2<TM, false>(T1, T2, (real)1.0); __syncthreads();
+    stage3<TM, false>(T2, V); __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int div35(int x, int n) { return n == 5 ? x / 5 : x / 3; }
+
+// Stream the tile's finished rows of one block out in CSR order, with the block's
+// folded elimination: A rows and columns of Dirichlet nodes zeroed and a unit
+// diagonal; C and Wum rows zeroed; Wmm untouched.  A warp covers one x-run of up to
+// four rows, which is contiguous in the CSR arrays, lanes on consecutive positions.
+template <int BLK, typename real>
+__device__ __forceinline__ void tile_write(const TileSmem<real>& S, const Lattice& L,
+                                           const TileCtx& c, double* __restrict__ vals) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarp = blockDim.x >> 5;
+  for (int run = warp; run < 16; run += nwarp) {
+    const int r2 = run & 3, r3 = run >> 2;
+    const int gy = 4 * c.t2 + r2, gz = 4 * c.t3 + r3;
+    if (gy >= L.Ny || gz >= L.Nz) continue;
+    const int n2 = stencil_n(gy, L.Ny), lo2 = stencil_lo(gy);
+    const int n3 = stencil_n(gz, L.Nz), lo3 = stencil_lo(gz);
+    int len[4], pre[5];
+    pre[0] = 0;
+#pragma unroll
+    for (int r1 = 0; r1 < 4; ++r1) {
+      const int gx = 4 * c.t1 + r1;
+      len[r1] = gx < L.Nx ? stencil_n(gx, L.Nx) * n2 * n3 : 0;
+      pre[r1 + 1] = pre[r1] + len[r1];
+    }
+    const int64_t base = S.rowptr[r3][r2][0];
+    const bool ress_yz = false;
+    (void)ress_yz;
+    for (int j = lane; j < pre[4]; j += 32) {
+      const int r1 = j < pre[1] ? 0 : j < pre[2] ? 1 : j < pre[3] ? 2 : 3;
+      const int pos = j - pre[r1];
+      const int gx = 4 * c.t1 + r1;
+      const int n1 = stencil_n(gx, L.Nx), lo1 = stencil_lo(gx);
+      const int kd = ((gz - lo3) * n2 + (gy - lo2)) * n1 + (gx - lo1);
+      const int rank = pos == 0 ? kd : (pos <= kd ? pos - 1 : pos);
+      const int t = div35(rank, n1);
+      const int k1 = rank - t * n1;
+      const int k3 = div35(t, n2);
+      const int k2 = t - k3 * n2;
+      // local column nodes (0..6) and the 1D pair of each axis
+      const int s1 = lo1 + k1 - (4 * c.t1 - 2), s2 = lo2 + k2 - (4 * c.t2 - 2), s3 = lo3 + k3 - (4 * c.t3 - 2);
+      const int p1 = row_pair_base(r1) + s1 - row_col_start(r1);
+      const int p2 = row_pair_base(r2) + s2 - row_col_start(r2);
+      const int p3 = row_pair_base(r3) + s3 - row_col_start(r3);
+      double v = (double)S.V[p3][p2][p1];
+      if (BLK != BK_WMM) {
+        const bool ress = S.ess[r3 + 2][r2 + 2][r1 + 2] != 0;
+        if (BLK == BK_A) {
+          const bool cess = S.ess[s3][s2][s1] != 0;
+          if (ress || cess) v = (pos == 0 && ress) ? 1.0 : 0.0;
+        } else if (ress) {
+          v = 0.0;
+        }
+      }
+      vals[base + j] = v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ assembled vectors
+// dR/dp = sum_g E.grad phi - f w|J| phi,  dR/du = sum_g F.grad phi,  dR/dm = sum_g W psi,
+// by the same sum factorisation with single-index tables of the owned rows.
+template <int TZ, typename real>
+__device__ __forceinline__ void vstage1(const real* __restrict__ Wc, real* __restrict__ U1,
+                                        int task, bool wdet, const Lattice& L, const TileCtx& c) {
+  const int g1 = task % 9, g2 = task / 9;
+  real w[9];
+#pragma unroll
+  for (int l = 0; l < 9; ++l) {
+    if (wdet) {
+      const bool in = ((c.vl[0] >> (g1 / 3)) & 1) && ((c.vl[1] >> (g2 / 3)) & 1) && ((c.vl[2] >> (l / 3)) & 1);
+      w[l] = in ? (real)(wq(g1 % 3) * wq(g2 % 3) * wq(l % 3) * L.hx * L.hy * L.hz) : (real)0;
+    } else {
+      w[l] = Wc[(l * 9 + g2) * 9 + g1];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    real acc = 0;
+#pragma unroll
+    for (int t = 0; t < 6; ++t)
+      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TZ, r, t), w[vrow_g0(r) + t], acc);
+    U1[(r * 9 + g2) * 9 + g1] = acc;
+  }
+}
+
+template <int TY, typename real>
+__device__ __forceinline__ void vstage2(const real* __restrict__ U1, real* __restrict__ U2, int task) {
+  const int g1 = task % 9, r3 = task / 9;
+  real w[9];
+#pragma unroll
+  for (int l = 0; l < 9; ++l) w[l] = U1[(r3 * 9 + l) * 9 + g1];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    real acc = 0;
+#pragma unroll
+    for (int t = 0; t < 6; ++t)
+      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TY, r, t), w[vrow_g0(r) + t], acc);
+    U2[(r3 * 4 + r) * 9 + g1] = acc;
+  }
+}
+
+template <int TX, typename real>
+__device__ __forceinline__ void vstage3(const real* __restrict__ U2, real (&y)[4], int r2, int r3, real scale) {
+  real w[9];
+#pragma unroll
+  for (int l = 0; l < 9; ++l) w[l] = U2[(r3 * 4 + r2) * 9 + l];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    real acc = 0;
+#pragma unroll
+    for (int t = 0; t < 6; ++t)
+      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TX, r, t), w[vrow_g0(r) + t], acc);
+    y[r] = fma(scale, acc, y[r]);
+  }
+}
+
+// the 8 vector terms: (weight, x/y/z tables); term 3 is the source (w|J|, scaled -f)
+struct VTerm { int w, tx, ty, tz; };
+__device__ __constant__ VTerm c_vterms[8] = {
+    {1, VD, VB, VB}, {2, VB, VD, VB}, {3, VB, VB, VD}, {-1, VB, VB, VB},   // dR/dp
+    {4, VD, VB, VB}, {5, VB, VD, VB}, {6, VB, VB, VD},                     // dR/du
+    {7, VB, VB, VB}};                                                       // dR/dm
+
+template <typename real>
+__device__ __forceinline__ void tile_vectors(TileSmem<real>& S, const Lattice& L, const TileCtx& c,
+                                             double f, double* __restrict__ vstate,
+                                             double* __restrict__ vparam,
+                                             double* __restrict__ vadj, bool zero_ess) {
+  real* U1 = &S.T1[0][0][0];  // 8 terms x [4][9][9]  (spans T1 and T2)
+  real* U2 = &S.V[0][0][0];   // 8 terms x [4][4][9]
+  const int tid = threadIdx.x;
+  for (int task = tid; task < 8 * 81; task += blockDim.x) {
+    const int term = task / 81, tt = task % 81;
+    const VTerm vt = c_vterms[term];
+    const real* Wc = vt.w >= 0 ? &S.W[vt.w][0][0][0] : nullptr;
+    real* out = U1 + term * 324;
+    if (vt.tz == VB) vstage1<VB>(Wc, out, tt, vt.w < 0, L, c);
+    else vstage1<VD>(Wc, out, tt, vt.w < 0, L, c);
+  }
+  __syncthreads();
+  for (int task = tid; task < 8 * 36; task += blockDim.x) {
+    const int term = task / 36, tt = task % 36;
+    const VTerm vt = c_vterms[term];
+    if (vt.ty == VB) vstage2<VB>(U1 + term * 324, U2 + term * 144, tt);
+    else vstage2<VD>(U1 + term * 324, U2 + term * 144, tt);
+  }
+  __syncthreads();
+  // 3 slots x 16 (r2, r3): each sums its terms over r1
+  if (tid < 48) {
+    const int slot = tid / 16, r2 = tid % 4, r3 = (tid / 4) % 4;
+    real y[4] = {0, 0, 0, 0};
+    const int t0 = slot == 0 ? 0 : slot == 1 ? 4 : 7;
+    const int t1 = slot == 0 ? 4 : slot == 1 ? 7 : 8;
+    const real sc[3] = {(real)(1.0 / L.hx), (real)(1.0 / L.hy), (real)(1.0 / L.hz)};
+    for (int term = t0; term < t1; ++term) {
+      const VTerm vt = c_vterms[term];
+      const real scale = term == 3 ? (real)(-f) : term == 7 ? (real)1 : sc[(term - t0) % 3];
+      if (vt.tx == VB) vstage3<VB>(U2 + term * 144, y, r2, r3, scale);
+      else vstage3<VD>(U2 + term * 144, y, r2, r3, scale);
+    }
+    double* dst = slot == 0 ? vadj : slot == 1 ? vstate : vparam;
+    const int gy = 4 * c.t2 + r2, gz = 4 * c.t3 + r3;
+    if (dst != nullptr && gy < L.Ny && gz < L.Nz) {
+#pragma unroll
+      for (int r1 = 0; r1 < 4; ++r1) {
+        const int gx = 4 * c.t1 + r1;
+        if (gx >= L.Nx) continue;
+        double v = (double)y[r1];
+        if (zero_ess && slot != 2 && S.ess[r3 + 2][r2 + 2][r1 + 2]) v = 0.0;
+        dst[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] = v;
+      }
+    }
+  }
+}
+
+template <typename real>
+__device__ __forceinline__ void tile_load(TileSmem<real>& S, const Lattice& L, TileCtx& c,
+                                          const real* __restrict__ quad,
+                                          const uint8_t* __restrict__ ess,
+                                          const int32_t* __restrict__ indptr, int ncomp) {
+  const int tid = threadIdx.x;
+  c.t1 = blockIdx.x; c.t2 = blockIdx.y; c.t3 = blockIdx.z;
+  const int eb[3] = {2 * c.t1 - 1, 2 * c.t2 - 1, 2 * c.t3 - 1};
+  const int ne[3] = {L.nx, L.ny, L.nz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    c.vl[d] = 0;
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+      if (eb[d] + l >= 0 && eb[d] + l < ne[d]) c.vl[d] |= 1 << l;
+  }
+  const int per = ncomp * 27;
+  for (int i = tid; i < 27 * per; i += blockDim.x) {
+    const int l = i / per, f = i - l * per;
+    const int comp = f / 27, q = f - comp * 27;
+    const int l1 = l % 3, l2 = (l / 3) % 3, l3 = l / 9;
+    const int ex = eb[0] + l1, ey = eb[1] + l2, ez = eb[2] + l3;
+    real v = 0;
+    if (((c.vl[0] >> l1) & 1) && ((c.vl[1] >> l2) & 1) && ((c.vl[2] >> l3) & 1)) {
+      const int64_t e = ex + (int64_t)L.nx * (ey + (int64_t)L.ny * ez);
+      v = quad[e * 216 + f];
+    }
+    const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
+    S.W[comp][3 * l3 + q3][3 * l2 + q2][3 * l1 + q1] = v;
+  }
+  for (int i = tid; i < 343; i += blockDim.x) {
+    const int s1 = i % 7, s2 = (i / 7) % 7, s3 = i / 49;
+    const int gx = 4 * c.t1 - 2 + s1, gy = 4 * c.t2 - 2 + s2, gz = 4 * c.t3 - 2 + s3;
+    uint8_t m = 0;
+    if (ess != nullptr && gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 && gz < L.Nz)
+      m = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
+    S.ess[s3][s2][s1] = m;
+  }
+  if (indptr != nullptr && tid < 64) {
+    const int r1 = tid % 4, r2 = (tid / 4) % 4, r3 = tid / 16;
+    const int gx = 4 * c.t1 + r1, gy = 4 * c.t2 + r2, gz = 4 * c.t3 + r3;
+    int32_t v = 0;
+    if (gx < L.Nx && gy < L.Ny && gz < L.Nz) v = indptr[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
+    S.rowptr[r3][r2][r1] = v;
+  }
+  __syncthreads();
+}
+
+struct AssembleOut {
+  double* vals[4];
+  double* vec_state;
+  double* vec_param;
+  double* vec_adj;
+  double f;
+  int zero_ess;
+};
+
+template <typename real>
+__global__ void __launch_bounds__(256, 2)
+    k_tile_assemble(Lattice L, const real* __restrict__ quad, const uint8_t* __restrict__ ess,
+                    const int32_t* __restrict__ indptr, AssembleOut o) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileSmem<real>& S = *reinterpret_cast<TileSmem<real>*>(smem_raw);
+  TileCtx c;
+  tile_load(S, L, c, quad, ess, indptr, 8);
+  if (o.vals[BK_A]) { tile_block<BK_A>(S, L); tile_write<BK_A>(S, L, c, o.vals[BK_A]); }
+  if (o.vals[BK_C]) { tile_block<BK_C>(S, L); tile_write<BK_C>(S, L, c, o.vals[BK_C]); }
+  if (o.vals[BK_WUM]) { tile_block<BK_WUM>(S, L); tile_write<BK_WUM>(S, L, c, o.vals[BK_WUM]); }
+  if (o.vals[BK_WMM]) { tile_block<BK_WMM>(S, L); tile_write<BK_WMM>(S, L, c, o.vals[BK_WMM]); }
+  if (o.vec_state || o.vec_param || o.vec_adj) {
+    __syncthreads();
+    tile_vectors(S, L, c, o.f, o.vec_state, o.vec_param, o.vec_adj, o.zero_ess != 0);
+  }
+}
+
+// ====================================================== matrix-free Jacobian apply
+// y = A(D) x on the tile's owned rows: gradients of x at the 9^3 local Gauss points
+// (node lattice -> Gauss lattice, one axis at a time), flux D grad x / h^2, and back
+// to the owned rows with the single-index tables.  x is zeroed on Dirichlet nodes,
+// and y = x there (the Jacobian's elimination).
+template <typename real>
+struct ApplySmem {
+  real x[7][7][7];        // [s3][s2][s1]
+  real D[9][9][9];        // [g3][g2][g1]
+  real Xb[9][7][7];       // [g3][s2][s1]  z interpolated
+  real Xd[9][7][7];       //               z derivative
+  real Y[3][9][9][7];     // [bb, db, bd][g3][g2][s1]
+  real G[3][9][9][9];     // flux [d][g3][g2][g1]
+  real Z[3][9][9][4];     // [term][g3][g2][r1]
+  real U[2][9][4][4];     // [B, D][g3][r2][r1]
+  uint8_t ess[7][7][7];
+};
+
+template <typename real>
+__global__ void __launch_bounds__(256)
+    k_tile_apply_A(Lattice L, const real* __restrict__ quad, const uint8_t* __restrict__ ess,
+                   const double* __restrict__ xin, double* __restrict__ yout) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ApplySmem<real>& S = *reinterpret_cast<ApplySmem<real>*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int t1 = blockIdx.x, t2 = blockIdx.y, t3 = blockIdx.z;
+  const int eb1 = 2 * t1 - 1, eb2 = 2 * t2 - 1, eb3 = 2 * t3 - 1;
+  for (int i = tid; i < 343; i += blockDim.x) {
+    const int s1 = i % 7, s2 = (i / 7) % 7, s3 = i / 49;
+    const int gx = 4 * t1 - 2 + s1, gy = 4 * t2 - 2 + s2, gz = 4 * t3 - 2 + s3;
+    real v = 0;
+    uint8_t m = 0;
+    if (gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 && gz < L.Nz) {
+      const int64_t n = gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz);
+      m = ess != nullptr ? ess[n] : 0;
+      v = m ? (real)0 : (real)xin[n];
+    }
+    S.x[s3][s2][s1] = v;
+    S.ess[s3][s2][s1] = m;
+  }
+  for (int i = tid; i < 27 * 27; i += blockDim.x) {
+    const int l = i / 27, q = i % 27;
+    const int l1 = l % 3, l2 = (l / 3) % 3, l3 = l / 9;
+    const int ex = eb1 + l1, ey = eb2 + l2, ez = eb3 + l3;
+    real v = 0;
+    if (ex >= 0 && ex < L.nx && ey >= 0 && ey < L.ny && ez >= 0 && ez < L.nz)
+      v = quad[(ex + (int64_t)L.nx * (ey + (int64_t)L.ny * ez)) * 216 + q];
+    S.D[3 * l3 + q / 9][3 * l2 + (q / 3) % 3][3 * l1 + q % 3] = v;
+  }
+  __syncthreads();
+  // z: nodes -> Gauss points
+  for (int task = tid; task < 49; task += blockDim.x) {
+    const int s1 = task % 7, s2 = task / 7;
+    real xs[7];
+#pragma unroll
+    for (int s = 0; s < 7; ++s) xs[s] = S.x[s][s2][s1];
+#pragma unroll
+    for (int g = 0; g < 9; ++g) {
+      real vb = 0, vd = 0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        vb = fma((real)bq(g % 3, a), xs[2 * (g / 3) + a], vb);
+        vd = fma((real)dbq(g % 3, a), xs[2 * (g / 3) + a], vd);
+      }
+      S.Xb[g][s2][s1] = vb;
+      S.Xd[g][s2][s1] = vd;
+    }
+  }
+  __syncthreads();
+  // y: nodes -> Gauss points
+  for (int task = tid; task < 63; task += blockDim.x) {
+    const int s1 = task % 7, g3 = task / 7;
+    real xb[7], xd[7];
+#pragma unroll
+    for (int s = 0; s < 7; ++s) { xb[s] = S.Xb[g3][s][s1]; xd[s] = S.Xd[g3][s][s1]; }
+#pragma unroll
+    for (int g = 0; g < 9; ++g) {
+      real bb = 0, db = 0, bd = 0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const real B = (real)bq(g % 3, a), Dd = (real)dbq(g % 3, a);
+        bb = fma(B, xb[2 * (g / 3) + a], bb);
+        db = fma(Dd, xb[2 * (g / 3) + a], db);
+        bd = fma(B, xd[2 * (g / 3) + a], bd);
+      }
+      S.Y[0][g3][g][s1] = bb;
+      S.Y[1][g3][g][s1] = db;
+      S.Y[2][g3][g][s1] = bd;
+    }
+  }
+  __syncthreads();
+  // x: nodes -> Gauss points, then the flux D grad x / h^2
+  const real sx = (real)(1.0 / (L.hx * L.hx)), sy = (real)(1.0 / (L.hy * L.hy)),
+             sz = (real)(1.0 / (L.hz * L.hz));
+  for (int task = tid; task < 81; task += blockDim.x) {
+    const int g2 = task % 9, g3 = task / 9;
+    real bb[7], db[7], bd[7];
+#pragma unroll
+    for (int s = 0; s < 7; ++s) { bb[s] = S.Y[0][g3][g2][s]; db[s] = S.Y[1][g3][g2][s]; bd[s] = S.Y[2][g3][g2][s]; }
+#pragma unroll
+    for (int g = 0; g < 9; ++g) {
+      real gx = 0, gy = 0, gz = 0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const real B = (real)bq(g % 3, a), Dd = (real)dbq(g % 3, a);
+        gx = fma(Dd, bb[2 * (g / 3) + a], gx);
+        gy = fma(B, db[2 * (g / 3) + a], gy);
+        gz = fma(B, bd[2 * (g / 3) + a], gz);
+      }
+      const real d = S.D[g3][g2][g];
+      S.G[0][g3][g2][g] = d * gx * sx;
+      S.G[1][g3][g2][g] = d * gy * sy;
+      S.G[2][g3][g2][g] = d * gz * sz;
+    }
+  }
+  __syncthreads();
+  // back along x: Z0 = VD.Gx, Z1 = VB.Gy, Z2 = VB.Gz  -> [term][g3][g2][r1]
+  for (int task = tid; task < 81; task += blockDim.x) {
+    const int g2 = task % 9, g3 = task / 9;
+    real w0[9], w1[9], w2[9];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) { w0[l] = S.G[0][g3][g2][l]; w1[l] = S.G[1][g3][g2][l]; w2[l] = S.G[2][g3][g2][l]; }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      real a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t < vrow_cnt(r)) {
+          a0 = fma((real)vrow_coef(VD, r, t), w0[vrow_g0(r) + t], a0);
+          a1 = fma((real)vrow_coef(VB, r, t), w1[vrow_g0(r) + t], a1);
+          a2 = fma((real)vrow_coef(VB, r, t), w2[vrow_g0(r) + t], a2);
+        }
+      S.Z[0][g3][g2][r] = a0; S.Z[1][g3][g2][r] = a1; S.Z[2][g3][g2][r] = a2;
+    }
+  }
+  __syncthreads();
+  // back along y: UB = VB.Z0 + VD.Z1 (then VB in z), UD = VB.Z2 (then VD in z)
+  for (int task = tid; task < 36; task += blockDim.x) {
+    const int r1 = task % 4, g3 = task / 4;
+    real w0[9], w1[9], w2[9];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) { w0[l] = S.Z[0][g3][l][r1]; w1[l] = S.Z[1][g3][l][r1]; w2[l] = S.Z[2][g3][l][r1]; }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      real ub = 0, ud = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t < vrow_cnt(r)) {
+          ub = fma((real)vrow_coef(VB, r, t), w0[vrow_g0(r) + t], ub);
+          ub = fma((real)vrow_coef(VD, r, t), w1[vrow_g0(r) + t], ub);
+          ud = fma((real)vrow_coef(VB, r, t), w2[vrow_g0(r) + t], ud);
+        }
+      S.U[0][g3][r][r1] = ub; S.U[1][g3][r][r1] = ud;
+    }
+  }
+  __syncthreads();
+  // back along z and out
+  if (tid < 16) {
+    const int r1 = tid % 4, r2 = tid / 4;
+    real wb[9], wd[9];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) { wb[l] = S.U[0][l][r2][r1]; wd[l] = S.U[1][l][r2][r1]; }
+    const int gx = 4 * t1 + r1, gy = 4 * t2 + r2;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      real acc = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t < vrow_cnt(r)) {
+          acc = fma((real)vrow_coef(VB, r, t), wb[vrow_g0(r) + t], acc);
+          acc = fma((real)vrow_coef(VD, r, t), wd[vrow_g0(r) + t], acc);
+        }
+      const int gz = 4 * t3 + r;
+      if (gx < L.Nx && gy < L.Ny && gz < L.Nz) {
+        const int64_t n = gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz);
+        yout[n] = S.ess[r + 2][r2 + 2][r1 + 2] ? xin[n] : (double)acc;
+      }
+    }
+  }
+}
+
+// diagonal of A(D): sum_g D(g) sum_d (d_d phi_n)^2, one thread per node
+template <typename real>
+__global__ void k_diag_A(Lattice L, const real* __restrict__ quad, const uint8_t* __restrict__ ess,
+                         double* __restrict__ diag) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= L.ndof) return;
+  const int i = (int)(n % L.Nx), j = (int)((n / L.Nx) % L.Ny), k = (int)(n / ((int64_t)L.Nx * L.Ny));
+  if (ess != nullptr && ess[n]) { diag[n] = 1.0; return; }
+  const int gi[3] = {i, j, k};
+  const int ne[3] = {L.nx, L.ny, L.nz};
+  const double h2[3] = {1.0 / (L.hx * L.hx), 1.0 / (L.hy * L.hy), 1.0 / (L.hz * L.hz)};
+  // elements touching the node along each axis
+  int el0[3], nel[3];
+  for (int d = 0; d < 3; ++d) {
+    if (gi[d] & 1) { el0[d] = gi[d] / 2; nel[d] = 1; }
+    else {
+      el0[d] = gi[d] / 2 - 1; nel[d] = 2;
+      if (el0[d] < 0) { el0[d] = 0; nel[d] = 1; }
+      else if (el0[d] + 1 >= ne[d]) nel[d] = 1;
+    }
+  }
+  double acc = 0.0;
+  for (int c3 = 0; c3 < nel[2]; ++c3)
+    for (int c2 = 0; c2 < nel[1]; ++c2)
+      for (int c1 = 0; c1 < nel[0]; ++c1) {
+        const int e1 = el0[0] + c1, e2 = el0[1] + c2, e3 = el0[2] + c3;
+        const int a1 = i - 2 * e1, a2 = j - 2 * e2, a3 = k - 2 * e3;
+        const real* Dq = quad + (e1 + (int64_t)L.nx * (e2 + (int64_t)L.ny * e3)) * 216;
+        for (int q = 0; q < 27; ++q) {
+          const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
+          const double b1 = bq(q1, a1), b2 = bq(q2, a2), b3 = bq(q3, a3);
+          const double d1 = dbq(q1, a1), d2 = dbq(q2, a2), d3 = dbq(q3, a3);
+          const double s = d1 * d1 * b2 * b2 * b3 * b3 * h2[0] + b1 * b1 * d2 * d2 * b3 * b3 * h2[1] +
+                           b1 * b1 * b2 * b2 * d3 * d3 * h2[2];
+          acc += (double)Dq[q] * s;
+        }
+      }
+  diag[n] = acc;
+}
+
+}  // namespace hm
+
+// ================================================================= host launchers
+using namespace hm;
+
+namespace {
+inline int grid1(int64_t n, int block) { return (int)((n + block - 1) / block); }
+inline cudaStream_t S_(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+}
+
+int hm_launch_pattern(const Lattice& L, int32_t* indptr, int32_t* indices, int32_t* slot, void* stream) {
+  cudaStream_t s = S_(stream);
+  k_pattern_indptr<<<grid1(L.ndof + 1, 256), 256, 0, s>>>(L, indptr);
+  if (indices) k_pattern_indices<<<grid1(L.ndof * 32, 256), 256, 0, s>>>(L, indptr, indices);
+  if (slot) k_pattern_slot<<<grid1(L.ne * 729, 256), 256, 0, s>>>(L, slot);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+int hm_launch_tpos(const Lattice& L, const int32_t* indptr, int32_t* tpos, void* stream) {
+  k_pattern_tpos<<<grid1(L.ndof * 32, 256), 256, 0, S_(stream)>>>(L, indptr, tpos);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+int hm_launch_quad(const Lattice& L, const double* u, const double* m, const double* p,
+                   int precision, void* quad, uint32_t* status, void* stream) {
+  const int blocks = grid1(L.ne, 8);
+  if (precision == HM_FP32)
+    k_quad<float><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, (float*)quad, status);
+  else
+    k_quad<double><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, (double*)quad, status);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+template <typename real>
+static int launch_assemble_t(const Lattice& L, const void* quad, const int32_t* indptr,
+                             const uint8_t* ess, const AssembleOut& o, void* stream) {
+  const size_t smem = sizeof(TileSmem<real>);
+  static bool configured[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !configured[dev]) {
+    if (cudaFuncSetAttribute(k_tile_assemble<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return HM_ERR_CUDA;
+    configured[dev] = true;
+  }
+  dim3 grid(L.tx, L.ty, L.tz);
+  k_tile_assemble<real><<<grid, 256, smem, S_(stream)>>>(L, (const real*)quad, ess, indptr, o);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+int hm_launch_assemble(const Lattice& L, const void* quad, int precision, const int32_t* indptr,
+                       const uint8_t* ess, double f, double* vA, double* vC, double* vWum,
+                       double* vWmm, double* vs, double* vp, double* va, int zero_ess, void* stream) {
+  AssembleOut o;
+  o.vals[0] = vA; o.vals[1] = vC; o.vals[2] = vWum; o.vals[3] = vWmm;
+  o.vec_state = vs; o.vec_param = vp; o.vec_adj = va; o.f = f; o.zero_ess = zero_ess;
+  if (precision == HM_FP32) return launch_assemble_t<float>(L, quad, indptr, ess, o, stream);
+  return launch_assemble_t<double>(L, quad, indptr, ess, o, stream);
+}
+
+template <typename real>
+static int launch_apply_t(const Lattice& L, const void* quad, const uint8_t* ess, const double* x,
+                          double* y, void* stream) {
+  const size_t smem = sizeof(ApplySmem<real>);
+  static bool configured[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !configured[dev]) {
+    if (cudaFuncSetAttribute(k_tile_apply_A<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return HM_ERR_CUDA;
+    configured[dev] = true;
+  }
+  dim3 grid(L.tx, L.ty, L.tz);
+  k_tile_apply_A<real><<<grid, 256, smem, S_(stream)>>>(L, (const real*)quad, ess, x, y);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+int hm_launch_apply_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,
+                      const double* x, double* y, void* stream) {
+  if (precision == HM_FP32) return launch_apply_t<float>(L, quad, ess, x, y, stream);
+  return launch_apply_t<double>(L, quad, ess, x, y, stream);
+}
+
+int hm_launch_diag_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,
+                     double* diag, void* stream) {
+  if (precision == HM_FP32)
+    k_diag_A<float><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, (const float*)quad, ess, diag);
+  else
+    k_diag_A<double><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, (const double*)quad, ess, diag);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}

@@ -1,0 +1,270 @@
+"""Misfit, model and reduced Hessian on top of ``PDEVariationalProblem``.
+
+Mirrors, with the same method names and signs:
+
+* ``DiscreteStateObservation`` / ``PointwiseStateObservation`` --
+  hippymfem/modeling/misfit.py:65-125 and the observation operator of
+  hippymfem/modeling/pointwiseObservation.py:36-224 (rows of Q2 basis values at the
+  points), held as device CSR matrices ``B`` and ``B^T``;
+* ``Model`` -- the block dispatch of hippymfem/modeling/model.py:100-261 (misfit only:
+  the prior is not part of this path, so ``applyR`` is zero);
+* ``ReducedHessian`` -- hippymfem/modeling/reducedHessian.py:30-131.
+"""
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from ._lib import check, lib, ptr, stream_ptr
+from .problem import ADJOINT, PARAMETER, STATE
+
+
+def _lagrange3(x):
+    return np.stack([2.0 * (x - 0.5) * (x - 1.0), -4.0 * x * (x - 1.0), 2.0 * x * (x - 0.5)], -1)
+
+
+def observation_operator(mesh, points):
+    """Host CSR ``B``: row ``o`` holds the 27 Q2 basis values of the element that
+    contains ``points[o]`` (clamped into the box)."""
+    pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+    h = np.asarray(mesh.h)
+    n = np.asarray(mesh.n)
+    e = np.clip(np.floor(pts / h).astype(np.int64), 0, n - 1)
+    xi = pts / h - e
+    B1 = [_lagrange3(xi[:, d]) for d in range(3)]
+    Nx, Ny, _ = mesh.N
+    a = np.arange(27)
+    a1, a2, a3 = a % 3, (a // 3) % 3, a // 9
+    cols = ((2 * e[:, 0:1] + a1) + Nx * ((2 * e[:, 1:2] + a2) + Ny * (2 * e[:, 2:3] + a3)))
+    vals = B1[0][:, a1] * B1[1][:, a2] * B1[2][:, a3]
+    rows = np.repeat(np.arange(len(pts)), 27)
+    return sp.csr_matrix((vals.reshape(-1), (rows, cols.reshape(-1))),
+                         shape=(len(pts), mesh.ndof))
+
+
+class DeviceCSR:
+    """A general (rectangular) CSR matrix on the device, applied by ``hm_csr_spmv``."""
+
+    def __init__(self, M, device):
+        M = sp.csr_matrix(M)
+        M.sort_indices()
+        self.shape = M.shape
+        self.indptr = torch.as_tensor(M.indptr.astype(np.int32), device=device)
+        self.indices = torch.as_tensor(M.indices.astype(np.int32), device=device)
+        self.values = torch.as_tensor(M.data.astype(np.float64), device=device)
+
+    def mult(self, x, y, alpha=1.0, beta=0.0):
+        check(lib.hm_csr_spmv(self.shape[0], ptr(self.indptr), ptr(self.indices),
+                              ptr(self.values), ptr(x), ptr(y), float(alpha), float(beta),
+                              stream_ptr()), "hm_csr_spmv")
+        return y
+
+
+class DiscreteStateObservation:
+    """Gaussian misfit ``1/(2 sigma^2) |B u - d|^2`` (misfit.py:65-110)."""
+
+    def __init__(self, B, data=None, noise_variance=None, device="cuda"):
+        if noise_variance is None:
+            raise ValueError("noise_variance must be specified")
+        if noise_variance == 0:
+            raise ZeroDivisionError("noise_variance must not be 0; use 1.0 for a deterministic "
+                                    "inverse problem")
+        self.Bh = sp.csr_matrix(B)
+        self.B = DeviceCSR(self.Bh, device)
+        self.Bt = DeviceCSR(self.Bh.T.tocsr(), device)
+        nobs = self.Bh.shape[0]
+        self.d = (torch.as_tensor(np.asarray(data, dtype=np.float64), device=device)
+                  if data is not None else torch.zeros(nobs, dtype=torch.float64, device=device))
+        self.Bu = torch.zeros(nobs, dtype=torch.float64, device=device)
+        self.noise_variance = float(noise_variance)
+
+    def cost(self, x):
+        self.B.mult(x[STATE], self.Bu)
+        self.Bu.sub_(self.d)
+        return 0.5 / self.noise_variance * float(torch.dot(self.Bu, self.Bu))
+
+    def grad(self, i, x, out):
+        if i == STATE:
+            self.B.mult(x[STATE], self.Bu)
+            self.Bu.sub_(self.d)
+            self.Bt.mult(self.Bu, out, alpha=1.0 / self.noise_variance)
+        elif i == PARAMETER:
+            out.zero_()
+        else:
+            raise IndexError("grad index %r" % (i,))
+        return out
+
+    def setLinearizationPoint(self, x, gauss_newton_approx=False):
+        return self
+
+    def block_is_zero(self, i, j):
+        return not (i == STATE and j == STATE)
+
+    def apply_ij(self, i, j, dir, out):
+        if i == STATE and j == STATE:
+            self.B.mult(dir, self.Bu)
+            self.Bt.mult(self.Bu, out, alpha=1.0 / self.noise_variance)
+        else:
+            out.zero_()
+        return out
+
+
+def PointwiseStateObservation(Vh, obs_points, data=None, noise_variance=None):
+    """Misfit for pointwise observations of the state at ``obs_points``."""
+    mesh = Vh.mesh
+    return DiscreteStateObservation(observation_operator(mesh, obs_points), data,
+                                    noise_variance, device=mesh.device)
+
+
+class Model:
+    """``Model(problem, prior, misfit)``: the block dispatch of model.py (prior: the
+    ``R`` term is not part of this path; pass ``None``)."""
+
+    def __init__(self, problem, prior, misfit):
+        if prior is not None:
+            raise NotImplementedError("priors are not part of this path (misfit-only Hessian)")
+        self.problem = problem
+        self.prior = prior
+        self.misfit = misfit
+        self.gauss_newton_approx = False
+        self.n_fwd_solve = self.n_adj_solve = self.n_inc_solve = 0
+
+    def generate_vector(self, component="ALL"):
+        gen = {STATE: self.problem.generate_state, PARAMETER: self.problem.generate_parameter,
+               ADJOINT: self.problem.generate_adjoint}
+        if component == "ALL":
+            return [gen[i]() for i in (STATE, PARAMETER, ADJOINT)]
+        return gen[component]()
+
+    def cost(self, x):
+        misfit = self.misfit.cost(x)
+        return [misfit, 0.0, misfit]
+
+    def solveFwd(self, out, x):
+        self.n_fwd_solve += 1
+        return self.problem.solveFwd(out, x)
+
+    def solveAdj(self, out, x):
+        self.n_adj_solve += 1
+        rhs = self.problem.generate_state()
+        self.misfit.grad(STATE, x, rhs)
+        rhs.neg_()
+        return self.problem.solveAdj(out, x, rhs)
+
+    def evalGradientParameter(self, x, mg, misfit_only=True):
+        self.problem.evalGradientParameter(x, mg)
+        return float(torch.sqrt(torch.dot(mg, mg)))
+
+    def setPointForHessianEvaluations(self, x, gauss_newton_approx=False):
+        self.gauss_newton_approx = bool(gauss_newton_approx)
+        self.problem.setLinearizationPoint(x, self.gauss_newton_approx)
+        self.misfit.setLinearizationPoint(x, self.gauss_newton_approx)
+        return self
+
+    def solveFwdIncremental(self, sol, rhs, rel_tolerance=None):
+        self.n_inc_solve += 1
+        return self.problem.solveIncremental(sol, rhs, False, rel_tolerance=rel_tolerance)
+
+    def solveAdjIncremental(self, sol, rhs, rel_tolerance=None):
+        self.n_inc_solve += 1
+        return self.problem.solveIncremental(sol, rhs, True, rel_tolerance=rel_tolerance)
+
+    def applyC(self, dm, out):
+        return self.problem.apply_ij(ADJOINT, PARAMETER, dm, out)
+
+    def applyCt(self, dp, out):
+        return self.problem.apply_ij(PARAMETER, ADJOINT, dp, out)
+
+    def applyWuu(self, du, out):
+        self.misfit.apply_ij(STATE, STATE, du, out)
+        return out
+
+    def _second_order(self, i, j, d, out):
+        if self.gauss_newton_approx:
+            out.zero_()
+            return out
+        return self.problem.apply_ij(i, j, d, out)
+
+    def applyWum(self, dm, out):
+        return self._second_order(STATE, PARAMETER, dm, out)
+
+    def applyWmu(self, du, out):
+        return self._second_order(PARAMETER, STATE, du, out)
+
+    def applyWmm(self, dm, out):
+        return self._second_order(PARAMETER, PARAMETER, dm, out)
+
+    def applyR(self, dm, out):
+        out.zero_()
+        return out
+
+
+class ReducedHessian:
+    """Matrix-free reduced Hessian at the point set on the model (reducedHessian.py)."""
+
+    def __init__(self, model, misfit_only=True):
+        self.model = model
+        self.gauss_newton_approx = model.gauss_newton_approx
+        self.misfit_only = bool(misfit_only)
+        self.ncalls = 0
+        self.rhs_fwd = model.generate_vector(STATE)
+        self.rhs_adj = model.generate_vector(ADJOINT)
+        self.rhs_adj2 = model.generate_vector(ADJOINT)
+        self.uhat = model.generate_vector(STATE)
+        self.phat = model.generate_vector(ADJOINT)
+        self.yhelp = model.generate_vector(PARAMETER)
+        self.accuracy = None
+        self.iterations = []
+
+    def set_accuracy(self, tolerance):
+        self.accuracy = float(tolerance) if tolerance else None
+        return self
+
+    def _incremental(self, adjoint, sol, rhs):
+        solve = self.model.solveAdjIncremental if adjoint else self.model.solveFwdIncremental
+        solve(sol, rhs, rel_tolerance=self.accuracy)
+        self.iterations.append(self.model.problem.last_solve.iterations)
+        return sol
+
+    def mult(self, x, y):
+        if self.gauss_newton_approx:
+            self.GNHessian(x, y)
+        else:
+            self.TrueHessian(x, y)
+        self.ncalls += 1
+        return y
+
+    multTranspose = mult
+
+    def inner(self, x, y):
+        Hx = self.model.generate_vector(PARAMETER)
+        self.mult(x, Hx)
+        return float(torch.dot(Hx, y))
+
+    def GNHessian(self, x, y):
+        self.model.applyC(x, self.rhs_fwd)
+        self._incremental(False, self.uhat, self.rhs_fwd)
+        self.model.applyWuu(self.uhat, self.rhs_adj)
+        self._incremental(True, self.phat, self.rhs_adj)
+        self.model.applyCt(self.phat, y)
+        if not self.misfit_only:
+            self.model.applyR(x, self.yhelp)
+            y.add_(self.yhelp)
+        return y
+
+    def TrueHessian(self, x, y):
+        self.model.applyC(x, self.rhs_fwd)
+        self._incremental(False, self.uhat, self.rhs_fwd)
+        self.model.applyWuu(self.uhat, self.rhs_adj)
+        self.model.applyWum(x, self.rhs_adj2)
+        self.rhs_adj.sub_(self.rhs_adj2)
+        self._incremental(True, self.phat, self.rhs_adj)
+        self.model.applyWmm(x, y)
+        self.model.applyCt(self.phat, self.yhelp)
+        y.add_(self.yhelp)
+        self.model.applyWmu(self.uhat, self.yhelp)
+        y.sub_(self.yhelp)
+        if not self.misfit_only:
+            self.model.applyR(x, self.yhelp)
+            y.add_(self.yhelp)
+        return y

@@ -1,0 +1,147 @@
+"""Assembled blocks on the device and the FP64 Jacobi-PCG of the incremental solves.
+
+``CSRBlock`` stands where the reference holds a ``HypreParMatrix`` built over the
+scatter pattern (hippymfem/fem/parmat.py:106-171): its ``Mult``/``MultTranspose`` are
+``hm_csr_spmv`` / ``hm_csr_spmv_t``.  ``pcg`` replaces the hypre PCG behind
+``KrylovSolver.solve`` (hippymfem/algorithms/linSolvers.py:709); the preconditioner is
+Jacobi (BoomerAMG is out of scope).
+"""
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_ptr
+
+
+class CSRBlock:
+    """A square block in a (shared) device pattern, FP64 values."""
+
+    def __init__(self, pattern, values):
+        self.pattern = pattern
+        self.values = values
+        self.nrow = pattern.nrow
+        self.ncol = pattern.ncol
+
+    def Height(self):
+        return self.nrow
+
+    def Width(self):
+        return self.ncol
+
+    def mult(self, x, y, alpha=1.0, beta=0.0, stream=None):
+        """``y = alpha A x + beta y``."""
+        p = self.pattern
+        check(lib.hm_csr_spmv(self.nrow, ptr(p.indptr), ptr(p.indices), ptr(self.values), ptr(x),
+                              ptr(y), float(alpha), float(beta), stream_ptr(stream)), "hm_csr_spmv")
+        return y
+
+    def mult_transpose(self, x, y, alpha=1.0, beta=0.0, stream=None):
+        """``y = alpha A^T x + beta y`` (a gather through the transpose map)."""
+        p = self.pattern
+        if p.tpos is None:
+            raise ValueError("the pattern was built without its transpose map")
+        check(lib.hm_csr_spmv_t(self.nrow, ptr(p.indptr), ptr(p.indices), ptr(p.tpos),
+                                ptr(self.values), ptr(x), ptr(y), float(alpha), float(beta),
+                                stream_ptr(stream)), "hm_csr_spmv_t")
+        return y
+
+    Mult = mult
+    MultTranspose = mult_transpose
+
+    def diagonal(self, out=None, stream=None):
+        out = out if out is not None else torch.empty(self.nrow, dtype=torch.float64,
+                                                      device=self.values.device)
+        check(lib.hm_csr_diag(self.nrow, ptr(self.pattern.indptr), ptr(self.values), ptr(out),
+                              stream_ptr(stream)), "hm_csr_diag")
+        return out
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+
+        p = self.pattern
+        return sp.csr_matrix((self.values.cpu().numpy(), p.indices.cpu().numpy(),
+                              p.indptr.cpu().numpy()), shape=(self.nrow, self.ncol))
+
+
+class MatrixFreeJacobian:
+    """The Jacobian ``A(m)`` applied from the quadrature data of a point, with its
+    elimination (``apply_ij_at`` for the (ADJOINT, STATE) pair)."""
+
+    def __init__(self, mesh, quad, ess_marker, precision=_lib.HM_FP64):
+        self.mesh, self.quad, self.ess, self.precision = mesh, quad, ess_marker, precision
+        self.nrow = self.ncol = mesh.ndof
+
+    def mult(self, x, y, stream=None):
+        check(lib.hm_lattice_apply_A(self.mesh.handle, ptr(self.quad), self.precision,
+                                     ptr(self.ess), ptr(x), ptr(y), stream_ptr(stream)),
+              "hm_lattice_apply_A")
+        return y
+
+    Mult = mult
+    # the Jacobian of this density is symmetric (A^T = A)
+    mult_transpose = MultTranspose = mult
+
+    def diagonal(self, out=None, stream=None):
+        out = out if out is not None else torch.empty(self.nrow, dtype=torch.float64,
+                                                      device=self.mesh.device)
+        check(lib.hm_lattice_diag_A(self.mesh.handle, ptr(self.quad), self.precision,
+                                    ptr(self.ess), ptr(out), stream_ptr(stream)),
+              "hm_lattice_diag_A")
+        return out
+
+
+class PCGResult:
+    __slots__ = ("iterations", "relres", "converged")
+
+    def __init__(self, iterations, relres, converged):
+        self.iterations, self.relres, self.converged = iterations, relres, converged
+
+    def __repr__(self):
+        return "PCGResult(iterations=%d, relres=%.3e, converged=%s)" % (
+            self.iterations, self.relres, self.converged)
+
+
+class PCGSolver:
+    """Jacobi-PCG for ``A x = b``, FP64 throughout, on the device.
+
+    ``operator`` is a ``CSRBlock`` or a ``MatrixFreeJacobian``; the workspace and the
+    diagonal are allocated once and kept (the reference keeps its solver objects and
+    AMG hierarchies per operator the same way)."""
+
+    def __init__(self, operator, rel_tolerance=1e-12, max_iter=20000, check_every=16,
+                 raise_on_fail=True):
+        self.parameters = {"rel_tolerance": float(rel_tolerance), "max_iter": int(max_iter),
+                           "check_every": int(check_every)}
+        self.raise_on_fail = raise_on_fail
+        self.last = None
+        self.set_operator(operator)
+
+    def set_operator(self, operator):
+        self.op = operator
+        n = operator.nrow
+        dev = (operator.values.device if isinstance(operator, CSRBlock)
+               else operator.mesh.device)
+        self.diag = operator.diagonal()
+        nbytes = lib.hm_pcg_workspace_bytes(n)
+        self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=dev)
+        return self
+
+    def solve(self, x, b, stream=None):
+        op = self.op
+        it, rr = ctypes.c_int(), ctypes.c_double()
+        prm = self.parameters
+        if isinstance(op, CSRBlock):
+            p = op.pattern
+            args = (ptr(p.indptr), ptr(p.indices), ptr(op.values), None, None, _lib.HM_FP64, None)
+        else:
+            args = (None, None, None, op.mesh.handle, ptr(op.quad), op.precision, ptr(op.ess))
+        rc = lib.hm_pcg(op.nrow, *args, ptr(self.diag), ptr(b), ptr(x),
+                        prm["rel_tolerance"], prm["max_iter"], prm["check_every"], ptr(self.work),
+                        ctypes.byref(it), ctypes.byref(rr), stream_ptr(stream))
+        self.last = PCGResult(it.value, rr.value, rc == _lib.HM_OK)
+        if rc == _lib.HM_ERR_NOCONV and not self.raise_on_fail:
+            return x
+        check(rc, "hm_pcg")
+        return x

@@ -1,0 +1,173 @@
+/*
+ * hippymfem_b200 -- C ABI of the B200 kernels for the Q2 log-conductivity diffusion
+ * path:  -div(e^m grad u) = f  on hexahedra, density  e^m grad u . grad p - f p.
+ *
+ * Conventions
+ *   - every function returns an int status: HM_OK (0) or one of HM_ERR_*;
+ *   - pointers named d_* are device pointers (any allocator: torch, cudaMalloc, ...);
+ *     the library allocates no device memory in any of these calls: scratch is passed
+ *     in as a workspace whose size the *_workspace_bytes functions report;
+ *   - `stream` is a cudaStream_t passed as void* (NULL: the legacy default stream);
+ *     every launch goes to that stream and nothing synchronises unless stated;
+ *   - d_status, where taken, is one device uint32 that kernels OR bits into
+ *     (HM_STATUS_*); the caller zeroes it and reads it when it wants to;
+ *   - slots follow the reference: STATE = 0, PARAMETER = 1, ADJOINT = 2
+ *     (hippymfem/modeling/variables.py); a block (i, j) has test slot i as rows.
+ *
+ * The interfaces each call replaces are named as file:line in the hIPPyMFEM tree.
+ */
+#ifndef HIPPYMFEM_B200_H
+#define HIPPYMFEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; the Python layer maps them onto the reference's exceptions */
+#define HM_OK 0
+#define HM_ERR_ARG 1         /* ValueError: sizes or arguments do not match        */
+#define HM_ERR_CUDA 2        /* a CUDA runtime call failed                          */
+#define HM_ERR_NONFINITE 3   /* RuntimeError: non-finite element values            */
+#define HM_ERR_NOMEM 4       /* MemoryError: a workspace is too small              */
+#define HM_ERR_NOCONV 5      /* an iterative solve did not reach its tolerance     */
+#define HM_ERR_RANGE 6       /* an index was out of range                          */
+#define HM_ERR_UNSUPPORTED 7 /* a case this build does not cover                   */
+
+/* bits of the device status word */
+#define HM_STATUS_NONFINITE 1u
+#define HM_STATUS_RANGE 2u
+
+/* arithmetic of the element contractions; CSR values are always FP64 */
+#define HM_FP64 0
+#define HM_FP32 1
+
+const char* hm_error_string(int code);
+int hm_version(void);
+
+/* ------------------------------------------------------------------ sparsity pattern
+ * hm_pattern_build: CSR graph and entry->slot map of the element-assembly map of one
+ * element group, from its two dof tables.  Replaces patternbuild.build_tables
+ * (hippymfem/fem/patternbuild.py:209-253) and the sort route of
+ * ScatterPattern._build (hippymfem/fem/pattern.py:548-663); identical arrays.
+ *   tdofs (ne, ndt), cdofs (ne, ndr): host int64 dof tables, row-major;
+ *   entry k = (e*ndt + a)*ndr + b is row tdofs[e,a], column cdofs[e,b];
+ *   diag_first: rows lead with their diagonal (a square pattern, as hypre keeps it).
+ * Two calls: with indices == NULL and slot == NULL it fills indptr (nrow+1) and *nnz;
+ * with both given (indices of capacity >= *nnz, slot of ne*ndt*ndr) it fills all.
+ * Host memory, nthreads host threads (0: all). */
+int hm_pattern_build(const int64_t* tdofs, const int64_t* cdofs, int64_t ne, int ndt,
+                     int ndr, int64_t nrow, int64_t ncol, int diag_first, int nthreads,
+                     int32_t* indptr, int32_t* indices, int64_t indices_capacity,
+                     int32_t* slot, int64_t* nnz);
+
+/* --------------------------------------------------------------- structured lattice
+ * A uniform nx x ny x nz hexahedral mesh of [0,Lx]x[0,Ly]x[0,Lz] with the Q2 dofs
+ * numbered lexicographically on the (2nx+1)(2ny+1)(2nz+1) node lattice and elements
+ * e = ex + nx (ey + ny ez); element-local dof a = a1 + 3 a2 + 9 a3.  Plays the role of
+ * MeshBatches / ElementGroup / SpaceTables (hippymfem/fem/elementbatch.py:159-294,
+ * 413-565) for this mesh: geometry and dof tables are arithmetic, nothing is stored.
+ * The handle is host memory only; it may be shared by any number of streams. */
+typedef struct hm_lattice hm_lattice;
+
+int hm_lattice_create(int nx, int ny, int nz, double Lx, double Ly, double Lz,
+                      hm_lattice** out);
+int hm_lattice_destroy(hm_lattice* h);
+/* ne, ndof, nnz of a Q2 x Q2 block, and the bytes of the quadrature workspace of
+ * hm_lattice_quadrature at the given precision */
+int hm_lattice_sizes(const hm_lattice* h, int precision, int64_t* ne, int64_t* ndof,
+                     int64_t* nnz, int64_t* quad_bytes);
+
+/* The pattern of a Q2 x Q2 block on the lattice, on the device, arithmetically:
+ * d_indptr (ndof+1), d_indices (nnz) and, if d_slot is not NULL, the entry->slot map
+ * (ne*729) -- the arrays hm_pattern_build / patternbuild.build_tables give for the
+ * lattice's dof table.  Replaces get_pattern (hippymfem/fem/pattern.py:1094). */
+int hm_lattice_pattern(const hm_lattice* h, int32_t* d_indptr, int32_t* d_indices,
+                       int32_t* d_slot, void* stream);
+
+/* Position of the transposed entry: d_tpos[s] = slot of (col, row) for the entry s =
+ * (row, col) of the lattice pattern (structurally symmetric).  Lets a block be applied
+ * transposed as a gather (hm_csr_spmv_t), the B200 replacement of
+ * HypreParMatrix::MultTranspose in apply_ij (modeling/PDEVariationalProblem.py:1629). */
+int hm_lattice_transpose_map(const hm_lattice* h, const int32_t* d_indptr,
+                             int32_t* d_tpos, void* stream);
+
+/* Quadrature data of the point (u, m, p): per element and Gauss point
+ * D = w|J| e^m, E = D grad u, F = D grad p, W = D grad u . grad p, the pointwise
+ * second derivatives of the density that the quadrature route of the reference's
+ * element kernel forms (hippymfem/fem/kernel.py:1431-1485) after the field
+ * evaluation of _eval_field (kernel.py:378-394).  d_quad: quad_bytes of workspace.
+ * Non-finite values set HM_STATUS_NONFINITE in *d_status (require_finite_arrays,
+ * modeling/PDEVariationalProblem.py:1844-1892). */
+int hm_lattice_quadrature(const hm_lattice* h, const double* d_u, const double* d_m,
+                          const double* d_p, int precision, void* d_quad,
+                          uint32_t* d_status, void* stream);
+
+/* Fused assembly from quadrature data: the CSR values of the blocks whose pointer is
+ * not NULL -- A = d2R/dp du (ADJOINT, STATE), C = d2R/dp dm (ADJOINT, PARAMETER),
+ * Wum = d2R/du dm (STATE, PARAMETER), Wmm = d2R/dm dm -- in the lattice pattern
+ * (d_indptr of hm_lattice_pattern), each value written once, with the folded
+ * Dirichlet elimination of hippymfem/fem/bcs.py:13-30 on the nodes d_ess marks
+ * (uint8 per dof, NULL: none): A rows and columns zeroed with a unit diagonal, C and
+ * Wum rows zeroed, Wmm untouched.  And the assembled vectors whose pointer is not
+ * NULL: dR/du (STATE), dR/dm (PARAMETER), dR/dp (ADJOINT, the residual with source f);
+ * with zero_ess_vectors the STATE and ADJOINT ones are zeroed on d_ess.
+ * Replaces setLinearizationPoint's shared pass (modeling/PDEVariationalProblem.py:
+ * 1372-1482), _jacobian (:542), _residual (:423), element_matrices_many /
+ * element_vectors (hippymfem/fem/kernel.py:2048,2070) and the scatter
+ * ScatterPattern.data (hippymfem/fem/pattern.py:749-791). */
+int hm_lattice_assemble(const hm_lattice* h, const void* d_quad, int precision,
+                        const int32_t* d_indptr, const uint8_t* d_ess, double f,
+                        double* d_vals_A, double* d_vals_C, double* d_vals_Wum,
+                        double* d_vals_Wmm, double* d_vec_state, double* d_vec_param,
+                        double* d_vec_adjoint, int zero_ess_vectors, void* stream);
+
+/* Matrix-free Q2 operator y = A(D) x with the Jacobian's elimination (x zeroed on
+ * d_ess, y = x there), D the first component of the quadrature data: the product
+ * apply_ij_at gives for (ADJOINT, STATE) (modeling/PDEVariationalProblem.py:1672). */
+int hm_lattice_apply_A(const hm_lattice* h, const void* d_quad, int precision,
+                       const uint8_t* d_ess, const double* d_x, double* d_y, void* stream);
+/* diagonal of A(D) (eliminated rows: 1), for Jacobi preconditioning */
+int hm_lattice_diag_A(const hm_lattice* h, const void* d_quad, int precision,
+                      const uint8_t* d_ess, double* d_diag, void* stream);
+
+/* ----------------------------------------------------------------- sparse / solve
+ * y = alpha * M x + beta * y for a CSR block (hypre's Mult, apply_ij). */
+int hm_csr_spmv(int64_t nrow, const int32_t* d_indptr, const int32_t* d_indices,
+                const double* d_vals, const double* d_x, double* d_y, double alpha,
+                double beta, void* stream);
+/* y = alpha * M^T x + beta * y for a square block with a structurally symmetric
+ * pattern, through d_tpos of hm_lattice_transpose_map (MultTranspose, apply_ij). */
+int hm_csr_spmv_t(int64_t nrow, const int32_t* d_indptr, const int32_t* d_indices,
+                  const int32_t* d_tpos, const double* d_vals, const double* d_x,
+                  double* d_y, double alpha, double beta, void* stream);
+/* diagonal of a CSR block whose rows lead with their diagonal */
+int hm_csr_diag(int64_t nrow, const int32_t* d_indptr, const double* d_vals,
+                double* d_diag, void* stream);
+
+/* Jacobi-preconditioned CG in FP64 for A x = b with A a CSR block (d_indptr != NULL)
+ * or the lattice's matrix-free operator (lattice != NULL, d_quad its D), stopped at
+ * ||r||_2 <= rtol ||b||_2 or maxiter.  The B200 replacement of the incremental
+ * solves' hypre PCG (modeling/PDEVariationalProblem.py:1583-1609,
+ * algorithms/linSolvers.py:709).  x is the initial guess on entry.  The iteration
+ * runs on the device; the host reads the residual norm every check_every
+ * iterations (one synchronisation each).  d_work: hm_pcg_workspace_bytes(n). */
+int64_t hm_pcg_workspace_bytes(int64_t n);
+int hm_pcg(int64_t n, const int32_t* d_indptr, const int32_t* d_indices,
+           const double* d_vals, const hm_lattice* lattice, const void* d_quad,
+           int precision, const uint8_t* d_ess, const double* d_diag, const double* d_b,
+           double* d_x, double rtol, int maxiter, int check_every, void* d_work,
+           int* iterations, double* relres, void* stream);
+
+/* deterministic FP64 dot product into *d_out (a fixed-order two-pass reduction) */
+int64_t hm_dot_workspace_bytes(int64_t n);
+int hm_dot(int64_t n, const double* d_x, const double* d_y, double* d_out, void* d_work,
+           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIPPYMFEM_B200_H */

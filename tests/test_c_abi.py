@@ -1,0 +1,96 @@
+"""The C ABI without a GPU: the library loads, exports every declared entry point, and
+its host pattern build reproduces the reference's arrays.  CPU only."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_cases, load_golden
+from oracle import q2
+
+HEADER = os.path.join(ROOT, "include", "hippymfem_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hm_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from hippymfem_b200 import _lib
+
+    names = declared_symbols()
+    assert len(names) >= 18
+    for n in names:
+        assert hasattr(_lib.lib, n), n
+        assert n in _lib.SIGNATURES, "no ctypes signature for %s" % n
+    assert _lib.lib.hm_version() >= 100
+    assert _lib.lib.hm_error_string(1).decode().startswith("invalid")
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_host_pattern_build_matches_reference_golden(name):
+    from hippymfem_b200.pattern import build_tables
+
+    z = load_golden(name)
+    got = build_tables(z["tdofs"], z["cdofs"], int(z["nrow"]), int(z["ncol"]),
+                       bool(z["diag_first"]), nthreads=3)
+    for a, key in zip(got[:3], ("indptr", "indices", "slot")):
+        assert a.dtype == z[key].dtype, key
+        assert np.array_equal(a, z[key]), key
+    assert got[3] == int(z["nnz"])
+
+
+def test_host_pattern_build_large_lattice_matches_oracle():
+    from hippymfem_b200.pattern import build_tables
+
+    mesh = q2.Lattice((6, 5, 7))
+    E = mesh.edofs()
+    rng = np.random.default_rng(1)
+    perm = rng.permutation(mesh.ndof)
+    E = perm[E]                                  # an arbitrary global numbering
+    got = build_tables(E, E, mesh.ndof, mesh.ndof, nthreads=4)
+    ref = q2.build_tables(E, E, mesh.ndof, mesh.ndof, True)
+    for a, b in zip(got[:3], ref[:3]):
+        assert np.array_equal(a, b)
+    assert got[3] == ref[3]
+
+
+def test_host_pattern_build_errors():
+    from hippymfem_b200.pattern import build_tables
+
+    t = np.array([[0, 1, 2], [2, 3, 9]])
+    with pytest.raises(IndexError):
+        build_tables(t, t, 5, 5)
+    with pytest.raises(ValueError):
+        build_tables(t, t[:1], 5, 5)
+
+
+def test_lattice_handle_sizes():
+    from hippymfem_b200 import _lib
+
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib.hm_lattice_create(64, 64, 64, 1.0, 1.0, 1.0, ctypes.byref(h)))
+    ne, nd, nnz, qb = (ctypes.c_int64() for _ in range(4))
+    _lib.check(_lib.lib.hm_lattice_sizes(h, _lib.HM_FP64, ctypes.byref(ne), ctypes.byref(nd),
+                                         ctypes.byref(nnz), ctypes.byref(qb)))
+    assert (ne.value, nd.value, nnz.value) == (262144, 2146689, 135005697)
+    assert qb.value == 262144 * 216 * 8
+    _lib.lib.hm_lattice_destroy(h)
+    with pytest.raises(ValueError):
+        _lib.check(_lib.lib.hm_lattice_create(0, 4, 4, 1.0, 1.0, 1.0, ctypes.byref(h)))
+    with pytest.raises(NotImplementedError):      # nnz beyond int32 (hypre's HYPRE_Int)
+        _lib.check(_lib.lib.hm_lattice_create(256, 256, 256, 1.0, 1.0, 1.0, ctypes.byref(h)))
+
+
+def test_ops_refuse_host_tensors():
+    """No CPU fallback: a host tensor is an error, not a slow path."""
+    import torch
+    from hippymfem_b200._lib import ptr
+
+    with pytest.raises(ValueError):
+        ptr(torch.zeros(4, dtype=torch.float64))
