@@ -192,22 +192,63 @@ __global__ void __launch_bounds__(216) k_quad(Lattice L, const double* __restric
 }
 
 // ================================================================ tile assembly
+// Position of every (p1, p2, p3) output of an interior tile (no stencil clipped) in the
+// tile's CSR-ordered output: runs (r2, r3) of four consecutive rows r1, each row
+// diagonal first and then its columns ascending (z, then y, then x rank).
+struct TileTabs {
+  uint16_t inv[16][16][16];  // [p3][p2][p1] -> position in the tile output
+  uint16_t runoff[17];       // start of run r2 + 4 r3
+};
+HM_HD constexpr TileTabs make_tile_tabs() {
+  TileTabs t{};
+  int off = 0;
+  for (int run = 0; run < 16; ++run) {
+    const int r2 = run & 3, r3 = run >> 2;
+    t.runoff[run] = (uint16_t)off;
+    const int n2 = row_stencil(r2), n3 = row_stencil(r3);
+    const int d2 = (r2 & 1) ? 1 : 2, d3 = (r3 & 1) ? 1 : 2;
+    for (int r1 = 0; r1 < 4; ++r1) {
+      const int n1 = row_stencil(r1), d1 = (r1 & 1) ? 1 : 2;
+      const int kd = (d3 * n2 + d2) * n1 + d1;
+      for (int k3 = 0; k3 < n3; ++k3)
+        for (int k2 = 0; k2 < n2; ++k2)
+          for (int k1 = 0; k1 < n1; ++k1) {
+            const int rank = (k3 * n2 + k2) * n1 + k1;
+            const int pos = rank == kd ? 0 : (rank < kd ? rank + 1 : rank);
+            t.inv[row_pair_base(r3) + k3][row_pair_base(r2) + k2][row_pair_base(r1) + k1] =
+                (uint16_t)(off + pos);
+          }
+      off += n1 * n2 * n3;
+    }
+  }
+  t.runoff[16] = (uint16_t)off;
+  return t;
+}
+__device__ const TileTabs kTileTabs = make_tile_tabs();
+
 template <typename real>
 struct TileSmem {
-  real W[8][9][9][9];      // pointwise data on the tile's 9^3 local Gauss lattice
+  real W[8][9][9][9];      // pointwise data of the 27 halo'd elements on the 9^3 Gauss lattice
   real T1[16][9][9];       // after the z contraction: [p3][g2][g1]
   real T2[16][16][9];      // after the y contraction: [p3][p2][g1]
-  real V[16][16][17];      // finished values [p3][p2][p1] (padded: conflict-free)
-  uint8_t ess[7][7][7];    // Dirichlet markers of the halo'd nodes [s3][s2][s1]
+  real O[4096];            // the tile's rows of one block, CSR-ordered (run-major)
   int32_t rowptr[4][4][4]; // CSR offsets of the owned rows [r3][r2][r1]
+  int32_t rowoff[4][4][4]; // offsets of the rows in O (tiles with clipped stencils)
+  int32_t runoff[17];      // offsets of the runs in O
+  uint8_t ess[7][7][7];    // Dirichlet markers of the halo'd nodes [s3][s2][s1]
+  int8_t nst[3][4];        // stencil size of each owned row, per axis (0: no row)
+  int8_t clip[3][4];       // columns clipped at the low end of that stencil
+  int8_t dk[3][4];         // the row's own place in its (clipped) stencil
 };
 
 struct TileCtx {
   int t1, t2, t3;      // tile coordinates
   int vl[3];           // bit l set: halo'd element l is inside the mesh, per axis
+  bool clipped;        // some owned row has a clipped stencil or lies outside the mesh
+  bool has_ess;        // some halo'd node is a Dirichlet node
 };
 
-// stage 1: contract the z axis of weight c with table TZ -> T1[p3][g2][g1]
+// stage 1: contract the z axis of one weight with table TZ -> T1[p3][g2][g1]
 template <int TZ, typename real>
 __device__ __forceinline__ void stage1(const real* __restrict__ Wc, real* __restrict__ T1) {
   for (int task = threadIdx.x; task < 81; task += blockDim.x) {
@@ -247,27 +288,71 @@ __device__ __forceinline__ void stage2(const real* __restrict__ T1, real* __rest
   }
 }
 
-// stage 3: contract the x axis with table TX -> V[p3][p2][p1] (= or +=)
-template <int TX, bool ACC, typename real>
-__device__ __forceinline__ void stage3(const real* __restrict__ T2, real* __restrict__ V) {
+enum BlockKind { BK_A = 0, BK_C = 1, BK_WUM = 2, BK_WMM = 3 };
+
+// Place of output (p1, p2, p3) in O for a tile with clipped stencils; -1 if its column
+// lies outside the mesh (or its row does).
+template <typename real>
+__device__ __forceinline__ int clipped_pos(const TileSmem<real>& S, int p1, int p2, int p3) {
+  const int r1 = pair_row_of(p1), r2 = pair_row_of(p2), r3 = pair_row_of(p3);
+  const int n1 = S.nst[0][r1], n2 = S.nst[1][r2], n3 = S.nst[2][r3];
+  if (n1 == 0 || n2 == 0 || n3 == 0) return -1;
+  const int k1 = p1 - row_pair_base(r1) - S.clip[0][r1];
+  const int k2 = p2 - row_pair_base(r2) - S.clip[1][r2];
+  const int k3 = p3 - row_pair_base(r3) - S.clip[2][r3];
+  if (k1 < 0 || k1 >= n1 || k2 < 0 || k2 >= n2 || k3 < 0 || k3 >= n3) return -1;
+  const int rank = (k3 * n2 + k2) * n1 + k1;
+  const int kd = (S.dk[2][r3] * n2 + S.dk[1][r2]) * n1 + S.dk[0][r1];
+  const int pos = rank == kd ? 0 : (rank < kd ? rank + 1 : rank);
+  return S.rowoff[r3][r2][r1] + pos;
+}
+
+// stage 3: contract the x axis with table TX and scatter into the CSR-ordered tile
+// output O (= or +=); the last group of a block applies its folded elimination:
+// A rows and columns of Dirichlet nodes zeroed with a unit diagonal, C and Wum rows
+// zeroed, Wmm untouched.
+template <int TX, bool ACC, int BLK, bool FINAL, typename real>
+__device__ __forceinline__ void stage3(TileSmem<real>& S, const TileCtx& c) {
+  const real* __restrict__ T2 = &S.T2[0][0][0];
   for (int task = threadIdx.x; task < 256; task += blockDim.x) {
     const int p2 = task % 16, p3 = task / 16;
     real w[9];
 #pragma unroll
     for (int l = 0; l < 9; ++l) w[l] = T2[(p3 * 16 + p2) * 9 + l];
-    real* out = V + (p3 * 16 + p2) * 17;
+    uint16_t pos[16];
+    if (!c.clipped) {
+      const uint4* src = reinterpret_cast<const uint4*>(&kTileTabs.inv[p3][p2][0]);
+      const uint4 a = __ldg(src), b = __ldg(src + 1);
+      const uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i) { pos[2 * i] = wv[i] & 0xffffu; pos[2 * i + 1] = wv[i] >> 16; }
+    }
+    const bool check = FINAL && BLK != BK_WMM && c.has_ess;
+    const int r2 = pair_row_of(p2), r3 = pair_row_of(p3);
+    const int c2 = pair_c(p2), c3 = pair_c(p3);
+    const bool diag23 = pair_s(p2) == c2 && pair_s(p3) == c3;
 #pragma unroll
     for (int p = 0; p < 16; ++p) {
       real acc = 0;
 #pragma unroll
       for (int t = 0; t < 6; ++t)
         if (t < pair_cnt(p)) acc = fma((real)pair_coef(TX, p, t), w[pair_g0(p) + t], acc);
-      out[p] = ACC ? out[p] + acc : acc;
+      const int at = c.clipped ? clipped_pos(S, p, p2, p3) : (int)pos[p];
+      if (at < 0) continue;
+      real v = ACC ? S.O[at] + acc : acc;
+      if (check) {
+        const bool ress = S.ess[r3 + 2][r2 + 2][pair_row_of(p) + 2] != 0;
+        if (BLK == BK_A) {
+          const bool cess = S.ess[c3][c2][pair_c(p)] != 0;
+          if (ress || cess) v = (ress && diag23 && pair_s(p) == pair_c(p)) ? (real)1 : (real)0;
+        } else if (ress) {
+          v = 0;
+        }
+      }
+      S.O[at] = v;
     }
   }
 }
-
-enum BlockKind { BK_A = 0, BK_C = 1, BK_WUM = 2, BK_WMM = 3 };
 
 // The separable terms of each block; terms that share the x table form one stage-3
 // group, and each group's y/z partial sums are added before the x contraction:
@@ -277,19 +362,18 @@ enum BlockKind { BK_A = 0, BK_C = 1, BK_WUM = 2, BK_WMM = 3 };
 //   Wmm = M.M.M (W)
 // (tables as x.y.z; the weights carry w|J| and the physical gradients)
 template <int BLK, typename real>
-__device__ __forceinline__ void tile_block(TileSmem<real>& S, const Lattice& L) {
+__device__ __forceinline__ void tile_block(TileSmem<real>& S, const Lattice& L, const TileCtx& c) {
   real* T1 = &S.T1[0][0][0];
   real* T2 = &S.T2[0][0][0];
-  real* V = &S.V[0][0][0];
   if (BLK == BK_A) {
     const real* D = &S.W[0][0][0][0];
     stage1<TM>(D, T1); __syncthreads();
     stage2<TM, false>(T1, T2, (real)(1.0 / (L.hx * L.hx))); __syncthreads();
-    stage3<TK, false>(T2, V); __syncthreads();
+    stage3<TK, false, BLK, false>(S, c); __syncthreads();
     stage2<TK, false>(T1, T2, (real)(1.0 / (L.hy * L.hy))); __syncthreads();
     stage1<TK>(D, T1); __syncthreads();
     stage2<TM, true>(T1, T2, (real)(1.0 / (L.hz * L.hz))); __syncthreads();
-    stage3<TM, true>(T2, V); __syncthreads();
+    stage3<TM, true, BLK, true>(S, c); __syncthreads();
   } else if (BLK == BK_C || BLK == BK_WUM) {
     const int c0 = BLK == BK_C ? 1 : 4;
     const real* Gx = &S.W[c0][0][0][0];
@@ -297,76 +381,35 @@ __device__ __forceinline__ void tile_block(TileSmem<real>& S, const Lattice& L) 
     const real* Gz = &S.W[c0 + 2][0][0][0];
     stage1<TM>(Gx, T1); __syncthreads();
     stage2<TM, false>(T1, T2, (real)(1.0 / L.hx)); __syncthreads();
-    stage3<TR, false>(T2, V); __syncthreads();
+    stage3<TR, false, BLK, false>(S, c); __syncthreads();
     stage1<TM>(Gy, T1); __syncthreads();
     stage2<TR, false>(T1, T2, (real)(1.0 / L.hy)); __syncthreads();
     stage1<TR>(Gz, T1); __syncthreads();
     stage2<TM, true>(T1, T2, (real)(1.0 / L.hz)); __syncthreads();
-    stage3<TM, true>(T2, V); __syncthreads();
+    stage3<TM, true, BLK, true>(S, c); __syncthreads();
   } else {
     const real* Wq = &S.W[7][0][0][0];
     stage1<TM>(Wq, T1); __syncthreads();
     stage2<TM, false>(T1, T2, (real)1.0); __syncthreads();
-    stage3<TM, false>(T2, V); __syncthreads();
+    stage3<TM, false, BLK, true>(S, c); __syncthreads();
   }
 }
 
-__device__ __forceinline__ int div35(int x, int n) { return n == 5 ? x / 5 : x / 3; }
-
-// Stream the tile's finished rows of one block out in CSR order, with the block's
-// folded elimination: A rows and columns of Dirichlet nodes zeroed and a unit
-// diagonal; C and Wum rows zeroed; Wmm untouched.  A warp covers one x-run of up to
-// four rows, which is contiguous in the CSR arrays, lanes on consecutive positions.
-template <int BLK, typename real>
-__device__ __forceinline__ void tile_write(const TileSmem<real>& S, const Lattice& L,
-                                           const TileCtx& c, double* __restrict__ vals) {
+// Stream the tile's rows of one block out: each run of four consecutive rows is one
+// contiguous stretch of the CSR values and of O; a warp copies a run, lanes on
+// consecutive positions.
+template <typename real>
+__device__ __forceinline__ void tile_write(const TileSmem<real>& S, const TileCtx& c,
+                                           double* __restrict__ vals) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarp = blockDim.x >> 5;
   for (int run = warp; run < 16; run += nwarp) {
     const int r2 = run & 3, r3 = run >> 2;
-    const int gy = 4 * c.t2 + r2, gz = 4 * c.t3 + r3;
-    if (gy >= L.Ny || gz >= L.Nz) continue;
-    const int n2 = stencil_n(gy, L.Ny), lo2 = stencil_lo(gy);
-    const int n3 = stencil_n(gz, L.Nz), lo3 = stencil_lo(gz);
-    int len[4], pre[5];
-    pre[0] = 0;
-#pragma unroll
-    for (int r1 = 0; r1 < 4; ++r1) {
-      const int gx = 4 * c.t1 + r1;
-      len[r1] = gx < L.Nx ? stencil_n(gx, L.Nx) * n2 * n3 : 0;
-      pre[r1 + 1] = pre[r1] + len[r1];
-    }
-    const int64_t base = S.rowptr[r3][r2][0];
-    const bool ress_yz = false;
-    (void)ress_yz;
-    for (int j = lane; j < pre[4]; j += 32) {
-      const int r1 = j < pre[1] ? 0 : j < pre[2] ? 1 : j < pre[3] ? 2 : 3;
-      const int pos = j - pre[r1];
-      const int gx = 4 * c.t1 + r1;
-      const int n1 = stencil_n(gx, L.Nx), lo1 = stencil_lo(gx);
-      const int kd = ((gz - lo3) * n2 + (gy - lo2)) * n1 + (gx - lo1);
-      const int rank = pos == 0 ? kd : (pos <= kd ? pos - 1 : pos);
-      const int t = div35(rank, n1);
-      const int k1 = rank - t * n1;
-      const int k3 = div35(t, n2);
-      const int k2 = t - k3 * n2;
-      // local column nodes (0..6) and the 1D pair of each axis
-      const int s1 = lo1 + k1 - (4 * c.t1 - 2), s2 = lo2 + k2 - (4 * c.t2 - 2), s3 = lo3 + k3 - (4 * c.t3 - 2);
-      const int p1 = row_pair_base(r1) + s1 - row_col_start(r1);
-      const int p2 = row_pair_base(r2) + s2 - row_col_start(r2);
-      const int p3 = row_pair_base(r3) + s3 - row_col_start(r3);
-      double v = (double)S.V[p3][p2][p1];
-      if (BLK != BK_WMM) {
-        const bool ress = S.ess[r3 + 2][r2 + 2][r1 + 2] != 0;
-        if (BLK == BK_A) {
-          const bool cess = S.ess[s3][s2][s1] != 0;
-          if (ress || cess) v = (pos == 0 && ress) ? 1.0 : 0.0;
-        } else if (ress) {
-          v = 0.0;
-        }
-      }
-      vals[base + j] = v;
-    }
+    const int a = c.clipped ? S.runoff[run] : (int)kTileTabs.runoff[run];
+    const int b = c.clipped ? S.runoff[run + 1] : (int)kTileTabs.runoff[run + 1];
+    if (b <= a) continue;
+    double* dst = vals + (int64_t)S.rowptr[r3][r2][0];
+    for (int j = lane; j < b - a; j += 32) dst[j] = (double)S.O[a + j];
   }
 }
 
@@ -441,7 +484,7 @@ __device__ __forceinline__ void tile_vectors(TileSmem<real>& S, const Lattice& L
                                              double* __restrict__ vparam,
                                              double* __restrict__ vadj, bool zero_ess) {
   real* U1 = &S.T1[0][0][0];  // 8 terms x [4][9][9]  (spans T1 and T2)
-  real* U2 = &S.V[0][0][0];   // 8 terms x [4][4][9]
+  real* U2 = &S.O[0];         // 8 terms x [4][4][9]
   const int tid = threadIdx.x;
   for (int task = tid; task < 8 * 81; task += blockDim.x) {
     const int term = task / 81, tt = task % 81;
@@ -491,32 +534,42 @@ template <typename real>
 __device__ __forceinline__ void tile_load(TileSmem<real>& S, const Lattice& L, TileCtx& c,
                                           const real* __restrict__ quad,
                                           const uint8_t* __restrict__ ess,
-                                          const int32_t* __restrict__ indptr, int ncomp) {
+                                          const int32_t* __restrict__ indptr) {
   const int tid = threadIdx.x;
   c.t1 = blockIdx.x; c.t2 = blockIdx.y; c.t3 = blockIdx.z;
+  const int tt[3] = {c.t1, c.t2, c.t3};
   const int eb[3] = {2 * c.t1 - 1, 2 * c.t2 - 1, 2 * c.t3 - 1};
   const int ne[3] = {L.nx, L.ny, L.nz};
+  const int Nn[3] = {L.Nx, L.Ny, L.Nz};
+  bool clipped = false;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     c.vl[d] = 0;
 #pragma unroll
     for (int l = 0; l < 3; ++l)
       if (eb[d] + l >= 0 && eb[d] + l < ne[d]) c.vl[d] |= 1 << l;
+    // the first tile clips row 0's stencil; the last holds the last node (clipped) and
+    // may hold rows outside the mesh
+    clipped |= tt[d] == 0 || 4 * tt[d] + 4 > Nn[d] - 1;
   }
-  const int per = ncomp * 27;
-  for (int i = tid; i < 27 * per; i += blockDim.x) {
-    const int l = i / per, f = i - l * per;
-    const int comp = f / 27, q = f - comp * 27;
-    const int l1 = l % 3, l2 = (l / 3) % 3, l3 = l / 9;
-    const int ex = eb[0] + l1, ey = eb[1] + l2, ez = eb[2] + l3;
-    real v = 0;
-    if (((c.vl[0] >> l1) & 1) && ((c.vl[1] >> l2) & 1) && ((c.vl[2] >> l3) & 1)) {
-      const int64_t e = ex + (int64_t)L.nx * (ey + (int64_t)L.ny * ez);
-      v = quad[e * 216 + f];
+  c.clipped = clipped;
+  // pointwise data: thread (component, point) walks the 27 halo'd elements
+  if (tid < 216) {
+    const int q = tid % 27, comp = tid / 27;
+    real* dst = &S.W[comp][q / 9][(q / 3) % 3][q % 3];
+    const int64_t sy = L.nx, sz = (int64_t)L.nx * L.ny;
+    const int64_t e0 = eb[0] + sy * eb[1] + sz * eb[2];
+    real v[27];
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+      const int l1 = l % 3, l2 = (l / 3) % 3, l3 = l / 9;
+      const bool in = ((c.vl[0] >> l1) & 1) && ((c.vl[1] >> l2) & 1) && ((c.vl[2] >> l3) & 1);
+      v[l] = in ? quad[(e0 + l1 + sy * l2 + sz * l3) * 216 + tid] : (real)0;
     }
-    const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
-    S.W[comp][3 * l3 + q3][3 * l2 + q2][3 * l1 + q1] = v;
+#pragma unroll
+    for (int l = 0; l < 27; ++l) dst[(3 * (l / 9)) * 81 + (3 * ((l / 3) % 3)) * 9 + 3 * (l % 3)] = v[l];
   }
+  int any = 0;
   for (int i = tid; i < 343; i += blockDim.x) {
     const int s1 = i % 7, s2 = (i / 7) % 7, s3 = i / 49;
     const int gx = 4 * c.t1 - 2 + s1, gy = 4 * c.t2 - 2 + s2, gz = 4 * c.t3 - 2 + s3;
@@ -524,6 +577,7 @@ __device__ __forceinline__ void tile_load(TileSmem<real>& S, const Lattice& L, T
     if (ess != nullptr && gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 && gz < L.Nz)
       m = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
     S.ess[s3][s2][s1] = m;
+    any |= m;
   }
   if (indptr != nullptr && tid < 64) {
     const int r1 = tid % 4, r2 = (tid / 4) % 4, r3 = tid / 16;
@@ -531,6 +585,35 @@ __device__ __forceinline__ void tile_load(TileSmem<real>& S, const Lattice& L, T
     int32_t v = 0;
     if (gx < L.Nx && gy < L.Ny && gz < L.Nz) v = indptr[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
     S.rowptr[r3][r2][r1] = v;
+  }
+  if (clipped && tid < 12) {
+    // per axis and owned row: clipped stencil size, low-end clip, own place
+    const int d = tid / 4, r = tid % 4;
+    const int g = 4 * tt[d] + r;
+    if (g < Nn[d]) {
+      const int lo = stencil_lo(g);
+      S.nst[d][r] = (int8_t)stencil_n(g, Nn[d]);
+      S.clip[d][r] = (int8_t)(lo - (4 * tt[d] - 2 + row_col_start(r)));
+      S.dk[d][r] = (int8_t)(g - lo);
+    } else {
+      S.nst[d][r] = 0; S.clip[d][r] = 0; S.dk[d][r] = 0;
+    }
+  }
+  c.has_ess = __syncthreads_or(any) != 0;
+  if (clipped && tid < 16) {
+    // O layout of a clipped tile: run r2 + 4 r3, rows r1 inside, clipped lengths
+    const int r2 = tid & 3, r3 = tid >> 2;
+    int off = 0;
+    for (int run = 0; run < tid; ++run) {
+      const int a2 = run & 3, a3 = run >> 2;
+      for (int r1 = 0; r1 < 4; ++r1) off += S.nst[0][r1] * S.nst[1][a2] * S.nst[2][a3];
+    }
+    S.runoff[tid] = off;
+    for (int r1 = 0; r1 < 4; ++r1) {
+      S.rowoff[r3][r2][r1] = off;
+      off += S.nst[0][r1] * S.nst[1][r2] * S.nst[2][r3];
+    }
+    if (tid == 15) S.runoff[16] = off;
   }
   __syncthreads();
 }
@@ -544,6 +627,9 @@ struct AssembleOut {
   int zero_ess;
 };
 
+// The fused assembly: one CTA per tile of 4 x 4 x 4 node rows, all pointwise data of
+// the 27 halo'd elements resident, the blocks one after the other, each streamed out
+// as soon as it is complete, then the vectors.
 template <typename real>
 __global__ void __launch_bounds__(256, 2)
     k_tile_assemble(Lattice L, const real* __restrict__ quad, const uint8_t* __restrict__ ess,
@@ -551,11 +637,11 @@ __global__ void __launch_bounds__(256, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TileSmem<real>& S = *reinterpret_cast<TileSmem<real>*>(smem_raw);
   TileCtx c;
-  tile_load(S, L, c, quad, ess, indptr, 8);
-  if (o.vals[BK_A]) { tile_block<BK_A>(S, L); tile_write<BK_A>(S, L, c, o.vals[BK_A]); }
-  if (o.vals[BK_C]) { tile_block<BK_C>(S, L); tile_write<BK_C>(S, L, c, o.vals[BK_C]); }
-  if (o.vals[BK_WUM]) { tile_block<BK_WUM>(S, L); tile_write<BK_WUM>(S, L, c, o.vals[BK_WUM]); }
-  if (o.vals[BK_WMM]) { tile_block<BK_WMM>(S, L); tile_write<BK_WMM>(S, L, c, o.vals[BK_WMM]); }
+  tile_load(S, L, c, quad, ess, indptr);
+  if (o.vals[BK_A]) { tile_block<BK_A>(S, L, c); tile_write(S, c, o.vals[BK_A]); }
+  if (o.vals[BK_C]) { tile_block<BK_C>(S, L, c); tile_write(S, c, o.vals[BK_C]); }
+  if (o.vals[BK_WUM]) { tile_block<BK_WUM>(S, L, c); tile_write(S, c, o.vals[BK_WUM]); }
+  if (o.vals[BK_WMM]) { tile_block<BK_WMM>(S, L, c); tile_write(S, c, o.vals[BK_WMM]); }
   if (o.vec_state || o.vec_param || o.vec_adj) {
     __syncthreads();
     tile_vectors(S, L, c, o.f, o.vec_state, o.vec_param, o.vec_adj, o.zero_ess != 0);
