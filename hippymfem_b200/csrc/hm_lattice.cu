@@ -226,12 +226,23 @@ HM_HD constexpr TileTabs make_tile_tabs() {
 }
 __device__ const TileTabs kTileTabs = make_tile_tabs();
 
+// Strides of the stage buffers: the p3 stride is 9 (mod 16) doubles, so the 16 lanes of
+// a half-warp (9 consecutive g1 of one p3 and 7 of the next, or 16 p2 of one p3) hit 16
+// distinct 8-byte bank pairs.
+constexpr int kT1P = 89;    // T1[p3 * kT1P + g2 * 9 + g1]
+constexpr int kT2P = 153;   // T2[p3 * kT2P + p2 * 9 + g1]
+
+// O is swizzled: position j lives at j ^ ((j >> 4) & 15), a permutation inside each
+// aligned group of 16, so the contiguous copy-out stays conflict-free and the scattered
+// stage-3 stores spread over the banks.
+HM_HD int oswz(int j) { return j ^ ((j >> 4) & 15); }
+
 template <typename real>
 struct TileSmem {
   real W[8][9][9][9];      // pointwise data of the 27 halo'd elements on the 9^3 Gauss lattice
-  real T1[16][9][9];       // after the z contraction: [p3][g2][g1]
-  real T2[16][16][9];      // after the y contraction: [p3][p2][g1]
-  real O[4096];            // the tile's rows of one block, CSR-ordered (run-major)
+  real T1[16 * kT1P];      // after the z contraction
+  real T2[16 * kT2P];      // after the y contraction
+  real O[4096];            // the tile's rows of one block, CSR-ordered (run-major), swizzled
   int32_t rowptr[4][4][4]; // CSR offsets of the owned rows [r3][r2][r1]
   int32_t rowoff[4][4][4]; // offsets of the rows in O (tiles with clipped stencils)
   int32_t runoff[17];      // offsets of the runs in O
@@ -248,9 +259,12 @@ struct TileCtx {
   bool has_ess;        // some halo'd node is a Dirichlet node
 };
 
-// stage 1: contract the z axis of one weight with table TZ -> T1[p3][g2][g1]
+// The stages are instantiated once per 1D table and not inlined: the blocks share
+// them, which keeps the kernel's code small enough for the instruction cache.
+
+// stage 1: contract the z axis of one weight with table TZ -> T1
 template <int TZ, typename real>
-__device__ __forceinline__ void stage1(const real* __restrict__ Wc, real* __restrict__ T1) {
+__device__ __noinline__ void stage1(const real* __restrict__ Wc, real* __restrict__ T1) {
   for (int task = threadIdx.x; task < 81; task += blockDim.x) {
     const int g1 = task % 9, g2 = task / 9;
     real w[9];
@@ -262,94 +276,107 @@ __device__ __forceinline__ void stage1(const real* __restrict__ Wc, real* __rest
 #pragma unroll
       for (int t = 0; t < 6; ++t)
         if (t < pair_cnt(p)) acc = fma((real)pair_coef(TZ, p, t), w[pair_g0(p) + t], acc);
-      T1[(p * 9 + g2) * 9 + g1] = acc;
+      T1[p * kT1P + g2 * 9 + g1] = acc;
     }
   }
 }
 
-// stage 2: contract the y axis with table TY -> T2[p3][p2][g1] (= or +=) scale * ...
-template <int TY, bool ACC, typename real>
-__device__ __forceinline__ void stage2(const real* __restrict__ T1, real* __restrict__ T2,
-                                       real scale) {
+// stage 2: contract the y axis with table TY -> T2 = scale * ... (+ T2 when acc)
+template <int TY, typename real>
+__device__ __noinline__ void stage2(const real* __restrict__ T1, real* __restrict__ T2, real scale,
+                                    bool acc_in) {
   for (int task = threadIdx.x; task < 144; task += blockDim.x) {
     const int g1 = task % 9, p3 = task / 9;
     real w[9];
 #pragma unroll
-    for (int l = 0; l < 9; ++l) w[l] = T1[(p3 * 9 + l) * 9 + g1];
+    for (int l = 0; l < 9; ++l) w[l] = T1[p3 * kT1P + l * 9 + g1];
+    real* out = T2 + p3 * kT2P + g1;
 #pragma unroll
     for (int p = 0; p < 16; ++p) {
       real acc = 0;
 #pragma unroll
       for (int t = 0; t < 6; ++t)
         if (t < pair_cnt(p)) acc = fma((real)pair_coef(TY, p, t), w[pair_g0(p) + t], acc);
-      const int idx = (p3 * 16 + p) * 9 + g1;
-      T2[idx] = ACC ? fma(scale, acc, T2[idx]) : scale * acc;
+      out[p * 9] = acc_in ? fma(scale, acc, out[p * 9]) : scale * acc;
     }
   }
 }
 
 enum BlockKind { BK_A = 0, BK_C = 1, BK_WUM = 2, BK_WMM = 3 };
+// elimination applied by the last stage 3 of a block
+enum Elim { EL_NONE = 0, EL_ROWCOL_DIAG = 1, EL_ROW = 2 };
 
-// Place of output (p1, p2, p3) in O for a tile with clipped stencils; -1 if its column
-// lies outside the mesh (or its row does).
+// Places of outputs (p1 = 0..15, p2, p3) in O for a tile with clipped stencils; -1 if
+// the column lies outside the mesh (or the row does).
 template <typename real>
-__device__ __forceinline__ int clipped_pos(const TileSmem<real>& S, int p1, int p2, int p3) {
-  const int r1 = pair_row_of(p1), r2 = pair_row_of(p2), r3 = pair_row_of(p3);
-  const int n1 = S.nst[0][r1], n2 = S.nst[1][r2], n3 = S.nst[2][r3];
-  if (n1 == 0 || n2 == 0 || n3 == 0) return -1;
-  const int k1 = p1 - row_pair_base(r1) - S.clip[0][r1];
+__device__ __noinline__ void clipped_positions(const TileSmem<real>& S, int p2, int p3, int* pos) {
+  const int r2 = pair_row_of(p2), r3 = pair_row_of(p3);
+  const int n2 = S.nst[1][r2], n3 = S.nst[2][r3];
   const int k2 = p2 - row_pair_base(r2) - S.clip[1][r2];
   const int k3 = p3 - row_pair_base(r3) - S.clip[2][r3];
-  if (k1 < 0 || k1 >= n1 || k2 < 0 || k2 >= n2 || k3 < 0 || k3 >= n3) return -1;
-  const int rank = (k3 * n2 + k2) * n1 + k1;
-  const int kd = (S.dk[2][r3] * n2 + S.dk[1][r2]) * n1 + S.dk[0][r1];
-  const int pos = rank == kd ? 0 : (rank < kd ? rank + 1 : rank);
-  return S.rowoff[r3][r2][r1] + pos;
+  const bool ok23 = n2 > 0 && n3 > 0 && k2 >= 0 && k2 < n2 && k3 >= 0 && k3 < n3;
+#pragma unroll 1
+  for (int p1 = 0; p1 < 16; ++p1) {
+    const int r1 = pair_row_of(p1);
+    const int n1 = S.nst[0][r1];
+    const int k1 = p1 - row_pair_base(r1) - S.clip[0][r1];
+    if (!ok23 || n1 == 0 || k1 < 0 || k1 >= n1) { pos[p1] = -1; continue; }
+    const int rank = (k3 * n2 + k2) * n1 + k1;
+    const int kd = (S.dk[2][r3] * n2 + S.dk[1][r2]) * n1 + S.dk[0][r1];
+    pos[p1] = S.rowoff[r3][r2][r1] + (rank == kd ? 0 : (rank < kd ? rank + 1 : rank));
+  }
 }
 
 // stage 3: contract the x axis with table TX and scatter into the CSR-ordered tile
-// output O (= or +=); the last group of a block applies its folded elimination:
-// A rows and columns of Dirichlet nodes zeroed with a unit diagonal, C and Wum rows
-// zeroed, Wmm untouched.
-template <int TX, bool ACC, int BLK, bool FINAL, typename real>
-__device__ __forceinline__ void stage3(TileSmem<real>& S, const TileCtx& c) {
-  const real* __restrict__ T2 = &S.T2[0][0][0];
+// output O (= or +=); with elim the block's folded elimination is applied:
+// EL_ROWCOL_DIAG (A) zeroes rows and columns of Dirichlet nodes and puts 1 on their
+// diagonal, EL_ROW (C, Wum) zeroes their rows.
+template <int TX, typename real>
+__device__ __forceinline__ void stage3_out(TileSmem<real>& S, const TileCtx& c, const real (&w)[9],
+                                           int p2, int p3, int p, int at, bool acc_in, int elim,
+                                           bool check) {
+  real acc = 0;
+#pragma unroll
+  for (int t = 0; t < 6; ++t)
+    if (t < pair_cnt(p)) acc = fma((real)pair_coef(TX, p, t), w[pair_g0(p) + t], acc);
+  if (at < 0) return;
+  at = oswz(at);
+  real v = acc_in ? S.O[at] + acc : acc;
+  if (check) {
+    const int r2 = pair_row_of(p2), r3 = pair_row_of(p3);
+    const bool ress = S.ess[r3 + 2][r2 + 2][pair_row_of(p) + 2] != 0;
+    if (elim == EL_ROWCOL_DIAG) {
+      const bool cess = S.ess[pair_c(p3)][pair_c(p2)][pair_c(p)] != 0;
+      const bool diag = pair_s(p2) == pair_c(p2) && pair_s(p3) == pair_c(p3) && pair_s(p) == pair_c(p);
+      if (ress || cess) v = (ress && diag) ? (real)1 : (real)0;
+    } else if (ress) {
+      v = 0;
+    }
+  }
+  S.O[at] = v;
+}
+
+template <int TX, typename real>
+__device__ __noinline__ void stage3(TileSmem<real>& S, const TileCtx& c, bool acc_in, int elim) {
+  const bool check = elim != EL_NONE && c.has_ess;
   for (int task = threadIdx.x; task < 256; task += blockDim.x) {
     const int p2 = task % 16, p3 = task / 16;
     real w[9];
 #pragma unroll
-    for (int l = 0; l < 9; ++l) w[l] = T2[(p3 * 16 + p2) * 9 + l];
-    uint16_t pos[16];
+    for (int l = 0; l < 9; ++l) w[l] = S.T2[p3 * kT2P + p2 * 9 + l];
     if (!c.clipped) {
       const uint4* src = reinterpret_cast<const uint4*>(&kTileTabs.inv[p3][p2][0]);
       const uint4 a = __ldg(src), b = __ldg(src + 1);
       const uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-      for (int i = 0; i < 8; ++i) { pos[2 * i] = wv[i] & 0xffffu; pos[2 * i + 1] = wv[i] >> 16; }
-    }
-    const bool check = FINAL && BLK != BK_WMM && c.has_ess;
-    const int r2 = pair_row_of(p2), r3 = pair_row_of(p3);
-    const int c2 = pair_c(p2), c3 = pair_c(p3);
-    const bool diag23 = pair_s(p2) == c2 && pair_s(p3) == c3;
+      for (int p = 0; p < 16; ++p)
+        stage3_out<TX>(S, c, w, p2, p3, p, (int)((wv[p >> 1] >> (16 * (p & 1))) & 0xffffu), acc_in,
+                       elim, check);
+    } else {
+      int pos[16];
+      clipped_positions(S, p2, p3, pos);
 #pragma unroll
-    for (int p = 0; p < 16; ++p) {
-      real acc = 0;
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (t < pair_cnt(p)) acc = fma((real)pair_coef(TX, p, t), w[pair_g0(p) + t], acc);
-      const int at = c.clipped ? clipped_pos(S, p, p2, p3) : (int)pos[p];
-      if (at < 0) continue;
-      real v = ACC ? S.O[at] + acc : acc;
-      if (check) {
-        const bool ress = S.ess[r3 + 2][r2 + 2][pair_row_of(p) + 2] != 0;
-        if (BLK == BK_A) {
-          const bool cess = S.ess[c3][c2][pair_c(p)] != 0;
-          if (ress || cess) v = (ress && diag23 && pair_s(p) == pair_c(p)) ? (real)1 : (real)0;
-        } else if (ress) {
-          v = 0;
-        }
-      }
-      S.O[at] = v;
+      for (int p = 0; p < 16; ++p) stage3_out<TX>(S, c, w, p2, p3, p, pos[p], acc_in, elim, check);
     }
   }
 }
@@ -361,37 +388,38 @@ __device__ __forceinline__ void stage3(TileSmem<real>& S, const TileCtx& c) {
 //   Wum = C with F in place of E
 //   Wmm = M.M.M (W)
 // (tables as x.y.z; the weights carry w|J| and the physical gradients)
-template <int BLK, typename real>
-__device__ __forceinline__ void tile_block(TileSmem<real>& S, const Lattice& L, const TileCtx& c) {
-  real* T1 = &S.T1[0][0][0];
-  real* T2 = &S.T2[0][0][0];
-  if (BLK == BK_A) {
+template <typename real>
+__device__ __forceinline__ void tile_block(int blk, TileSmem<real>& S, const Lattice& L,
+                                           const TileCtx& c) {
+  real* T1 = S.T1;
+  real* T2 = S.T2;
+  if (blk == BK_A) {
     const real* D = &S.W[0][0][0][0];
     stage1<TM>(D, T1); __syncthreads();
-    stage2<TM, false>(T1, T2, (real)(1.0 / (L.hx * L.hx))); __syncthreads();
-    stage3<TK, false, BLK, false>(S, c); __syncthreads();
-    stage2<TK, false>(T1, T2, (real)(1.0 / (L.hy * L.hy))); __syncthreads();
+    stage2<TM>(T1, T2, (real)(1.0 / (L.hx * L.hx)), false); __syncthreads();
+    stage3<TK>(S, c, false, EL_NONE); __syncthreads();
+    stage2<TK>(T1, T2, (real)(1.0 / (L.hy * L.hy)), false); __syncthreads();
     stage1<TK>(D, T1); __syncthreads();
-    stage2<TM, true>(T1, T2, (real)(1.0 / (L.hz * L.hz))); __syncthreads();
-    stage3<TM, true, BLK, true>(S, c); __syncthreads();
-  } else if (BLK == BK_C || BLK == BK_WUM) {
-    const int c0 = BLK == BK_C ? 1 : 4;
+    stage2<TM>(T1, T2, (real)(1.0 / (L.hz * L.hz)), true); __syncthreads();
+    stage3<TM>(S, c, true, EL_ROWCOL_DIAG); __syncthreads();
+  } else if (blk == BK_C || blk == BK_WUM) {
+    const int c0 = blk == BK_C ? 1 : 4;
     const real* Gx = &S.W[c0][0][0][0];
     const real* Gy = &S.W[c0 + 1][0][0][0];
     const real* Gz = &S.W[c0 + 2][0][0][0];
     stage1<TM>(Gx, T1); __syncthreads();
-    stage2<TM, false>(T1, T2, (real)(1.0 / L.hx)); __syncthreads();
-    stage3<TR, false, BLK, false>(S, c); __syncthreads();
+    stage2<TM>(T1, T2, (real)(1.0 / L.hx), false); __syncthreads();
+    stage3<TR>(S, c, false, EL_NONE); __syncthreads();
     stage1<TM>(Gy, T1); __syncthreads();
-    stage2<TR, false>(T1, T2, (real)(1.0 / L.hy)); __syncthreads();
+    stage2<TR>(T1, T2, (real)(1.0 / L.hy), false); __syncthreads();
     stage1<TR>(Gz, T1); __syncthreads();
-    stage2<TM, true>(T1, T2, (real)(1.0 / L.hz)); __syncthreads();
-    stage3<TM, true, BLK, true>(S, c); __syncthreads();
+    stage2<TM>(T1, T2, (real)(1.0 / L.hz), true); __syncthreads();
+    stage3<TM>(S, c, true, EL_ROW); __syncthreads();
   } else {
     const real* Wq = &S.W[7][0][0][0];
     stage1<TM>(Wq, T1); __syncthreads();
-    stage2<TM, false>(T1, T2, (real)1.0); __syncthreads();
-    stage3<TM, false, BLK, true>(S, c); __syncthreads();
+    stage2<TM>(T1, T2, (real)1.0, false); __syncthreads();
+    stage3<TM>(S, c, false, EL_NONE); __syncthreads();
   }
 }
 
@@ -409,7 +437,7 @@ __device__ __forceinline__ void tile_write(const TileSmem<real>& S, const TileCt
     const int b = c.clipped ? S.runoff[run + 1] : (int)kTileTabs.runoff[run + 1];
     if (b <= a) continue;
     double* dst = vals + (int64_t)S.rowptr[r3][r2][0];
-    for (int j = lane; j < b - a; j += 32) dst[j] = (double)S.O[a + j];
+    for (int j = lane; j < b - a; j += 32) dst[j] = (double)S.O[oswz(a + j)];
   }
 }
 
@@ -483,7 +511,7 @@ __device__ __forceinline__ void tile_vectors(TileSmem<real>& S, const Lattice& L
                                              double f, double* __restrict__ vstate,
                                              double* __restrict__ vparam,
                                              double* __restrict__ vadj, bool zero_ess) {
-  real* U1 = &S.T1[0][0][0];  // 8 terms x [4][9][9]  (spans T1 and T2)
+  real* U1 = S.T1;            // 8 terms x [4][9][9]  (spans T1 and T2)
   real* U2 = &S.O[0];         // 8 terms x [4][4][9]
   const int tid = threadIdx.x;
   for (int task = tid; task < 8 * 81; task += blockDim.x) {
@@ -638,10 +666,12 @@ __global__ void __launch_bounds__(256, 2)
   TileSmem<real>& S = *reinterpret_cast<TileSmem<real>*>(smem_raw);
   TileCtx c;
   tile_load(S, L, c, quad, ess, indptr);
-  if (o.vals[BK_A]) { tile_block<BK_A>(S, L, c); tile_write(S, c, o.vals[BK_A]); }
-  if (o.vals[BK_C]) { tile_block<BK_C>(S, L, c); tile_write(S, c, o.vals[BK_C]); }
-  if (o.vals[BK_WUM]) { tile_block<BK_WUM>(S, L, c); tile_write(S, c, o.vals[BK_WUM]); }
-  if (o.vals[BK_WMM]) { tile_block<BK_WMM>(S, L, c); tile_write(S, c, o.vals[BK_WMM]); }
+#pragma unroll 1
+  for (int blk = 0; blk < 4; ++blk) {
+    if (o.vals[blk] == nullptr) continue;
+    tile_block(blk, S, L, c);
+    tile_write(S, c, o.vals[blk]);
+  }
   if (o.vec_state || o.vec_param || o.vec_adj) {
     __syncthreads();
     tile_vectors(S, L, c, o.f, o.vec_state, o.vec_param, o.vec_adj, o.zero_ess != 0);
