@@ -29,7 +29,7 @@ _EXC = {HM_ERR_ARG: ValueError, HM_ERR_CUDA: RuntimeError, HM_ERR_NONFINITE: Run
 
 if not os.path.exists(LIBPATH):
     raise ImportError("libhippymfem_b200.so is not built (%s); run "
-                      "`python -m hippymfem_b200.build`" % LIBPATH)
+                      "`python hippymfem_b200/build.py`" % LIBPATH)
 
 lib = ctypes.CDLL(LIBPATH)
 
@@ -63,7 +63,11 @@ SIGNATURES = {
 }
 
 for _name, (_res, _args) in SIGNATURES.items():
-    _f = getattr(lib, _name)
+    try:
+        _f = getattr(lib, _name)
+    except AttributeError as exc:
+        raise ImportError("libhippymfem_b200.so lacks %s: it is older than its sources; run "
+                          "`python hippymfem_b200/build.py`" % _name) from exc
     _f.restype = _res
     _f.argtypes = _args
 

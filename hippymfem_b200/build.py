@@ -1,8 +1,10 @@
 """Build ``libhippymfem_b200.so`` in-tree with nvcc for sm_100a.
 
-    python -m hippymfem_b200.build            # build if a source is newer than the .so
-    python -m hippymfem_b200.build --force    # rebuild
-    python -m hippymfem_b200.build --ptxas    # also print registers / spills / smem
+    python hippymfem_b200/build.py            # build if a source is newer than the .so
+    python hippymfem_b200/build.py --force    # rebuild
+    python hippymfem_b200/build.py --ptxas    # also print registers / spills / smem
+
+(Run as a script: importing the package would load the library being rebuilt.)
 
 Objects go to ``hippymfem_b200/_build`` (git-ignored); the library lands next to this
 file so that it travels with the source tree.
