@@ -13,6 +13,8 @@ namespace {
 inline bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
 }  // namespace
 
+const hm::Lattice* hm_lattice_geometry(const hm_lattice* h) { return &h->L; }
+
 extern "C" const char* hm_error_string(int code) {
   switch (code) {
     case HM_OK: return "ok";

@@ -9,6 +9,9 @@ namespace hm {
 struct Lattice;
 }
 
+// the geometry behind a lattice handle
+const hm::Lattice* hm_lattice_geometry(const hm_lattice* h);
+
 int hm_launch_pattern(const hm::Lattice& L, int32_t* indptr, int32_t* indices, int32_t* slot,
                       void* stream);
 int hm_launch_tpos(const hm::Lattice& L, const int32_t* indptr, int32_t* tpos, void* stream);

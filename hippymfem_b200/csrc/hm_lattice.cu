@@ -992,3 +992,58 @@ int hm_launch_diag_A(const Lattice& L, const void* quad, int precision, const ui
     k_diag_A<double><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, (const double*)quad, ess, diag);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
+
+// ================================================== allocation-free residual / gradient
+// A caller that cannot allocate device memory when it needs a residual or a gradient
+// (a process whose GPU memory another runtime's pool has already claimed -- JAX/XLA
+// preallocates most of the device by default, hypre/MFEM may sit on an Umpire pool --
+// or a loop that must not pay for an allocation) gets the assembled vectors through
+// hm_lattice_residual_noalloc.  Its one scratch buffer, the pointwise data of the
+// lattice's elements, is this fixed array: every GPU that loads the library holds it
+// (HM_NOALLOC_MAX_ELEMENTS * 216 doubles, 14.2 MB) until the process exits.
+#define HM_NOALLOC_MAX_ELEMENTS 8192
+static __device__ __align__(256) double g_noalloc_quad[HM_NOALLOC_MAX_ELEMENTS * 216];
+
+#include <mutex>
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[64] = {nullptr};  // device address of g_noalloc_quad, per device
+}  // namespace
+
+// The device address of the scratch array on the current device, looked up once per
+// device (the array's name is only a host-side stand-in for it).
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return HM_ERR_CUDA;
+  if (dev < 0 || dev >= 64) return HM_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_quad) != cudaSuccess || ptr == nullptr) return HM_ERR_CUDA;
+    g_noalloc_addr[dev] = ptr;
+  }
+  *out = g_noalloc_addr[dev];
+  return HM_OK;
+}
+
+extern "C" int hm_lattice_residual_noalloc(const hm_lattice* h, const double* d_u, const double* d_m,
+                                           const double* d_p, double f, const uint8_t* d_ess,
+                                           double* d_vec_state, double* d_vec_param,
+                                           double* d_vec_adjoint, int zero_ess_vectors,
+                                           uint32_t* d_status, void* stream) {
+  if (!h || !d_u || !d_m || !d_p || !d_status) return HM_ERR_ARG;
+  if (!d_vec_state && !d_vec_param && !d_vec_adjoint) return HM_ERR_ARG;
+  const hm::Lattice& L = *hm_lattice_geometry(h);
+  if (L.ne > HM_NOALLOC_MAX_ELEMENTS) return HM_ERR_NOMEM;
+  void* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  // k_quad overwrites the scratch for every element before the assembly reads it, so
+  // nothing is carried over from the previous call
+  rc = hm_launch_quad(L, d_u, d_m, d_p, HM_FP64, scratch, d_status, stream);
+  if (rc) return rc;
+  return hm_launch_assemble(L, scratch, HM_FP64, nullptr, d_ess, f, nullptr, nullptr, nullptr,
+                            nullptr, d_vec_state, d_vec_param, d_vec_adjoint, zero_ess_vectors,
+                            stream);
+}

@@ -133,6 +133,28 @@ int hm_lattice_apply_A(const hm_lattice* h, const void* d_quad, int precision,
 int hm_lattice_diag_A(const hm_lattice* h, const void* d_quad, int precision,
                       const uint8_t* d_ess, double* d_diag, void* stream);
 
+/* The assembled vectors of hm_lattice_assemble (dR/du, dR/dm, dR/dp; any may be NULL,
+ * not all) without any device allocation, for callers that cannot allocate when they
+ * need them: a process whose GPU memory another runtime's pool already holds (JAX/XLA
+ * preallocates most of the device by default; MFEM/hypre may run on an Umpire pool),
+ * or a loop that must not pay for an allocation.  This entry point has no counterpart
+ * in the reference.  Its scratch (the pointwise data of the elements) is a fixed
+ * device array inside the library, so:
+ *   - the lattice must have at most 8192 elements (e.g. 20^3); a larger one returns
+ *     HM_ERR_NOMEM and launches nothing;
+ *   - every GPU that loads the library holds those 14.2 MB until the process exits;
+ *   - the first call on a device looks the array's address up for that device (with
+ *     the device current): make that first call before any stream capture;
+ *   - all calls share the array: calls that overlap on the GPU (other streams, other
+ *     threads) race and give wrong results; calls in one stream are ordered and safe.
+ *     Nothing has to be cleared between calls: each call overwrites the scratch it
+ *     reads.  *d_status is OR-ed as by hm_lattice_quadrature. */
+int hm_lattice_residual_noalloc(const hm_lattice* h, const double* d_u, const double* d_m,
+                                const double* d_p, double f, const uint8_t* d_ess,
+                                double* d_vec_state, double* d_vec_param,
+                                double* d_vec_adjoint, int zero_ess_vectors,
+                                uint32_t* d_status, void* stream);
+
 /* ----------------------------------------------------------------- sparse / solve
  * y = alpha * M x + beta * y for a CSR block (hypre's Mult, apply_ij). */
 int hm_csr_spmv(int64_t nrow, const int32_t* d_indptr, const int32_t* d_indices,
