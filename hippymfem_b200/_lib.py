@@ -51,6 +51,8 @@ SIGNATURES = {
     "hm_lattice_assemble": (_i32, [_p, _p, _i32, _p, _p, _d, _p, _p, _p, _p, _p, _p, _p, _i32,
                                    _p]),
     "hm_lattice_residual_noalloc": (_i32, [_p, _p, _p, _p, _d, _p, _p, _p, _p, _i32, _p, _p]),
+    "hm_lattice_jacobian_bytes": (_i64, [_p, _i32]),
+    "hm_lattice_jacobian_prepare": (_i32, [_p, _p, _i32, _p, _p]),
     "hm_lattice_apply_A": (_i32, [_p, _p, _i32, _p, _p, _p, _p]),
     "hm_lattice_diag_A": (_i32, [_p, _p, _i32, _p, _p, _p]),
     "hm_csr_spmv": (_i32, [_i64, _p, _p, _p, _p, _p, _d, _d, _p]),

@@ -100,11 +100,23 @@ extern "C" int hm_lattice_assemble(const hm_lattice* h, const void* quad, int pr
                             zero_ess, stream);
 }
 
-extern "C" int hm_lattice_apply_A(const hm_lattice* h, const void* quad, int precision,
-                                  const uint8_t* ess, const double* x, double* y, void* stream) {
-  if (!h || !quad || !x || !y || x == y) return HM_ERR_ARG;
+extern "C" int64_t hm_lattice_jacobian_bytes(const hm_lattice* h, int precision) {
+  if (!h) return 0;
+  return 2 * 27 * h->L.ne * (precision == HM_FP32 ? 4 : 8);
+}
+
+extern "C" int hm_lattice_jacobian_prepare(const hm_lattice* h, const void* quad, int precision,
+                                           void* jac, void* stream) {
+  if (!h || !quad || !jac) return HM_ERR_ARG;
   if (precision != HM_FP64 && precision != HM_FP32) return HM_ERR_ARG;
-  return hm_launch_apply_A(h->L, quad, precision, ess, x, y, stream);
+  return hm_launch_jacobian_prepare(h->L, quad, precision, jac, stream);
+}
+
+extern "C" int hm_lattice_apply_A(const hm_lattice* h, void* jac, int precision,
+                                  const uint8_t* ess, const double* x, double* y, void* stream) {
+  if (!h || !jac || !x || !y || x == y) return HM_ERR_ARG;
+  if (precision != HM_FP64 && precision != HM_FP32) return HM_ERR_ARG;
+  return hm_launch_apply_A(h->L, jac, precision, ess, x, y, stream);
 }
 
 extern "C" int hm_lattice_diag_A(const hm_lattice* h, const void* quad, int precision,
@@ -118,7 +130,7 @@ extern "C" int hm_lattice_diag_A(const hm_lattice* h, const void* quad, int prec
 int hm_pcg_operator(int64_t n, const int32_t* indptr, const int32_t* indices, const double* vals,
                     const hm::Lattice* L, const void* quad, int precision, const uint8_t* ess,
                     const double* x, double* y, void* stream) {
-  if (L) return hm_launch_apply_A(*L, quad, precision, ess, x, y, stream);
+  if (L) return hm_launch_apply_A(*L, const_cast<void*>(quad), precision, ess, x, y, stream);
   return hm_csr_spmv(n, indptr, indices, vals, x, y, 1.0, 0.0, stream);
 }
 

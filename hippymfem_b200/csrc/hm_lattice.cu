@@ -679,182 +679,193 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // ====================================================== matrix-free Jacobian apply
-// y = A(D) x on the tile's owned rows: gradients of x at the 9^3 local Gauss points
-// (node lattice -> Gauss lattice, one axis at a time), flux D grad x / h^2, and back
-// to the owned rows with the single-index tables.  x is zeroed on Dirichlet nodes,
-// and y = x there (the Jacobian's elimination).
-template <typename real>
-struct ApplySmem {
-  real x[7][7][7];        // [s3][s2][s1]
-  real D[9][9][9];        // [g3][g2][g1]
-  real Xb[9][7][7];       // [g3][s2][s1]  z interpolated
-  real Xd[9][7][7];       //               z derivative
-  real Y[3][9][9][7];     // [bb, db, bd][g3][g2][s1]
-  real G[3][9][9][9];     // flux [d][g3][g2][g1]
-  real Z[3][9][9][4];     // [term][g3][g2][r1]
-  real U[2][9][4][4];     // [B, D][g3][r2][r1]
-  uint8_t ess[7][7][7];
-};
+// y = A(D) x in two deterministic passes:
+//   k_elem_apply   three threads per element, thread t owning Gauss slice q3 = t:
+//                  x at the element's nodes -> gradients at the slice's 9 points (sum
+//                  factorisation in registers) -> flux D grad x / h^2 -> back to the
+//                  element's nodes; the three slices' contributions are combined with
+//                  warp shuffles and y_e written in SoA layout Ye[a][e]
+//   k_node_gather  one thread per node: the sum of its <= 8 element contributions in a
+//                  fixed order; y = x on Dirichlet nodes (the Jacobian's elimination,
+//                  x zeroed there on input)
+// D is kept in SoA layout Dq[q][e] (hm_lattice_jacobian_prepare), so both passes read
+// and write coalesced.
 
 template <typename real>
-__global__ void __launch_bounds__(256)
-    k_tile_apply_A(Lattice L, const real* __restrict__ quad, const uint8_t* __restrict__ ess,
-                   const double* __restrict__ xin, double* __restrict__ yout) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ApplySmem<real>& S = *reinterpret_cast<ApplySmem<real>*>(smem_raw);
-  const int tid = threadIdx.x;
-  const int t1 = blockIdx.x, t2 = blockIdx.y, t3 = blockIdx.z;
-  const int eb1 = 2 * t1 - 1, eb2 = 2 * t2 - 1, eb3 = 2 * t3 - 1;
-  for (int i = tid; i < 343; i += blockDim.x) {
-    const int s1 = i % 7, s2 = (i / 7) % 7, s3 = i / 49;
-    const int gx = 4 * t1 - 2 + s1, gy = 4 * t2 - 2 + s2, gz = 4 * t3 - 2 + s3;
-    real v = 0;
-    uint8_t m = 0;
-    if (gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 && gz < L.Nz) {
-      const int64_t n = gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz);
-      m = ess != nullptr ? ess[n] : 0;
-      v = m ? (real)0 : (real)xin[n];
-    }
-    S.x[s3][s2][s1] = v;
-    S.ess[s3][s2][s1] = m;
-  }
-  for (int i = tid; i < 27 * 27; i += blockDim.x) {
-    const int l = i / 27, q = i % 27;
-    const int l1 = l % 3, l2 = (l / 3) % 3, l3 = l / 9;
-    const int ex = eb1 + l1, ey = eb2 + l2, ez = eb3 + l3;
-    real v = 0;
-    if (ex >= 0 && ex < L.nx && ey >= 0 && ey < L.ny && ez >= 0 && ez < L.nz)
-      v = quad[(ex + (int64_t)L.nx * (ey + (int64_t)L.ny * ez)) * 216 + q];
-    S.D[3 * l3 + q / 9][3 * l2 + (q / 3) % 3][3 * l1 + q % 3] = v;
-  }
-  __syncthreads();
-  // z: nodes -> Gauss points
-  for (int task = tid; task < 49; task += blockDim.x) {
-    const int s1 = task % 7, s2 = task / 7;
-    real xs[7];
+__global__ void k_extract_D(Lattice L, const real* __restrict__ quad, real* __restrict__ Dq) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= L.ne * 27) return;
+  const int64_t e = i / 27;
+  const int q = (int)(i - e * 27);
+  Dq[(int64_t)q * L.ne + e] = quad[e * 216 + q];
+}
+
+// B(q, a) and B'(q, a) for a run-time point index q (a compile-time)
+template <typename real>
+__device__ __forceinline__ real bq_rt(int q, int a) {
+  return q == 0 ? (real)bq(0, a) : q == 1 ? (real)bq(1, a) : (real)bq(2, a);
+}
+template <typename real>
+__device__ __forceinline__ real dbq_rt(int q, int a) {
+  return q == 0 ? (real)dbq(0, a) : q == 1 ? (real)dbq(1, a) : (real)dbq(2, a);
+}
+
+template <typename real>
+__global__ void __launch_bounds__(256, 2)
+    k_elem_apply(Lattice L, const real* __restrict__ Dq, const uint8_t* __restrict__ ess,
+                 const double* __restrict__ xin, real* __restrict__ Ye) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int k = lane / 3, t = lane - 3 * k;                 // element slot, Gauss slice
+  const int64_t e = warp * 10 + k;
+  const bool live = lane < 30 && e < L.ne;
+  // 32-bit decode (the lattice keeps every index below 2^31)
+  const unsigned ec = live ? (unsigned)e : 0u;
+  const unsigned exy = ec / (unsigned)L.nx;
+  const int ex = (int)(ec - exy * (unsigned)L.nx);
+  const int ez = (int)(exy / (unsigned)L.ny), ey = (int)(exy - (unsigned)ez * (unsigned)L.ny);
+  const unsigned n0 = (unsigned)(2 * ex) + (unsigned)L.Nx * ((unsigned)(2 * ey) + (unsigned)L.Ny * (unsigned)(2 * ez));
+  const unsigned nsy = (unsigned)L.Nx, nsz = (unsigned)L.Nx * (unsigned)L.Ny;
+  // z interpolation onto slice t, one node plane a3 at a time: Xb[a2][a1], Xd[a2][a1]
+  real Xb[9], Xd[9];
 #pragma unroll
-    for (int s = 0; s < 7; ++s) xs[s] = S.x[s][s2][s1];
+  for (int a3 = 0; a3 < 3; ++a3) {
+    const real b3 = bq_rt<real>(t, a3), d3 = dbq_rt<real>(t, a3);
 #pragma unroll
-    for (int g = 0; g < 9; ++g) {
-      real vb = 0, vd = 0;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        vb = fma((real)bq(g % 3, a), xs[2 * (g / 3) + a], vb);
-        vd = fma((real)dbq(g % 3, a), xs[2 * (g / 3) + a], vd);
-      }
-      S.Xb[g][s2][s1] = vb;
-      S.Xd[g][s2][s1] = vd;
-    }
-  }
-  __syncthreads();
-  // y: nodes -> Gauss points
-  for (int task = tid; task < 63; task += blockDim.x) {
-    const int s1 = task % 7, g3 = task / 7;
-    real xb[7], xd[7];
-#pragma unroll
-    for (int s = 0; s < 7; ++s) { xb[s] = S.Xb[g3][s][s1]; xd[s] = S.Xd[g3][s][s1]; }
-#pragma unroll
-    for (int g = 0; g < 9; ++g) {
-      real bb = 0, db = 0, bd = 0;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const real B = (real)bq(g % 3, a), Dd = (real)dbq(g % 3, a);
-        bb = fma(B, xb[2 * (g / 3) + a], bb);
-        db = fma(Dd, xb[2 * (g / 3) + a], db);
-        bd = fma(B, xd[2 * (g / 3) + a], bd);
-      }
-      S.Y[0][g3][g][s1] = bb;
-      S.Y[1][g3][g][s1] = db;
-      S.Y[2][g3][g][s1] = bd;
+    for (int i = 0; i < 9; ++i) {
+      const unsigned n = n0 + (unsigned)(i % 3) + nsy * (unsigned)(i / 3) + nsz * (unsigned)a3;
+      const real xv = live ? (real)__ldg(xin + n) : (real)0;
+      const bool fixed = ess != nullptr && live && __ldg(ess + n) != 0;
+      const real x = fixed ? (real)0 : xv;
+      Xb[i] = a3 == 0 ? b3 * x : fma(b3, x, Xb[i]);
+      Xd[i] = a3 == 0 ? d3 * x : fma(d3, x, Xd[i]);
     }
   }
-  __syncthreads();
-  // x: nodes -> Gauss points, then the flux D grad x / h^2
   const real sx = (real)(1.0 / (L.hx * L.hx)), sy = (real)(1.0 / (L.hy * L.hy)),
              sz = (real)(1.0 / (L.hz * L.hz));
-  for (int task = tid; task < 81; task += blockDim.x) {
-    const int g2 = task % 9, g3 = task / 9;
-    real bb[7], db[7], bd[7];
+  // gradients and fluxes at the slice's points, folded straight back along x:
+  // Z0[a1][q2] = sum_q1 B'(q1,a1) Fx,  Z1 = sum B Fy,  Z2 = sum B Fz
+  real Z0[9], Z1[9], Z2[9];
 #pragma unroll
-    for (int s = 0; s < 7; ++s) { bb[s] = S.Y[0][g3][g2][s]; db[s] = S.Y[1][g3][g2][s]; bd[s] = S.Y[2][g3][g2][s]; }
+  for (int q2 = 0; q2 < 3; ++q2) {
+    real bb[3], db[3], bd[3];
 #pragma unroll
-    for (int g = 0; g < 9; ++g) {
-      real gx = 0, gy = 0, gz = 0;
+    for (int a1 = 0; a1 < 3; ++a1) {
+      bb[a1] = (real)bq(q2, 0) * Xb[a1] + (real)bq(q2, 1) * Xb[a1 + 3] + (real)bq(q2, 2) * Xb[a1 + 6];
+      db[a1] = (real)dbq(q2, 0) * Xb[a1] + (real)dbq(q2, 1) * Xb[a1 + 3] + (real)dbq(q2, 2) * Xb[a1 + 6];
+      bd[a1] = (real)bq(q2, 0) * Xd[a1] + (real)bq(q2, 1) * Xd[a1 + 3] + (real)bq(q2, 2) * Xd[a1 + 6];
+    }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const real B = (real)bq(g % 3, a), Dd = (real)dbq(g % 3, a);
-        gx = fma(Dd, bb[2 * (g / 3) + a], gx);
-        gy = fma(B, db[2 * (g / 3) + a], gy);
-        gz = fma(B, bd[2 * (g / 3) + a], gz);
+    for (int a1 = 0; a1 < 3; ++a1) { Z0[a1 * 3 + q2] = 0; Z1[a1 * 3 + q2] = 0; Z2[a1 * 3 + q2] = 0; }
+#pragma unroll
+    for (int q1 = 0; q1 < 3; ++q1) {
+      const real gx = (real)dbq(q1, 0) * bb[0] + (real)dbq(q1, 1) * bb[1] + (real)dbq(q1, 2) * bb[2];
+      const real gy = (real)bq(q1, 0) * db[0] + (real)bq(q1, 1) * db[1] + (real)bq(q1, 2) * db[2];
+      const real gz = (real)bq(q1, 0) * bd[0] + (real)bq(q1, 1) * bd[1] + (real)bq(q1, 2) * bd[2];
+      const real d = live ? Dq[(int64_t)(q1 + 3 * q2 + 9 * t) * L.ne + ec] : (real)0;  // coalesced in e
+      const real fx = d * gx * sx, fy = d * gy * sy, fz = d * gz * sz;
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+        Z0[a1 * 3 + q2] = fma((real)dbq(q1, a1), fx, Z0[a1 * 3 + q2]);
+        Z1[a1 * 3 + q2] = fma((real)bq(q1, a1), fy, Z1[a1 * 3 + q2]);
+        Z2[a1 * 3 + q2] = fma((real)bq(q1, a1), fz, Z2[a1 * 3 + q2]);
       }
-      const real d = S.D[g3][g2][g];
-      S.G[0][g3][g2][g] = d * gx * sx;
-      S.G[1][g3][g2][g] = d * gy * sy;
-      S.G[2][g3][g2][g] = d * gz * sz;
     }
   }
-  __syncthreads();
-  // back along x: Z0 = VD.Gx, Z1 = VB.Gy, Z2 = VB.Gz  -> [term][g3][g2][r1]
-  for (int task = tid; task < 81; task += blockDim.x) {
-    const int g2 = task % 9, g3 = task / 9;
-    real w0[9], w1[9], w2[9];
+  // back along y: UB[a2][a1] = sum_q2 B(q2,a2) Z0 + B'(q2,a2) Z1,  UD = sum_q2 B(q2,a2) Z2
+  real UB[9], UD[9];
 #pragma unroll
-    for (int l = 0; l < 9; ++l) { w0[l] = S.G[0][g3][g2][l]; w1[l] = S.G[1][g3][g2][l]; w2[l] = S.G[2][g3][g2][l]; }
+  for (int a2 = 0; a2 < 3; ++a2)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      real a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (t < vrow_cnt(r)) {
-          a0 = fma((real)vrow_coef(VD, r, t), w0[vrow_g0(r) + t], a0);
-          a1 = fma((real)vrow_coef(VB, r, t), w1[vrow_g0(r) + t], a1);
-          a2 = fma((real)vrow_coef(VB, r, t), w2[vrow_g0(r) + t], a2);
-        }
-      S.Z[0][g3][g2][r] = a0; S.Z[1][g3][g2][r] = a1; S.Z[2][g3][g2][r] = a2;
-    }
-  }
-  __syncthreads();
-  // back along y: UB = VB.Z0 + VD.Z1 (then VB in z), UD = VB.Z2 (then VD in z)
-  for (int task = tid; task < 36; task += blockDim.x) {
-    const int r1 = task % 4, g3 = task / 4;
-    real w0[9], w1[9], w2[9];
-#pragma unroll
-    for (int l = 0; l < 9; ++l) { w0[l] = S.Z[0][g3][l][r1]; w1[l] = S.Z[1][g3][l][r1]; w2[l] = S.Z[2][g3][l][r1]; }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int a1 = 0; a1 < 3; ++a1) {
       real ub = 0, ud = 0;
 #pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (t < vrow_cnt(r)) {
-          ub = fma((real)vrow_coef(VB, r, t), w0[vrow_g0(r) + t], ub);
-          ub = fma((real)vrow_coef(VD, r, t), w1[vrow_g0(r) + t], ub);
-          ud = fma((real)vrow_coef(VB, r, t), w2[vrow_g0(r) + t], ud);
-        }
-      S.U[0][g3][r][r1] = ub; S.U[1][g3][r][r1] = ud;
+      for (int q2 = 0; q2 < 3; ++q2) {
+        ub = fma((real)bq(q2, a2), Z0[a1 * 3 + q2], ub);
+        ub = fma((real)dbq(q2, a2), Z1[a1 * 3 + q2], ub);
+        ud = fma((real)bq(q2, a2), Z2[a1 * 3 + q2], ud);
+      }
+      UB[a2 * 3 + a1] = ub;
+      UD[a2 * 3 + a1] = ud;
+    }
+  // back along z: thread t owns node plane a3 = t and sums the three slices' parts,
+  // slice order 0, 1, 2 (fixed)
+  real y[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) y[i] = 0;
+  const int base = 3 * k;
+#pragma unroll
+  for (int src = 0; src < 3; ++src) {
+    const real cb = bq_rt<real>(src, 0) * (t == 0) + bq_rt<real>(src, 1) * (t == 1) + bq_rt<real>(src, 2) * (t == 2);
+    const real cd = dbq_rt<real>(src, 0) * (t == 0) + dbq_rt<real>(src, 1) * (t == 1) + dbq_rt<real>(src, 2) * (t == 2);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const real ub = __shfl_sync(0xffffffffu, UB[i], base + src);
+      const real ud = __shfl_sync(0xffffffffu, UD[i], base + src);
+      y[i] = fma(cb, ub, fma(cd, ud, y[i]));
     }
   }
-  __syncthreads();
-  // back along z and out
-  if (tid < 16) {
-    const int r1 = tid % 4, r2 = tid / 4;
-    real wb[9], wd[9];
+  if (live) {
 #pragma unroll
-    for (int l = 0; l < 9; ++l) { wb[l] = S.U[0][l][r2][r1]; wd[l] = S.U[1][l][r2][r1]; }
-    const int gx = 4 * t1 + r1, gy = 4 * t2 + r2;
+    for (int i = 0; i < 9; ++i) Ye[(int64_t)(i + 9 * t) * L.ne + e] = y[i];
+  }
+}
+
+// One thread per node; with part != nullptr each block also
+// writes its partial sum of dotw . y (the p.q of a CG step), in a fixed order.
+template <typename real>
+__global__ void __launch_bounds__(256)
+    k_node_gather(Lattice L, const real* __restrict__ Ye, const uint8_t* __restrict__ ess,
+                  const double* __restrict__ xin, double* __restrict__ yout,
+                  const double* __restrict__ dotw, double* __restrict__ part) {
+  const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = n < (unsigned)L.ndof;
+  const unsigned nxy = n / (unsigned)L.Nx;
+  const int ix = (int)(n - nxy * (unsigned)L.Nx);
+  const int iz = (int)(nxy / (unsigned)L.Ny), iy = (int)(nxy - (unsigned)iz * (unsigned)L.Ny);
+  double yv = 0.0;
+  if (live) {
+    if (ess != nullptr && ess[n]) {
+      yv = xin[n];
+    } else {
+      const int gi[3] = {ix, iy, iz};
+      const int nel[3] = {L.nx, L.ny, L.nz};
+      // per axis: up to two (element, local index) pairs
+      int e0[3], a0[3], cnt[3];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      real acc = 0;
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (t < vrow_cnt(r)) {
-          acc = fma((real)vrow_coef(VB, r, t), wb[vrow_g0(r) + t], acc);
-          acc = fma((real)vrow_coef(VD, r, t), wd[vrow_g0(r) + t], acc);
-        }
-      const int gz = 4 * t3 + r;
-      if (gx < L.Nx && gy < L.Ny && gz < L.Nz) {
-        const int64_t n = gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz);
-        yout[n] = S.ess[r + 2][r2 + 2][r1 + 2] ? xin[n] : (double)acc;
+      for (int d = 0; d < 3; ++d) {
+        const int i = gi[d];
+        if (i & 1) { e0[d] = i >> 1; a0[d] = 1; cnt[d] = 1; }
+        else if (i == 0) { e0[d] = 0; a0[d] = 0; cnt[d] = 1; }
+        else if ((i >> 1) >= nel[d]) { e0[d] = (i >> 1) - 1; a0[d] = 2; cnt[d] = 1; }
+        else { e0[d] = (i >> 1) - 1; a0[d] = 2; cnt[d] = 2; }   // elements i/2-1 (a=2), i/2 (a=0)
       }
+      const unsigned ne = (unsigned)L.ne;
+      real acc = 0;
+      for (int c3 = 0; c3 < cnt[2]; ++c3)
+        for (int c2 = 0; c2 < cnt[1]; ++c2)
+          for (int c1 = 0; c1 < cnt[0]; ++c1) {
+            const unsigned ex = e0[0] + c1, ey = e0[1] + c2, ez = e0[2] + c3;
+            const unsigned a1 = c1 ? 0 : a0[0], a2 = c2 ? 0 : a0[1], a3 = c3 ? 0 : a0[2];
+            const unsigned e = ex + (unsigned)L.nx * (ey + (unsigned)L.ny * ez);
+            acc += Ye[(size_t)(a1 + 3 * a2 + 9 * a3) * ne + e];
+          }
+      yv = (double)acc;
+    }
+    yout[n] = yv;
+  }
+  if (part != nullptr) {
+    __shared__ double sh[32];
+    double v = live ? dotw[n] * yv : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (threadIdx.x == 0) part[blockIdx.x] = t;
     }
   }
 }
@@ -960,28 +971,40 @@ int hm_launch_assemble(const Lattice& L, const void* quad, int precision, const 
   return launch_assemble_t<double>(L, quad, indptr, ess, o, stream);
 }
 
-template <typename real>
-static int launch_apply_t(const Lattice& L, const void* quad, const uint8_t* ess, const double* x,
-                          double* y, void* stream) {
-  const size_t smem = sizeof(ApplySmem<real>);
-  static bool configured[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !configured[dev]) {
-    if (cudaFuncSetAttribute(k_tile_apply_A<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-      return HM_ERR_CUDA;
-    configured[dev] = true;
-  }
-  dim3 grid(L.tx, L.ty, L.tz);
-  k_tile_apply_A<real><<<grid, 256, smem, S_(stream)>>>(L, (const real*)quad, ess, x, y);
+int hm_launch_jacobian_prepare(const Lattice& L, const void* quad, int precision, void* jac,
+                               void* stream) {
+  const int blocks = grid1(L.ne * 27, 256);
+  if (precision == HM_FP32)
+    k_extract_D<float><<<blocks, 256, 0, S_(stream)>>>(L, (const float*)quad, (float*)jac);
+  else
+    k_extract_D<double><<<blocks, 256, 0, S_(stream)>>>(L, (const double*)quad, (double*)jac);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 
-int hm_launch_apply_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,
+template <typename real>
+static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const double* x,
+                          double* y, const double* dotw, double* part, void* stream) {
+  real* Dq = static_cast<real*>(jac);
+  real* Ye = Dq + L.ne * 27;
+  const int64_t warps = (L.ne + 9) / 10;
+  k_elem_apply<real><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
+  k_node_gather<real><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, Ye, ess, x, y, dotw, part);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+// number of partial sums k_node_gather writes when asked for the fused dot product
+int64_t hm_apply_dot_parts(const Lattice& L) { return grid1(L.ndof, 256); }
+
+int hm_launch_apply_A(const Lattice& L, void* jac, int precision, const uint8_t* ess,
                       const double* x, double* y, void* stream) {
-  if (precision == HM_FP32) return launch_apply_t<float>(L, quad, ess, x, y, stream);
-  return launch_apply_t<double>(L, quad, ess, x, y, stream);
+  if (precision == HM_FP32) return launch_apply_t<float>(L, jac, ess, x, y, nullptr, nullptr, stream);
+  return launch_apply_t<double>(L, jac, ess, x, y, nullptr, nullptr, stream);
+}
+
+int hm_launch_apply_A_dot(const Lattice& L, void* jac, int precision, const uint8_t* ess,
+                          const double* x, double* y, double* part, void* stream) {
+  if (precision == HM_FP32) return launch_apply_t<float>(L, jac, ess, x, y, x, part, stream);
+  return launch_apply_t<double>(L, jac, ess, x, y, x, part, stream);
 }
 
 int hm_launch_diag_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,

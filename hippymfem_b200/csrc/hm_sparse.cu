@@ -13,7 +13,7 @@
 
 namespace hm {
 
-constexpr int kReduceBlocks = 296;  // 2 x 148 SMs
+constexpr int kReduceBlocks = 1184;  // 8 x 148 SMs
 constexpr int kReduceThreads = 256;
 
 // ------------------------------------------------------------------------ SpMV
@@ -128,10 +128,10 @@ __global__ void k_pcg_init_final(const double* __restrict__ part, double* __rest
   }
 }
 
-__global__ void k_pcg_alpha(const double* __restrict__ part, double* __restrict__ sc) {
+__global__ void k_pcg_alpha(const double* __restrict__ part, int64_t nparts, double* __restrict__ sc) {
   __shared__ double sh[32];
   double t = 0.0;
-  for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) t += part[b];
+  for (int64_t b = threadIdx.x; b < nparts; b += blockDim.x) t += part[b];
   t = block_sum(t, sh);
   if (threadIdx.x == 0) {
     sc[SC_PQ] = t;
@@ -238,13 +238,18 @@ extern "C" int hm_dot(int64_t n, const double* x, const double* y, double* out, 
   if (n < 0 || !out || !work || (n > 0 && (!x || !y))) return HM_ERR_ARG;
   double* part = static_cast<double*>(work);
   k_dot_partial<<<kReduceBlocks, kReduceThreads, 0, S_(stream)>>>(n, x, y, part);
-  k_reduce_final<<<1, 256, 0, S_(stream)>>>(part, 1, out);
+  k_reduce_final<<<1, 1024, 0, S_(stream)>>>(part, 1, out);
   return ok_or_cuda();
 }
 
 extern "C" int64_t hm_pcg_workspace_bytes(int64_t n) {
-  return (int64_t)sizeof(double) * (4 * n + SC_N + 3 * (int64_t)kReduceBlocks + 8);
+  // r, z, p, q, the partial sums of p.q (at most one per node), scalars, partials
+  return (int64_t)sizeof(double) * (5 * n + SC_N + 3 * (int64_t)kReduceBlocks + 8);
 }
+
+int hm_launch_apply_A_dot(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
+                          const double* x, double* y, double* part, void* stream);
+int64_t hm_apply_dot_parts(const hm::Lattice& L);
 
 int hm_pcg_operator(int64_t n, const int32_t* indptr, const int32_t* indices, const double* vals,
                     const hm::Lattice* L, const void* quad, int precision, const uint8_t* ess,
@@ -263,12 +268,13 @@ extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indi
   double* z = w + n;
   double* p = w + 2 * n;
   double* q = w + 3 * n;
-  double* sc = w + 4 * n;
+  double* pq_part = w + 4 * n;
+  double* sc = w + 5 * n;
   double* part = sc + SC_N;
   int rc = hm_pcg_operator(n, indptr, indices, vals, L, quad, precision, ess, x, q, stream);
   if (rc) return rc;
   k_pcg_init<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, q, diag, r, z, p, part);
-  k_pcg_init_final<<<1, 256, 0, s>>>(part, sc, rtol);
+  k_pcg_init_final<<<1, 1024, 0, s>>>(part, sc, rtol);
   double host[SC_N];
   int it = 0;
   for (;;) {
@@ -278,12 +284,19 @@ extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indi
     const int stop = it + check_every < maxiter ? it + check_every : maxiter;
     for (; it < stop;) {
       ++it;
-      rc = hm_pcg_operator(n, indptr, indices, vals, L, quad, precision, ess, p, q, stream);
+      int64_t nparts = kReduceBlocks;
+      if (L != nullptr) {
+        // the lattice operator sums p.q as it writes q
+        rc = hm_launch_apply_A_dot(*L, const_cast<void*>(quad), precision, ess, p, q, pq_part, stream);
+        nparts = hm_apply_dot_parts(*L);
+      } else {
+        rc = hm_pcg_operator(n, indptr, indices, vals, L, quad, precision, ess, p, q, stream);
+        if (!rc) k_dot_partial<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, q, pq_part);
+      }
       if (rc) return rc;
-      k_dot_partial<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, q, part);
-      k_pcg_alpha<<<1, 256, 0, s>>>(part, sc);
+      k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, nparts, sc);
       k_pcg_update<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, z, p, q, diag, part);
-      k_pcg_beta<<<1, 256, 0, s>>>(part, sc, it);
+      k_pcg_beta<<<1, 1024, 0, s>>>(part, sc, it);
       k_pcg_pupdate<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z, p);
     }
     if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;

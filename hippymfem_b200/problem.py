@@ -188,7 +188,7 @@ class PDEVariationalProblem:
         if self.matrix_free_solves:
             # the matrix-free operator keeps its own copy of the point's data
             self._require_finite("the Jacobian")
-            return MatrixFreeJacobian(self.mesh, quad.clone(), self.bc0.marker, self.precision)
+            return MatrixFreeJacobian(self.mesh, quad, self.bc0.marker, self.precision)
         blocks, _ = self._assemble(quad, blocks=("A",))
         self._require_finite("the Jacobian")
         return blocks["A"]

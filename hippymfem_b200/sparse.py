@@ -67,14 +67,24 @@ class CSRBlock:
 
 class MatrixFreeJacobian:
     """The Jacobian ``A(m)`` applied from the quadrature data of a point, with its
-    elimination (``apply_ij_at`` for the (ADJOINT, STATE) pair)."""
+    elimination (``apply_ij_at`` for the (ADJOINT, STATE) pair).  Keeps the operator's
+    data (D of the point in the layout the operator streams, plus its scratch); applies
+    that share one instance must run in one stream."""
 
-    def __init__(self, mesh, quad, ess_marker, precision=_lib.HM_FP64):
-        self.mesh, self.quad, self.ess, self.precision = mesh, quad, ess_marker, precision
+    def __init__(self, mesh, quad, ess_marker, precision=_lib.HM_FP64, stream=None):
+        self.mesh, self.ess, self.precision = mesh, ess_marker, precision
         self.nrow = self.ncol = mesh.ndof
+        nbytes = lib.hm_lattice_jacobian_bytes(mesh.handle, precision)
+        self.jac = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=mesh.device)
+        check(lib.hm_lattice_jacobian_prepare(mesh.handle, ptr(quad), precision, ptr(self.jac),
+                                              stream_ptr(stream)), "hm_lattice_jacobian_prepare")
+        # the diagonal (Jacobi) is taken now, so the point's quadrature data need not be kept
+        self._diag = torch.empty(self.nrow, dtype=torch.float64, device=mesh.device)
+        check(lib.hm_lattice_diag_A(mesh.handle, ptr(quad), precision, ptr(ess_marker),
+                                    ptr(self._diag), stream_ptr(stream)), "hm_lattice_diag_A")
 
     def mult(self, x, y, stream=None):
-        check(lib.hm_lattice_apply_A(self.mesh.handle, ptr(self.quad), self.precision,
+        check(lib.hm_lattice_apply_A(self.mesh.handle, ptr(self.jac), self.precision,
                                      ptr(self.ess), ptr(x), ptr(y), stream_ptr(stream)),
               "hm_lattice_apply_A")
         return y
@@ -84,11 +94,9 @@ class MatrixFreeJacobian:
     mult_transpose = MultTranspose = mult
 
     def diagonal(self, out=None, stream=None):
-        out = out if out is not None else torch.empty(self.nrow, dtype=torch.float64,
-                                                      device=self.mesh.device)
-        check(lib.hm_lattice_diag_A(self.mesh.handle, ptr(self.quad), self.precision,
-                                    ptr(self.ess), ptr(out), stream_ptr(stream)),
-              "hm_lattice_diag_A")
+        if out is None:
+            return self._diag.clone()
+        out.copy_(self._diag)
         return out
 
 
@@ -136,7 +144,7 @@ class PCGSolver:
             p = op.pattern
             args = (ptr(p.indptr), ptr(p.indices), ptr(op.values), None, None, _lib.HM_FP64, None)
         else:
-            args = (None, None, None, op.mesh.handle, ptr(op.quad), op.precision, ptr(op.ess))
+            args = (None, None, None, op.mesh.handle, ptr(op.jac), op.precision, ptr(op.ess))
         rc = lib.hm_pcg(op.nrow, *args, ptr(self.diag), ptr(b), ptr(x),
                         prm["rel_tolerance"], prm["max_iter"], prm["check_every"], ptr(self.work),
                         ctypes.byref(it), ctypes.byref(rr), stream_ptr(stream))

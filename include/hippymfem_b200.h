@@ -125,10 +125,16 @@ int hm_lattice_assemble(const hm_lattice* h, const void* d_quad, int precision,
                         double* d_vec_adjoint, int zero_ess_vectors, void* stream);
 
 /* Matrix-free Q2 operator y = A(D) x with the Jacobian's elimination (x zeroed on
- * d_ess, y = x there), D the first component of the quadrature data: the product
- * apply_ij_at gives for (ADJOINT, STATE) (modeling/PDEVariationalProblem.py:1672). */
-int hm_lattice_apply_A(const hm_lattice* h, const void* d_quad, int precision,
-                       const uint8_t* d_ess, const double* d_x, double* d_y, void* stream);
+ * d_ess, y = x there): the product apply_ij_at gives for (ADJOINT, STATE)
+ * (modeling/PDEVariationalProblem.py:1672).  Its data d_jac (hm_lattice_jacobian_bytes)
+ * holds D of the point in a layout the operator streams, filled once per point by
+ * hm_lattice_jacobian_prepare from the quadrature data, and the operator's own scratch:
+ * two applies with the same d_jac must not overlap on the GPU. */
+int64_t hm_lattice_jacobian_bytes(const hm_lattice* h, int precision);
+int hm_lattice_jacobian_prepare(const hm_lattice* h, const void* d_quad, int precision,
+                                void* d_jac, void* stream);
+int hm_lattice_apply_A(const hm_lattice* h, void* d_jac, int precision, const uint8_t* d_ess,
+                       const double* d_x, double* d_y, void* stream);
 /* diagonal of A(D) (eliminated rows: 1), for Jacobi preconditioning */
 int hm_lattice_diag_A(const hm_lattice* h, const void* d_quad, int precision,
                       const uint8_t* d_ess, double* d_diag, void* stream);
@@ -170,7 +176,7 @@ int hm_csr_diag(int64_t nrow, const int32_t* d_indptr, const double* d_vals,
                 double* d_diag, void* stream);
 
 /* Jacobi-preconditioned CG in FP64 for A x = b with A a CSR block (d_indptr != NULL)
- * or the lattice's matrix-free operator (lattice != NULL, d_quad its D), stopped at
+ * or the lattice's matrix-free operator (lattice != NULL, d_quad its d_jac), stopped at
  * ||r||_2 <= rtol ||b||_2 or maxiter.  The B200 replacement of the incremental
  * solves' hypre PCG (modeling/PDEVariationalProblem.py:1583-1609,
  * algorithms/linSolvers.py:709).  x is the initial guess on entry.  The iteration
