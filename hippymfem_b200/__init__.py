@@ -11,6 +11,6 @@ from .modeling import (DiscreteStateObservation, Model, PointwiseStateObservatio
                        ReducedHessian, observation_operator)
 from .pattern import LatticePattern, build_tables  # noqa: F401
 from .problem import ADJOINT, NVAR, PARAMETER, STATE, PDEVariationalProblem  # noqa: F401
-from .sparse import CSRBlock, MatrixFreeJacobian, PCGSolver  # noqa: F401
+from .sparse import CSRBlock, MatrixFreeJacobian, MixedPCGSolver, PCGSolver  # noqa: F401
 
 __version__ = "0.1.0"

@@ -52,7 +52,7 @@ SIGNATURES = {
                                    _p]),
     "hm_lattice_residual_noalloc": (_i32, [_p, _p, _p, _p, _d, _p, _p, _p, _p, _i32, _p, _p]),
     "hm_lattice_jacobian_bytes": (_i64, [_p, _i32]),
-    "hm_lattice_jacobian_prepare": (_i32, [_p, _p, _i32, _p, _p]),
+    "hm_lattice_jacobian_prepare": (_i32, [_p, _p, _i32, _p, _i32, _p]),
     "hm_lattice_apply_A": (_i32, [_p, _p, _i32, _p, _p, _p, _p]),
     "hm_lattice_diag_A": (_i32, [_p, _p, _i32, _p, _p, _p]),
     "hm_csr_spmv": (_i32, [_i64, _p, _p, _p, _p, _p, _d, _d, _p]),
@@ -61,6 +61,9 @@ SIGNATURES = {
     "hm_pcg_workspace_bytes": (_i64, [_i64]),
     "hm_pcg": (_i32, [_i64, _p, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _d, _i32, _i32, _p, _p,
                       _p, _p]),
+    "hm_pcg_mixed_workspace_bytes": (_i64, [_i64]),
+    "hm_pcg_mixed": (_i32, [_p, _p, _p, _p, _p, _p, _p, _d, _d, _i32, _i32, _i32, _p, _p, _p, _p,
+                            _p]),
     "hm_dot_workspace_bytes": (_i64, [_i64]),
     "hm_dot": (_i32, [_i64, _p, _p, _p, _p, _p]),
 }

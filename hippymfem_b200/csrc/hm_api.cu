@@ -105,11 +105,13 @@ extern "C" int64_t hm_lattice_jacobian_bytes(const hm_lattice* h, int precision)
   return 2 * 27 * h->L.ne * (precision == HM_FP32 ? 4 : 8);
 }
 
-extern "C" int hm_lattice_jacobian_prepare(const hm_lattice* h, const void* quad, int precision,
-                                           void* jac, void* stream) {
+extern "C" int hm_lattice_jacobian_prepare(const hm_lattice* h, const void* quad,
+                                           int quad_precision, void* jac, int precision,
+                                           void* stream) {
   if (!h || !quad || !jac) return HM_ERR_ARG;
   if (precision != HM_FP64 && precision != HM_FP32) return HM_ERR_ARG;
-  return hm_launch_jacobian_prepare(h->L, quad, precision, jac, stream);
+  if (quad_precision != HM_FP64 && quad_precision != HM_FP32) return HM_ERR_ARG;
+  return hm_launch_jacobian_prepare(h->L, quad, quad_precision, jac, precision, stream);
 }
 
 extern "C" int hm_lattice_apply_A(const hm_lattice* h, void* jac, int precision,
@@ -153,4 +155,20 @@ extern "C" int hm_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, 
   }
   return hm_pcg_impl(n, indptr, indices, vals, L, quad, precision, ess, diag, b, x, rtol, maxiter,
                      check_every, work, iterations, relres, stream);
+}
+
+extern "C" int64_t hm_pcg_mixed_workspace_bytes(int64_t n);
+extern "C" int hm_pcg_mixed_impl(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t* ess,
+                                 const double* diag, const double* b, double* x, double rtol,
+                                 double delta, int max_updates, int maxiter, int check_every,
+                                 void* work, int* iterations, int* updates, double* relres,
+                                 void* stream);
+
+extern "C" int hm_pcg_mixed(const hm_lattice* lattice, void* jac64, void* jac32, const uint8_t* ess,
+                            const double* diag, const double* b, double* x, double rtol,
+                            double delta, int max_updates, int maxiter, int check_every,
+                            void* work, int* iterations, int* updates, double* relres, void* stream) {
+  if (!lattice) return HM_ERR_ARG;
+  return hm_pcg_mixed_impl(&lattice->L, jac64, jac32, ess, diag, b, x, rtol, delta, max_updates,
+                           maxiter, check_every, work, iterations, updates, relres, stream);
 }

@@ -21,8 +21,8 @@ int hm_launch_assemble(const hm::Lattice& L, const void* quad, int precision,
                        const int32_t* indptr, const uint8_t* ess, double f, double* vA,
                        double* vC, double* vWum, double* vWmm, double* vs, double* vp,
                        double* va, int zero_ess, void* stream);
-int hm_launch_jacobian_prepare(const hm::Lattice& L, const void* quad, int precision, void* jac,
-                               void* stream);
+int hm_launch_jacobian_prepare(const hm::Lattice& L, const void* quad, int quad_precision,
+                               void* jac, int precision, void* stream);
 int hm_launch_apply_A(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
                       const double* x, double* y, void* stream);
 int hm_launch_diag_A(const hm::Lattice& L, const void* quad, int precision,
@@ -30,3 +30,5 @@ int hm_launch_diag_A(const hm::Lattice& L, const void* quad, int precision,
 int hm_launch_apply_A_dot(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
                           const double* x, double* y, double* part, void* stream);
 int64_t hm_apply_dot_parts(const hm::Lattice& L);
+int hm_launch_apply_A32_dot(const hm::Lattice& L, void* jac32, const uint8_t* ess, const float* x,
+                            float* y, double* part, void* stream);

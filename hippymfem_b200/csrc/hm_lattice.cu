@@ -691,13 +691,13 @@ __global__ void __launch_bounds__(256, 2)
 // D is kept in SoA layout Dq[q][e] (hm_lattice_jacobian_prepare), so both passes read
 // and write coalesced.
 
-template <typename real>
-__global__ void k_extract_D(Lattice L, const real* __restrict__ quad, real* __restrict__ Dq) {
+template <typename src, typename real>
+__global__ void k_extract_D(Lattice L, const src* __restrict__ quad, real* __restrict__ Dq) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= L.ne * 27) return;
   const int64_t e = i / 27;
   const int q = (int)(i - e * 27);
-  Dq[(int64_t)q * L.ne + e] = quad[e * 216 + q];
+  Dq[(int64_t)q * L.ne + e] = (real)quad[e * 216 + q];
 }
 
 // B(q, a) and B'(q, a) for a run-time point index q (a compile-time)
@@ -710,10 +710,10 @@ __device__ __forceinline__ real dbq_rt(int q, int a) {
   return q == 0 ? (real)dbq(0, a) : q == 1 ? (real)dbq(1, a) : (real)dbq(2, a);
 }
 
-template <typename real>
+template <typename real, typename vec>
 __global__ void __launch_bounds__(256, 2)
     k_elem_apply(Lattice L, const real* __restrict__ Dq, const uint8_t* __restrict__ ess,
-                 const double* __restrict__ xin, real* __restrict__ Ye) {
+                 const vec* __restrict__ xin, real* __restrict__ Ye) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int k = lane / 3, t = lane - 3 * k;                 // element slot, Gauss slice
@@ -813,11 +813,11 @@ __global__ void __launch_bounds__(256, 2)
 
 // One thread per node; with part != nullptr each block also
 // writes its partial sum of dotw . y (the p.q of a CG step), in a fixed order.
-template <typename real>
+template <typename real, typename vec>
 __global__ void __launch_bounds__(256)
     k_node_gather(Lattice L, const real* __restrict__ Ye, const uint8_t* __restrict__ ess,
-                  const double* __restrict__ xin, double* __restrict__ yout,
-                  const double* __restrict__ dotw, double* __restrict__ part) {
+                  const vec* __restrict__ xin, vec* __restrict__ yout,
+                  const vec* __restrict__ dotw, double* __restrict__ part) {
   const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = n < (unsigned)L.ndof;
   const unsigned nxy = n / (unsigned)L.Nx;
@@ -852,11 +852,11 @@ __global__ void __launch_bounds__(256)
           }
       yv = (double)acc;
     }
-    yout[n] = yv;
+    yout[n] = (vec)yv;
   }
   if (part != nullptr) {
     __shared__ double sh[32];
-    double v = live ? dotw[n] * yv : 0.0;
+    double v = live ? (double)dotw[n] * yv : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
@@ -971,24 +971,28 @@ int hm_launch_assemble(const Lattice& L, const void* quad, int precision, const 
   return launch_assemble_t<double>(L, quad, indptr, ess, o, stream);
 }
 
-int hm_launch_jacobian_prepare(const Lattice& L, const void* quad, int precision, void* jac,
-                               void* stream) {
+int hm_launch_jacobian_prepare(const Lattice& L, const void* quad, int quad_precision, void* jac,
+                               int precision, void* stream) {
   const int blocks = grid1(L.ne * 27, 256);
-  if (precision == HM_FP32)
-    k_extract_D<float><<<blocks, 256, 0, S_(stream)>>>(L, (const float*)quad, (float*)jac);
-  else
-    k_extract_D<double><<<blocks, 256, 0, S_(stream)>>>(L, (const double*)quad, (double*)jac);
+  cudaStream_t s = S_(stream);
+  if (quad_precision == HM_FP32) {
+    if (precision == HM_FP32) k_extract_D<float, float><<<blocks, 256, 0, s>>>(L, (const float*)quad, (float*)jac);
+    else k_extract_D<float, double><<<blocks, 256, 0, s>>>(L, (const float*)quad, (double*)jac);
+  } else {
+    if (precision == HM_FP32) k_extract_D<double, float><<<blocks, 256, 0, s>>>(L, (const double*)quad, (float*)jac);
+    else k_extract_D<double, double><<<blocks, 256, 0, s>>>(L, (const double*)quad, (double*)jac);
+  }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 
-template <typename real>
-static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const double* x,
-                          double* y, const double* dotw, double* part, void* stream) {
+template <typename real, typename vec>
+static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const vec* x,
+                          vec* y, const vec* dotw, double* part, void* stream) {
   real* Dq = static_cast<real*>(jac);
   real* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
-  k_elem_apply<real><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
-  k_node_gather<real><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, Ye, ess, x, y, dotw, part);
+  k_elem_apply<real, vec><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
+  k_node_gather<real, vec><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, Ye, ess, x, y, dotw, part);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 
@@ -997,14 +1001,21 @@ int64_t hm_apply_dot_parts(const Lattice& L) { return grid1(L.ndof, 256); }
 
 int hm_launch_apply_A(const Lattice& L, void* jac, int precision, const uint8_t* ess,
                       const double* x, double* y, void* stream) {
-  if (precision == HM_FP32) return launch_apply_t<float>(L, jac, ess, x, y, nullptr, nullptr, stream);
-  return launch_apply_t<double>(L, jac, ess, x, y, nullptr, nullptr, stream);
+  if (precision == HM_FP32)
+    return launch_apply_t<float, double>(L, jac, ess, x, y, nullptr, nullptr, stream);
+  return launch_apply_t<double, double>(L, jac, ess, x, y, nullptr, nullptr, stream);
 }
 
 int hm_launch_apply_A_dot(const Lattice& L, void* jac, int precision, const uint8_t* ess,
                           const double* x, double* y, double* part, void* stream) {
-  if (precision == HM_FP32) return launch_apply_t<float>(L, jac, ess, x, y, x, part, stream);
-  return launch_apply_t<double>(L, jac, ess, x, y, x, part, stream);
+  if (precision == HM_FP32) return launch_apply_t<float, double>(L, jac, ess, x, y, x, part, stream);
+  return launch_apply_t<double, double>(L, jac, ess, x, y, x, part, stream);
+}
+
+// the FP32 operator on FP32 vectors (the inner solves of the mixed-precision PCG)
+int hm_launch_apply_A32_dot(const Lattice& L, void* jac32, const uint8_t* ess, const float* x,
+                            float* y, double* part, void* stream) {
+  return launch_apply_t<float, float>(L, jac32, ess, x, y, part ? x : nullptr, part, stream);
 }
 
 int hm_launch_diag_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,

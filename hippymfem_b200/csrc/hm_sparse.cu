@@ -88,18 +88,24 @@ __global__ void k_reduce_final(const double* __restrict__ part, int nq, double* 
 // device scalars
 enum { SC_RZ = 0, SC_PQ, SC_ALPHA, SC_BETA, SC_RR, SC_BB, SC_TOL2, SC_CONV, SC_TMP0, SC_TMP1, SC_TMP2, SC_N };
 
-// r = b - q, z = dinv r, p = z; partials of r.z, r.r, b.b
+// Vector kernels, templated on the vector type T (double, or float for the inner solves
+// of the mixed-precision PCG); sums are accumulated in double.
+
+// r = b - q, z = r / diag, p = z; partials of r.z, r.r, b.b
+template <typename T>
 __global__ void __launch_bounds__(kReduceThreads)
-    k_pcg_init(int64_t n, const double* __restrict__ b, const double* __restrict__ q,
-               const double* __restrict__ dinv_src, double* __restrict__ r, double* __restrict__ z,
-               double* __restrict__ p, double* __restrict__ part) {
+    k_pcg_init(int64_t n, const T* __restrict__ b, const T* __restrict__ q,
+               const double* __restrict__ diag, T* __restrict__ r, T* __restrict__ z,
+               T* __restrict__ p, double* __restrict__ part) {
   __shared__ double sh[32];
   double rz = 0.0, rr = 0.0, bb = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double ri = b[i] - q[i];
-    const double zi = ri / dinv_src[i];
+    const T ri = b[i] - q[i];
+    const T zi = ri / (T)diag[i];
     r[i] = ri; z[i] = zi; p[i] = zi;
-    rz = fma(ri, zi, rz); rr = fma(ri, ri, rr); bb = fma(b[i], b[i], bb);
+    rz = fma((double)ri, (double)zi, rz);
+    rr = fma((double)ri, (double)ri, rr);
+    bb = fma((double)b[i], (double)b[i], bb);
   }
   rz = block_sum(rz, sh);
   rr = block_sum(rr, sh);
@@ -141,20 +147,21 @@ __global__ void k_pcg_alpha(const double* __restrict__ part, int64_t nparts, dou
 }
 
 // x += alpha p, r -= alpha q, z = r / diag; partials of r.z and r.r
+template <typename T>
 __global__ void __launch_bounds__(kReduceThreads)
-    k_pcg_update(int64_t n, const double* __restrict__ sc, double* __restrict__ x,
-                 double* __restrict__ r, double* __restrict__ z, const double* __restrict__ p,
-                 const double* __restrict__ q, const double* __restrict__ diag,
-                 double* __restrict__ part) {
+    k_pcg_update(int64_t n, const double* __restrict__ sc, T* __restrict__ x, T* __restrict__ r,
+                 T* __restrict__ z, const T* __restrict__ p, const T* __restrict__ q,
+                 const double* __restrict__ diag, double* __restrict__ part) {
   __shared__ double sh[32];
-  const double alpha = sc[SC_ALPHA];
+  const T alpha = (T)sc[SC_ALPHA];
   double rz = 0.0, rr = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] = fma(alpha, p[i], x[i]);
-    const double ri = fma(-alpha, q[i], r[i]);
-    const double zi = ri / diag[i];
+    const T ri = fma(-alpha, q[i], r[i]);
+    const T zi = ri / (T)diag[i];
     r[i] = ri; z[i] = zi;
-    rz = fma(ri, zi, rz); rr = fma(ri, ri, rr);
+    rz = fma((double)ri, (double)zi, rz);
+    rr = fma((double)ri, (double)ri, rr);
   }
   rz = block_sum(rz, sh);
   rr = block_sum(rr, sh);
@@ -184,12 +191,111 @@ __global__ void k_pcg_beta(const double* __restrict__ part, double* __restrict__
   }
 }
 
-__global__ void k_pcg_pupdate(int64_t n, const double* __restrict__ sc, const double* __restrict__ z,
-                              double* __restrict__ p) {
+template <typename T>
+__global__ void k_pcg_pupdate(int64_t n, const double* __restrict__ sc, const T* __restrict__ z,
+                              T* __restrict__ p) {
   if (sc[SC_CONV] >= 0.0) return;
-  const double beta = sc[SC_BETA];
+  const T beta = (T)sc[SC_BETA];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = fma(beta, p[i], z[i]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kReduceThreads)
+    k_dot_partial_t(int64_t n, const T* __restrict__ a, const T* __restrict__ b, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v = fma((double)a[i], (double)b[i], v);
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// Mixed precision (reliable updates): the FP32 vectors are scaled by s, the FP64 norm of
+// the residual at the last anchor (sc[SC_S]); sc[SC_SOLD] is the scale before it.
+enum { SC_S = SC_TMP0, SC_SOLD = SC_TMP1, SC_TRUE = SC_TMP2 };
+
+// x64 += s x32, x32 = 0
+__global__ void k_mx_accum(int64_t n, const double* __restrict__ sc, float* __restrict__ x32,
+                           double* __restrict__ x) {
+  const double s = sc[SC_S];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] = fma(s, (double)x32[i], x[i]);
+    x32[i] = 0.0f;
+  }
+}
+
+// r64 = b - t64; partials of r64.r64
+__global__ void __launch_bounds__(kReduceThreads)
+    k_residual64(int64_t n, const double* __restrict__ b, const double* __restrict__ t,
+                 double* __restrict__ r, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ri = b[i] - (t ? t[i] : 0.0);
+    r[i] = ri;
+    v = fma(ri, ri, v);
+  }
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// the true residual's r.r; the new scale
+__global__ void k_mx_scale(const double* __restrict__ part, double* __restrict__ sc) {
+  __shared__ double sh[32];
+  double t = 0.0;
+  for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) t += part[b];
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_TRUE] = t;
+    sc[SC_SOLD] = sc[SC_S];
+    sc[SC_S] = t > 0.0 ? sqrt(t) : 1.0;
+  }
+}
+
+// r32 = r64 / s, z32 = r32 / diag, p32 = z32 (reset) or p32 * s_old / s; partials r.z, r.r
+__global__ void __launch_bounds__(kReduceThreads)
+    k_mx_anchor(int64_t n, const double* __restrict__ r64, const double* __restrict__ diag,
+                const double* __restrict__ sc, int reset_p, float* __restrict__ r,
+                float* __restrict__ z, float* __restrict__ p, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const double inv = 1.0 / sc[SC_S];
+  const float pscale = (float)(sc[SC_SOLD] * inv);
+  double rz = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float ri = (float)(r64[i] * inv);
+    const float zi = ri / (float)diag[i];
+    r[i] = ri; z[i] = zi;
+    p[i] = reset_p ? zi : p[i] * pscale;
+    rz = fma((double)ri, (double)zi, rz);
+    rr = fma((double)ri, (double)ri, rr);
+  }
+  rz = block_sum(rz, sh);
+  rr = block_sum(rr, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rz;
+    part[kReduceBlocks + blockIdx.x] = rr;
+  }
+}
+
+// scalars of the recurrence after an anchor; bb and tol2 are in the scaled units
+__global__ void k_mx_anchor_final(const double* __restrict__ part, double* __restrict__ sc,
+                                  const double* __restrict__ bbp, double rtol) {
+  __shared__ double sh[32];
+  double v[2];
+  for (int q = 0; q < 2; ++q) {
+    double t = 0.0;
+    for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) t += part[q * kReduceBlocks + b];
+    v[q] = block_sum(t, sh);
+  }
+  if (threadIdx.x == 0) {
+    const double s = sc[SC_S];
+    sc[SC_RZ] = v[0];
+    sc[SC_RR] = v[1];
+    sc[SC_BB] = *bbp / (s * s);
+    sc[SC_TOL2] = rtol * rtol;
+    sc[SC_CONV] = -1.0;
+  }
 }
 
 }  // namespace hm
@@ -250,30 +356,66 @@ extern "C" int64_t hm_pcg_workspace_bytes(int64_t n) {
 int hm_launch_apply_A_dot(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
                           const double* x, double* y, double* part, void* stream);
 int64_t hm_apply_dot_parts(const hm::Lattice& L);
-
+int hm_launch_apply_A32_dot(const hm::Lattice& L, void* jac32, const uint8_t* ess, const float* x,
+                            float* y, double* part, void* stream);
 int hm_pcg_operator(int64_t n, const int32_t* indptr, const int32_t* indices, const double* vals,
                     const hm::Lattice* L, const void* quad, int precision, const uint8_t* ess,
                     const double* x, double* y, void* stream);
 
-extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indices,
-                           const double* vals, const hm::Lattice* L, const void* quad,
-                           int precision, const uint8_t* ess, const double* diag, const double* b,
-                           double* x, double rtol, int maxiter, int check_every, void* work,
-                           int* iterations, double* relres, void* stream) {
-  if (n <= 0 || !diag || !b || !x || !work || maxiter < 0) return HM_ERR_ARG;
-  if (check_every <= 0) check_every = 1;
+namespace {
+
+// The operator of one PCG: y = A x, and, when part is given, the partial sums of x.y
+// (returns their count through *nparts).
+struct PcgOp {
+  int64_t n;
+  const int32_t* indptr;
+  const int32_t* indices;
+  const double* vals;
+  const hm::Lattice* L;
+  void* jac;
+  int precision;
+  const uint8_t* ess;
+};
+
+int op_apply(const PcgOp& o, const double* x, double* y, double* part, int64_t* nparts, void* stream) {
+  if (o.L != nullptr) {
+    if (part) {
+      *nparts = hm_apply_dot_parts(*o.L);
+      return hm_launch_apply_A_dot(*o.L, o.jac, o.precision, o.ess, x, y, part, stream);
+    }
+    return hm_pcg_operator(o.n, nullptr, nullptr, nullptr, o.L, o.jac, o.precision, o.ess, x, y, stream);
+  }
+  int rc = hm_pcg_operator(o.n, o.indptr, o.indices, o.vals, nullptr, nullptr, HM_FP64, o.ess, x, y, stream);
+  if (rc || !part) return rc;
+  *nparts = kReduceBlocks;
+  k_dot_partial_t<double><<<kReduceBlocks, kReduceThreads, 0, S_(stream)>>>(o.n, x, y, part);
+  return ok_or_cuda();
+}
+
+int op_apply(const PcgOp& o, const float* x, float* y, double* part, int64_t* nparts, void* stream) {
+  if (part) *nparts = hm_apply_dot_parts(*o.L);
+  return hm_launch_apply_A32_dot(*o.L, o.jac, o.ess, x, y, part, stream);
+}
+
+// Jacobi-PCG on vectors of type T from initial guess x; work holds r, z, p, q (T), the
+// p.q partials (n doubles), the scalars and the partials.  Returns HM_OK / HM_ERR_NOCONV.
+template <typename T>
+int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, int maxiter,
+            int check_every, double* wd, T* wt, int* iterations, double* relres, void* stream) {
+  const int64_t n = o.n;
   cudaStream_t s = S_(stream);
-  double* w = static_cast<double*>(work);
-  double* r = w;
-  double* z = w + n;
-  double* p = w + 2 * n;
-  double* q = w + 3 * n;
-  double* pq_part = w + 4 * n;
-  double* sc = w + 5 * n;
+  T* r = wt;
+  T* z = wt + n;
+  T* p = wt + 2 * n;
+  T* q = wt + 3 * n;
+  double* pq_part = wd;
+  double* sc = wd + n;
   double* part = sc + SC_N;
-  int rc = hm_pcg_operator(n, indptr, indices, vals, L, quad, precision, ess, x, q, stream);
+  if (check_every <= 0) check_every = 1;
+  int64_t nparts = 0;
+  int rc = op_apply(o, x, q, nullptr, &nparts, stream);
   if (rc) return rc;
-  k_pcg_init<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, q, diag, r, z, p, part);
+  k_pcg_init<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, q, diag, r, z, p, part);
   k_pcg_init_final<<<1, 1024, 0, s>>>(part, sc, rtol);
   double host[SC_N];
   int it = 0;
@@ -284,25 +426,140 @@ extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indi
     const int stop = it + check_every < maxiter ? it + check_every : maxiter;
     for (; it < stop;) {
       ++it;
-      int64_t nparts = kReduceBlocks;
-      if (L != nullptr) {
-        // the lattice operator sums p.q as it writes q
-        rc = hm_launch_apply_A_dot(*L, const_cast<void*>(quad), precision, ess, p, q, pq_part, stream);
-        nparts = hm_apply_dot_parts(*L);
-      } else {
-        rc = hm_pcg_operator(n, indptr, indices, vals, L, quad, precision, ess, p, q, stream);
-        if (!rc) k_dot_partial<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, p, q, pq_part);
-      }
+      rc = op_apply(o, p, q, pq_part, &nparts, stream);
       if (rc) return rc;
       k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, nparts, sc);
-      k_pcg_update<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, z, p, q, diag, part);
+      k_pcg_update<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, z, p, q, diag, part);
       k_pcg_beta<<<1, 1024, 0, s>>>(part, sc, it);
-      k_pcg_pupdate<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z, p);
+      k_pcg_pupdate<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z, p);
     }
     if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
   }
   const bool conv = host[SC_CONV] >= 0.0;
   if (iterations) *iterations = conv ? (int)host[SC_CONV] : it;
   if (relres) *relres = host[SC_BB] > 0.0 ? std::sqrt(host[SC_RR] / host[SC_BB]) : 0.0;
+  return conv ? HM_OK : HM_ERR_NOCONV;
+}
+
+}  // namespace
+
+extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indices,
+                           const double* vals, const hm::Lattice* L, const void* quad,
+                           int precision, const uint8_t* ess, const double* diag, const double* b,
+                           double* x, double rtol, int maxiter, int check_every, void* work,
+                           int* iterations, double* relres, void* stream) {
+  if (n <= 0 || !diag || !b || !x || !work || maxiter < 0) return HM_ERR_ARG;
+  PcgOp o{n, indptr, indices, vals, L, const_cast<void*>(quad), precision, ess};
+  double* w = static_cast<double*>(work);
+  return pcg_run<double>(o, diag, b, x, rtol, maxiter, check_every, w + 4 * n, w, iterations,
+                         relres, stream);
+}
+
+extern "C" int64_t hm_pcg_mixed_workspace_bytes(int64_t n) {
+  // FP64: r, t, the p.q partials (at most one per node), scalars, partials, b.b;
+  // FP32: x, r, z, p, q of the single-precision recurrence
+  return (int64_t)sizeof(double) * (3 * n + SC_N + 3 * (int64_t)kReduceBlocks + 8) +
+         (int64_t)sizeof(float) * (5 * n + 16);
+}
+
+// Conjugate gradients with reliable updates (Sleijpen & van der Vorst, 1996): the
+// recurrence runs in FP32 (vectors and the FP32 matrix-free operator, sums in FP64) on
+// a system scaled by the residual norm s; when its residual has fallen by `delta` since
+// the last anchor, or it claims convergence, the correction is added to the FP64 x,
+// the true residual b - A64 x replaces the recurrence's (rescaled; the search direction
+// is kept), and the true residual decides convergence.  Goal and stall test follow the
+// reference's refined solves (modeling/PDEVariationalProblem.py:1236-1237, :1299): a
+// residual that no longer halves between anchors is at its rounding floor; it counts as
+// converged within 10 rtol.
+extern "C" int hm_pcg_mixed_impl(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t* ess,
+                                 const double* diag, const double* b, double* x, double rtol,
+                                 double delta, int max_updates, int maxiter, int check_every,
+                                 void* work, int* iterations, int* updates, double* relres,
+                                 void* stream) {
+  if (!L || !jac64 || !jac32 || !diag || !b || !x || !work || max_updates <= 0 || maxiter < 0 ||
+      !(delta > 0.0 && delta < 1.0) || !(rtol >= 0.0))
+    return HM_ERR_ARG;
+  const int64_t n = L->ndof;
+  cudaStream_t s = S_(stream);
+  double* w = static_cast<double*>(work);
+  double* r64 = w;
+  double* t64 = w + n;
+  double* pq_part = w + 2 * n;
+  double* sc = w + 3 * n;
+  double* part = sc + SC_N;
+  double* bbp = part + 3 * kReduceBlocks;
+  float* f32 = reinterpret_cast<float*>(bbp + 8);
+  float* x32 = f32;
+  float* r32 = f32 + n;
+  float* z32 = f32 + 2 * n;
+  float* p32 = f32 + 3 * n;
+  float* q32 = f32 + 4 * n;
+  PcgOp o32{n, nullptr, nullptr, nullptr, L, jac32, HM_FP32, ess};
+  PcgOp o64{n, nullptr, nullptr, nullptr, L, jac64, HM_FP64, ess};
+  if (check_every <= 0) check_every = 1;
+  double h[SC_N];
+  auto read = [&]() -> int {
+    if (cudaMemcpyAsync(h, sc, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HM_ERR_CUDA;
+    return cudaStreamSynchronize(s) == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+  };
+  // the anchor: [x += s x32; t = A64 x]; r = b - t; new scale; FP32 r, z, p from r
+  auto anchor = [&](bool first) -> int {
+    int64_t np = 0;
+    if (!first) {
+      k_mx_accum<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x32, x);
+      const int rc = op_apply(o64, x, t64, nullptr, &np, stream);
+      if (rc) return rc;
+    }
+    k_residual64<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, first ? nullptr : t64, r64, part);
+    k_mx_scale<<<1, 1024, 0, s>>>(part, sc);
+    if (first && cudaMemcpyAsync(bbp, sc + SC_TRUE, sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return HM_ERR_CUDA;
+    k_mx_anchor<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r64, diag, sc, first ? 1 : 0, r32, z32, p32, part);
+    k_mx_anchor_final<<<1, 1024, 0, s>>>(part, sc, bbp, rtol);
+    if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
+    return read();
+  };
+  if (cudaMemsetAsync(sc, 0, sizeof(double) * SC_N, s) != cudaSuccess ||
+      cudaMemsetAsync(x, 0, sizeof(double) * n, s) != cudaSuccess ||
+      cudaMemsetAsync(x32, 0, sizeof(float) * n, s) != cudaSuccess)
+    return HM_ERR_CUDA;
+  int rc = anchor(true);
+  if (rc) return rc;
+  const double bb = h[SC_TRUE];
+  const double tol2 = rtol * rtol * bb, goal2 = 100.0 * tol2;
+  double tr = bb, prev = bb;
+  int it = 0, nup = 0, stalls = 0;
+  bool conv = tr <= tol2;
+  while (!conv) {
+    const int stop = it + check_every < maxiter ? it + check_every : maxiter;
+    int64_t np = 0;
+    for (; it < stop;) {
+      ++it;
+      rc = op_apply(o32, p32, q32, pq_part, &np, stream);
+      if (rc) return rc;
+      k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
+      k_pcg_update<float><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x32, r32, z32, p32, q32, diag, part);
+      k_pcg_beta<<<1, 1024, 0, s>>>(part, sc, it);
+      k_pcg_pupdate<float><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z32, p32);
+    }
+    if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
+    if ((rc = read())) return rc;
+    const bool claim = h[SC_CONV] >= 0.0;
+    if (!claim && h[SC_RR] > delta * delta && it < maxiter) continue;
+    if ((rc = anchor(false))) return rc;
+    ++nup;
+    tr = h[SC_TRUE];
+    if (tr <= tol2) { conv = true; break; }
+    const bool stalled = tr > 0.25 * prev;
+    stalls = stalled ? stalls + 1 : 0;
+    prev = tr;
+    if ((stalled && claim) || stalls >= 2 || it >= maxiter || nup >= max_updates) {
+      conv = tr <= goal2;
+      break;
+    }
+  }
+  if (iterations) *iterations = it;
+  if (updates) *updates = nup;
+  if (relres) *relres = bb > 0.0 ? std::sqrt(tr / bb) : 0.0;
   return conv ? HM_OK : HM_ERR_NOCONV;
 }

@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import check, lib, ptr, stream_ptr
 from .mesh import DirichletBC
 from .pattern import LatticePattern
-from .sparse import CSRBlock, MatrixFreeJacobian, PCGSolver
+from .sparse import CSRBlock, MatrixFreeJacobian, MixedPCGSolver, PCGSolver
 
 STATE, PARAMETER, ADJOINT = 0, 1, 2
 NVAR = 3
@@ -56,10 +56,15 @@ class PDEVariationalProblem:
     check_finite : read the device status word after each assembly and raise
         ``RuntimeError`` on non-finite values (``require_finite_arrays``,
         modeling/PDEVariationalProblem.py:1844-1892); one synchronisation each.
+    solver_precision : ``"fp64"``, or ``"mixed"``: Jacobi-PCG whose recurrence runs in
+        FP32 with the FP32 matrix-free operator, re-anchored to the FP64 true residual
+        each time it falls by ``reliable_delta``, to the same tolerance (in place of the
+        reference's ``_refined_solve``, :1220-1329); implies ``matrix_free_solves``.
     """
 
     def __init__(self, Vh, f=1.0, bc=None, bc0=None, is_fwd_linear=True, solver_tolerance=1e-12,
-                 matrix_free_solves=False, check_finite=True, max_iter=50000):
+                 matrix_free_solves=False, check_finite=True, max_iter=50000,
+                 solver_precision="fp64", reliable_delta=0.1):
         if len(Vh) != NVAR:
             raise ValueError("Vh must have %d entries" % NVAR)
         self.Vh = list(Vh)
@@ -73,7 +78,11 @@ class PDEVariationalProblem:
         if not self.is_fwd_linear:
             raise NotImplementedError("the log-conductivity density is linear in the state")
         self.solver_tolerance = float(solver_tolerance)
-        self.matrix_free_solves = bool(matrix_free_solves)
+        if solver_precision not in ("fp64", "mixed"):
+            raise ValueError("solver_precision must be 'fp64' or 'mixed'")
+        self.solver_precision = solver_precision
+        self.reliable_delta = float(reliable_delta)
+        self.matrix_free_solves = bool(matrix_free_solves) or solver_precision == "mixed"
         self.check_finite = bool(check_finite)
         self.max_iter = int(max_iter)
         self.precision = _lib.HM_FP64
@@ -180,7 +189,7 @@ class PDEVariationalProblem:
             return self._jac_cache[1], self._jac_cache[1]
         quad = self._quadrature([None, m, None], "jacobian")
         A = self._make_jacobian(quad)
-        self._jac_cache = (key, A)
+        self._jac_cache = (key, A, quad)
         self.solver = None
         return A, A
 
@@ -194,6 +203,9 @@ class PDEVariationalProblem:
         return blocks["A"]
 
     def _get_solver(self, A):
+        if self.solver_precision == "mixed":
+            return MixedPCGSolver(A, self._jac_cache[2], rel_tolerance=self.solver_tolerance,
+                                  reliable_delta=self.reliable_delta, max_iter=self.max_iter)
         return PCGSolver(A, rel_tolerance=self.solver_tolerance, max_iter=self.max_iter)
 
     # ---------------------------------------------------------------- solves
@@ -255,7 +267,7 @@ class PDEVariationalProblem:
         self._require_finite("linearization point")
         if need_A:
             A = blocks["A"] if "A" in blocks else self._make_jacobian(quad)
-            self._jac_cache = (_key(m), A)
+            self._jac_cache = (_key(m), A, quad)
             self.solver = None
         self.A, self.At = self._jac_cache[1], self._jac_cache[1]
         self.C = blocks.get("C")

@@ -71,16 +71,18 @@ class MatrixFreeJacobian:
     data (D of the point in the layout the operator streams, plus its scratch); applies
     that share one instance must run in one stream."""
 
-    def __init__(self, mesh, quad, ess_marker, precision=_lib.HM_FP64, stream=None):
+    def __init__(self, mesh, quad, ess_marker, precision=_lib.HM_FP64, stream=None,
+                 quad_precision=None):
         self.mesh, self.ess, self.precision = mesh, ess_marker, precision
+        qp = precision if quad_precision is None else quad_precision
         self.nrow = self.ncol = mesh.ndof
         nbytes = lib.hm_lattice_jacobian_bytes(mesh.handle, precision)
         self.jac = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=mesh.device)
-        check(lib.hm_lattice_jacobian_prepare(mesh.handle, ptr(quad), precision, ptr(self.jac),
+        check(lib.hm_lattice_jacobian_prepare(mesh.handle, ptr(quad), qp, ptr(self.jac), precision,
                                               stream_ptr(stream)), "hm_lattice_jacobian_prepare")
         # the diagonal (Jacobi) is taken now, so the point's quadrature data need not be kept
         self._diag = torch.empty(self.nrow, dtype=torch.float64, device=mesh.device)
-        check(lib.hm_lattice_diag_A(mesh.handle, ptr(quad), precision, ptr(ess_marker),
+        check(lib.hm_lattice_diag_A(mesh.handle, ptr(quad), qp, ptr(ess_marker),
                                     ptr(self._diag), stream_ptr(stream)), "hm_lattice_diag_A")
 
     def mult(self, x, y, stream=None):
@@ -152,4 +154,48 @@ class PCGSolver:
         if rc == _lib.HM_ERR_NOCONV and not self.raise_on_fail:
             return x
         check(rc, "hm_pcg")
+        return x
+
+
+class MixedPCGSolver:
+    """Mixed-precision solve of ``A x = b`` with the lattice's matrix-free Jacobian:
+    conjugate gradients whose recurrence runs in FP32, re-anchored to the FP64 true
+    residual whenever it has fallen by ``reliable_delta`` (``hm_pcg_mixed``).  It takes
+    the place of the reference's refined single-precision solves
+    (modeling/PDEVariationalProblem.py:1220-1329) with the same goal and stall rule.
+    ``operator`` is the FP64 ``MatrixFreeJacobian``; the FP32 operator is derived from
+    the same point."""
+
+    def __init__(self, operator, quad, rel_tolerance=1e-12, reliable_delta=0.1,
+                 max_updates=200, max_iter=20000, check_every=16, raise_on_fail=True):
+        if not isinstance(operator, MatrixFreeJacobian):
+            raise TypeError("the mixed-precision solve needs the matrix-free Jacobian")
+        self.op = operator
+        self.op32 = MatrixFreeJacobian(operator.mesh, quad, operator.ess, _lib.HM_FP32,
+                                       quad_precision=operator.precision)
+        self.parameters = {"rel_tolerance": float(rel_tolerance),
+                           "reliable_delta": float(reliable_delta),
+                           "max_updates": int(max_updates), "max_iter": int(max_iter),
+                           "check_every": int(check_every)}
+        self.raise_on_fail = raise_on_fail
+        self.diag = operator.diagonal()
+        nbytes = lib.hm_pcg_mixed_workspace_bytes(operator.nrow)
+        self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64,
+                                device=operator.mesh.device)
+        self.last = None
+        self.last_updates = 0
+
+    def solve(self, x, b, stream=None):
+        op, prm = self.op, self.parameters
+        it, nup, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        rc = lib.hm_pcg_mixed(op.mesh.handle, ptr(op.jac), ptr(self.op32.jac), ptr(op.ess),
+                              ptr(self.diag), ptr(b), ptr(x), prm["rel_tolerance"],
+                              prm["reliable_delta"], prm["max_updates"], prm["max_iter"],
+                              prm["check_every"], ptr(self.work), ctypes.byref(it),
+                              ctypes.byref(nup), ctypes.byref(rr), stream_ptr(stream))
+        self.last = PCGResult(it.value, rr.value, rc == _lib.HM_OK)
+        self.last_updates = nup.value
+        if rc == _lib.HM_ERR_NOCONV and not self.raise_on_fail:
+            return x
+        check(rc, "hm_pcg_mixed")
         return x

@@ -131,8 +131,8 @@ int hm_lattice_assemble(const hm_lattice* h, const void* d_quad, int precision,
  * hm_lattice_jacobian_prepare from the quadrature data, and the operator's own scratch:
  * two applies with the same d_jac must not overlap on the GPU. */
 int64_t hm_lattice_jacobian_bytes(const hm_lattice* h, int precision);
-int hm_lattice_jacobian_prepare(const hm_lattice* h, const void* d_quad, int precision,
-                                void* d_jac, void* stream);
+int hm_lattice_jacobian_prepare(const hm_lattice* h, const void* d_quad, int quad_precision,
+                                void* d_jac, int precision, void* stream);
 int hm_lattice_apply_A(const hm_lattice* h, void* d_jac, int precision, const uint8_t* d_ess,
                        const double* d_x, double* d_y, void* stream);
 /* diagonal of A(D) (eliminated rows: 1), for Jacobi preconditioning */
@@ -188,6 +188,26 @@ int hm_pcg(int64_t n, const int32_t* d_indptr, const int32_t* d_indices,
            int precision, const uint8_t* d_ess, const double* d_diag, const double* d_b,
            double* d_x, double rtol, int maxiter, int check_every, void* d_work,
            int* iterations, double* relres, void* stream);
+
+/* Mixed-precision solve of A x = b on the lattice: conjugate gradients with reliable
+ * updates.  The Jacobi-preconditioned recurrence runs in FP32 (FP32 operator d_jac32,
+ * FP32 vectors, sums accumulated in FP64); whenever its residual has fallen by the
+ * factor delta (0 < delta < 1, e.g. 0.1) since the last anchor, or it claims
+ * convergence, the correction is added to the FP64 x and the true residual b - A x of
+ * the FP64 operator d_jac64 replaces the recurrence's, the search direction kept.
+ * Converged when ||b - A x||_2 <= rtol ||b||_2; a true residual that stops halving
+ * between anchors (its rounding floor) ends the solve, converged if within 10 rtol.
+ * x starts from zero.  The mixed-precision route of the reference's solves
+ * (_refined_solve, modeling/PDEVariationalProblem.py:1220-1329, a single-precision
+ * hypre inside FP64 refinement), here without restarting the Krylov space.
+ * *iterations counts FP32 iterations, *updates the anchors.
+ * d_work: hm_pcg_mixed_workspace_bytes(n).  HM_ERR_NOCONV after maxiter iterations or
+ * max_updates anchors. */
+int64_t hm_pcg_mixed_workspace_bytes(int64_t n);
+int hm_pcg_mixed(const hm_lattice* lattice, void* d_jac64, void* d_jac32, const uint8_t* d_ess,
+                 const double* d_diag, const double* d_b, double* d_x, double rtol,
+                 double delta, int max_updates, int maxiter, int check_every, void* d_work,
+                 int* iterations, int* updates, double* relres, void* stream);
 
 /* deterministic FP64 dot product into *d_out (a fixed-order two-pass reduction) */
 int64_t hm_dot_workspace_bytes(int64_t n);
