@@ -3,20 +3,9 @@
 //   k_pattern_*     the CSR graph (diagonal first), the entry->slot map and the
 //                   transpose map of a Q2 x Q2 block, arithmetically
 //   k_quad          pointwise data D, E = D grad u, F = D grad p, W = D grad u.grad p
-//   k_tile_assemble the fused assembly: every CSR value of A, C, Wum, Wmm and the
-//                   three assembled vectors, each written exactly once
-//   k_tile_apply_A  the matrix-free Jacobian apply
-//
-// The assembly is output-stationary.  On a uniform lattice every block is a sum of
-// separable terms over the global quadrature lattice, e.g.
-//     A(n, j) = sum_g D(g) sum_d  T_d,x(g_x; n_x, j_x) T_d,y(...) T_d,z(...)
-// with 1D pair tables T (B B, B' B', B' B) that vanish unless the row and column
-// nodes share an element.  A CTA owns a 4 x 4 x 4 tile of node rows, stages the
-// pointwise data of the 3 x 3 x 3 elements around it in shared memory, contracts the
-// three axes one after the other (sum factorisation over the tile's 16 ordered 1D
-// pairs per axis) and streams the finished rows out in CSR order.  No atomics, no
-// colouring, no slot map: every value is summed in registers in a fixed order and
-// stored once, so the assembly is bit-reproducible by construction.
+//   k_elem_apply,   the matrix-free Jacobian apply
+//   k_node_gather
+// (the fused assembly k_tile_assemble is in hm_tile.cu)
 #include <cstdio>
 
 #include "hm_common.cuh"
@@ -189,493 +178,6 @@ __global__ void __launch_bounds__(216) k_quad(Lattice L, const double* __restric
   const bool finite = isfinite(D) && isfinite(E[0]) && isfinite(E[1]) && isfinite(E[2]) &&
                       isfinite(F[0]) && isfinite(F[1]) && isfinite(F[2]) && isfinite(W);
   if (!finite) atomicOr(status, HM_STATUS_NONFINITE);
-}
-
-// ================================================================ tile assembly
-// Position of every (p1, p2, p3) output of an interior tile (no stencil clipped) in the
-// tile's CSR-ordered output: runs (r2, r3) of four consecutive rows r1, each row
-// diagonal first and then its columns ascending (z, then y, then x rank).
-struct TileTabs {
-  uint16_t inv[16][16][16];  // [p3][p2][p1] -> position in the tile output
-  uint16_t runoff[17];       // start of run r2 + 4 r3
-};
-HM_HD constexpr TileTabs make_tile_tabs() {
-  TileTabs t{};
-  int off = 0;
-  for (int run = 0; run < 16; ++run) {
-    const int r2 = run & 3, r3 = run >> 2;
-    t.runoff[run] = (uint16_t)off;
-    const int n2 = row_stencil(r2), n3 = row_stencil(r3);
-    const int d2 = (r2 & 1) ? 1 : 2, d3 = (r3 & 1) ? 1 : 2;
-    for (int r1 = 0; r1 < 4; ++r1) {
-      const int n1 = row_stencil(r1), d1 = (r1 & 1) ? 1 : 2;
-      const int kd = (d3 * n2 + d2) * n1 + d1;
-      for (int k3 = 0; k3 < n3; ++k3)
-        for (int k2 = 0; k2 < n2; ++k2)
-          for (int k1 = 0; k1 < n1; ++k1) {
-            const int rank = (k3 * n2 + k2) * n1 + k1;
-            const int pos = rank == kd ? 0 : (rank < kd ? rank + 1 : rank);
-            t.inv[row_pair_base(r3) + k3][row_pair_base(r2) + k2][row_pair_base(r1) + k1] =
-                (uint16_t)(off + pos);
-          }
-      off += n1 * n2 * n3;
-    }
-  }
-  t.runoff[16] = (uint16_t)off;
-  return t;
-}
-__device__ const TileTabs kTileTabs = make_tile_tabs();
-
-// Strides of the stage buffers: the p3 stride is 9 (mod 16) doubles, so the 16 lanes of
-// a half-warp (9 consecutive g1 of one p3 and 7 of the next, or 16 p2 of one p3) hit 16
-// distinct 8-byte bank pairs.
-constexpr int kT1P = 89;    // T1[p3 * kT1P + g2 * 9 + g1]
-constexpr int kT2P = 153;   // T2[p3 * kT2P + p2 * 9 + g1]
-
-// O is swizzled: position j lives at j ^ ((j >> 4) & 15), a permutation inside each
-// aligned group of 16, so the contiguous copy-out stays conflict-free and the scattered
-// stage-3 stores spread over the banks.
-HM_HD int oswz(int j) { return j ^ ((j >> 4) & 15); }
-
-template <typename real>
-struct TileSmem {
-  real W[8][9][9][9];      // pointwise data of the 27 halo'd elements on the 9^3 Gauss lattice
-  real T1[16 * kT1P];      // after the z contraction
-  real T2[16 * kT2P];      // after the y contraction
-  real O[4096];            // the tile's rows of one block, CSR-ordered (run-major), swizzled
-  int32_t rowptr[4][4][4]; // CSR offsets of the owned rows [r3][r2][r1]
-  int32_t rowoff[4][4][4]; // offsets of the rows in O (tiles with clipped stencils)
-  int32_t runoff[17];      // offsets of the runs in O
-  uint8_t ess[7][7][7];    // Dirichlet markers of the halo'd nodes [s3][s2][s1]
-  int8_t nst[3][4];        // stencil size of each owned row, per axis (0: no row)
-  int8_t clip[3][4];       // columns clipped at the low end of that stencil
-  int8_t dk[3][4];         // the row's own place in its (clipped) stencil
-};
-
-struct TileCtx {
-  int t1, t2, t3;      // tile coordinates
-  int vl[3];           // bit l set: halo'd element l is inside the mesh, per axis
-  bool clipped;        // some owned row has a clipped stencil or lies outside the mesh
-  bool has_ess;        // some halo'd node is a Dirichlet node
-};
-
-// The stages are instantiated once per 1D table and not inlined: the blocks share
-// them, which keeps the kernel's code small enough for the instruction cache.
-
-// stage 1: contract the z axis of one weight with table TZ -> T1
-template <int TZ, typename real>
-__device__ __noinline__ void stage1(const real* __restrict__ Wc, real* __restrict__ T1) {
-  for (int task = threadIdx.x; task < 81; task += blockDim.x) {
-    const int g1 = task % 9, g2 = task / 9;
-    real w[9];
-#pragma unroll
-    for (int l = 0; l < 9; ++l) w[l] = Wc[(l * 9 + g2) * 9 + g1];
-#pragma unroll
-    for (int p = 0; p < 16; ++p) {
-      real acc = 0;
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (t < pair_cnt(p)) acc = fma((real)pair_coef(TZ, p, t), w[pair_g0(p) + t], acc);
-      T1[p * kT1P + g2 * 9 + g1] = acc;
-    }
-  }
-}
-
-// stage 2: contract the y axis with table TY -> T2 = scale * ... (+ T2 when acc)
-template <int TY, typename real>
-__device__ __noinline__ void stage2(const real* __restrict__ T1, real* __restrict__ T2, real scale,
-                                    bool acc_in) {
-  for (int task = threadIdx.x; task < 144; task += blockDim.x) {
-    const int g1 = task % 9, p3 = task / 9;
-    real w[9];
-#pragma unroll
-    for (int l = 0; l < 9; ++l) w[l] = T1[p3 * kT1P + l * 9 + g1];
-    real* out = T2 + p3 * kT2P + g1;
-#pragma unroll
-    for (int p = 0; p < 16; ++p) {
-      real acc = 0;
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (t < pair_cnt(p)) acc = fma((real)pair_coef(TY, p, t), w[pair_g0(p) + t], acc);
-      out[p * 9] = acc_in ? fma(scale, acc, out[p * 9]) : scale * acc;
-    }
-  }
-}
-
-enum BlockKind { BK_A = 0, BK_C = 1, BK_WUM = 2, BK_WMM = 3 };
-// elimination applied by the last stage 3 of a block
-enum Elim { EL_NONE = 0, EL_ROWCOL_DIAG = 1, EL_ROW = 2 };
-
-// Places of outputs (p1 = 0..15, p2, p3) in O for a tile with clipped stencils; -1 if
-// the column lies outside the mesh (or the row does).
-template <typename real>
-__device__ __noinline__ void clipped_positions(const TileSmem<real>& S, int p2, int p3, int* pos) {
-  const int r2 = pair_row_of(p2), r3 = pair_row_of(p3);
-  const int n2 = S.nst[1][r2], n3 = S.nst[2][r3];
-  const int k2 = p2 - row_pair_base(r2) - S.clip[1][r2];
-  const int k3 = p3 - row_pair_base(r3) - S.clip[2][r3];
-  const bool ok23 = n2 > 0 && n3 > 0 && k2 >= 0 && k2 < n2 && k3 >= 0 && k3 < n3;
-#pragma unroll 1
-  for (int p1 = 0; p1 < 16; ++p1) {
-    const int r1 = pair_row_of(p1);
-    const int n1 = S.nst[0][r1];
-    const int k1 = p1 - row_pair_base(r1) - S.clip[0][r1];
-    if (!ok23 || n1 == 0 || k1 < 0 || k1 >= n1) { pos[p1] = -1; continue; }
-    const int rank = (k3 * n2 + k2) * n1 + k1;
-    const int kd = (S.dk[2][r3] * n2 + S.dk[1][r2]) * n1 + S.dk[0][r1];
-    pos[p1] = S.rowoff[r3][r2][r1] + (rank == kd ? 0 : (rank < kd ? rank + 1 : rank));
-  }
-}
-
-// stage 3: contract the x axis with table TX and scatter into the CSR-ordered tile
-// output O (= or +=); with elim the block's folded elimination is applied:
-// EL_ROWCOL_DIAG (A) zeroes rows and columns of Dirichlet nodes and puts 1 on their
-// diagonal, EL_ROW (C, Wum) zeroes their rows.
-template <int TX, typename real>
-__device__ __forceinline__ void stage3_out(TileSmem<real>& S, const TileCtx& c, const real (&w)[9],
-                                           int p2, int p3, int p, int at, bool acc_in, int elim,
-                                           bool check) {
-  real acc = 0;
-#pragma unroll
-  for (int t = 0; t < 6; ++t)
-    if (t < pair_cnt(p)) acc = fma((real)pair_coef(TX, p, t), w[pair_g0(p) + t], acc);
-  if (at < 0) return;
-  at = oswz(at);
-  real v = acc_in ? S.O[at] + acc : acc;
-  if (check) {
-    const int r2 = pair_row_of(p2), r3 = pair_row_of(p3);
-    const bool ress = S.ess[r3 + 2][r2 + 2][pair_row_of(p) + 2] != 0;
-    if (elim == EL_ROWCOL_DIAG) {
-      const bool cess = S.ess[pair_c(p3)][pair_c(p2)][pair_c(p)] != 0;
-      const bool diag = pair_s(p2) == pair_c(p2) && pair_s(p3) == pair_c(p3) && pair_s(p) == pair_c(p);
-      if (ress || cess) v = (ress && diag) ? (real)1 : (real)0;
-    } else if (ress) {
-      v = 0;
-    }
-  }
-  S.O[at] = v;
-}
-
-template <int TX, typename real>
-__device__ __noinline__ void stage3(TileSmem<real>& S, const TileCtx& c, bool acc_in, int elim) {
-  const bool check = elim != EL_NONE && c.has_ess;
-  for (int task = threadIdx.x; task < 256; task += blockDim.x) {
-    const int p2 = task % 16, p3 = task / 16;
-    real w[9];
-#pragma unroll
-    for (int l = 0; l < 9; ++l) w[l] = S.T2[p3 * kT2P + p2 * 9 + l];
-    if (!c.clipped) {
-      const uint4* src = reinterpret_cast<const uint4*>(&kTileTabs.inv[p3][p2][0]);
-      const uint4 a = __ldg(src), b = __ldg(src + 1);
-      const uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-      for (int p = 0; p < 16; ++p)
-        stage3_out<TX>(S, c, w, p2, p3, p, (int)((wv[p >> 1] >> (16 * (p & 1))) & 0xffffu), acc_in,
-                       elim, check);
-    } else {
-      int pos[16];
-      clipped_positions(S, p2, p3, pos);
-#pragma unroll
-      for (int p = 0; p < 16; ++p) stage3_out<TX>(S, c, w, p2, p3, p, pos[p], acc_in, elim, check);
-    }
-  }
-}
-
-// The separable terms of each block; terms that share the x table form one stage-3
-// group, and each group's y/z partial sums are added before the x contraction:
-//   A   = K.M.M/hx^2 (D)  +  M.[K.M/hy^2 + M.K/hz^2] (D)
-//   C   = R.M.M/hx (Ex)   +  M.[R.M/hy (Ey) + M.R/hz (Ez)]
-//   Wum = C with F in place of E
-//   Wmm = M.M.M (W)
-// (tables as x.y.z; the weights carry w|J| and the physical gradients)
-template <typename real>
-__device__ __forceinline__ void tile_block(int blk, TileSmem<real>& S, const Lattice& L,
-                                           const TileCtx& c) {
-  real* T1 = S.T1;
-  real* T2 = S.T2;
-  if (blk == BK_A) {
-    const real* D = &S.W[0][0][0][0];
-    stage1<TM>(D, T1); __syncthreads();
-    stage2<TM>(T1, T2, (real)(1.0 / (L.hx * L.hx)), false); __syncthreads();
-    stage3<TK>(S, c, false, EL_NONE); __syncthreads();
-    stage2<TK>(T1, T2, (real)(1.0 / (L.hy * L.hy)), false); __syncthreads();
-    stage1<TK>(D, T1); __syncthreads();
-    stage2<TM>(T1, T2, (real)(1.0 / (L.hz * L.hz)), true); __syncthreads();
-    stage3<TM>(S, c, true, EL_ROWCOL_DIAG); __syncthreads();
-  } else if (blk == BK_C || blk == BK_WUM) {
-    const int c0 = blk == BK_C ? 1 : 4;
-    const real* Gx = &S.W[c0][0][0][0];
-    const real* Gy = &S.W[c0 + 1][0][0][0];
-    const real* Gz = &S.W[c0 + 2][0][0][0];
-    stage1<TM>(Gx, T1); __syncthreads();
-    stage2<TM>(T1, T2, (real)(1.0 / L.hx), false); __syncthreads();
-    stage3<TR>(S, c, false, EL_NONE); __syncthreads();
-    stage1<TM>(Gy, T1); __syncthreads();
-    stage2<TR>(T1, T2, (real)(1.0 / L.hy), false); __syncthreads();
-    stage1<TR>(Gz, T1); __syncthreads();
-    stage2<TM>(T1, T2, (real)(1.0 / L.hz), true); __syncthreads();
-    stage3<TM>(S, c, true, EL_ROW); __syncthreads();
-  } else {
-    const real* Wq = &S.W[7][0][0][0];
-    stage1<TM>(Wq, T1); __syncthreads();
-    stage2<TM>(T1, T2, (real)1.0, false); __syncthreads();
-    stage3<TM>(S, c, false, EL_NONE); __syncthreads();
-  }
-}
-
-// Stream the tile's rows of one block out: each run of four consecutive rows is one
-// contiguous stretch of the CSR values and of O; a warp copies a run, lanes on
-// consecutive positions.
-template <typename real>
-__device__ __forceinline__ void tile_write(const TileSmem<real>& S, const TileCtx& c,
-                                           double* __restrict__ vals) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarp = blockDim.x >> 5;
-  for (int run = warp; run < 16; run += nwarp) {
-    const int r2 = run & 3, r3 = run >> 2;
-    const int a = c.clipped ? S.runoff[run] : (int)kTileTabs.runoff[run];
-    const int b = c.clipped ? S.runoff[run + 1] : (int)kTileTabs.runoff[run + 1];
-    if (b <= a) continue;
-    double* dst = vals + (int64_t)S.rowptr[r3][r2][0];
-    for (int j = lane; j < b - a; j += 32) dst[j] = (double)S.O[oswz(a + j)];
-  }
-}
-
-// ------------------------------------------------------------ assembled vectors
-// dR/dp = sum_g E.grad phi - f w|J| phi,  dR/du = sum_g F.grad phi,  dR/dm = sum_g W psi,
-// by the same sum factorisation with single-index tables of the owned rows.
-template <int TZ, typename real>
-__device__ __forceinline__ void vstage1(const real* __restrict__ Wc, real* __restrict__ U1,
-                                        int task, bool wdet, const Lattice& L, const TileCtx& c) {
-  const int g1 = task % 9, g2 = task / 9;
-  real w[9];
-#pragma unroll
-  for (int l = 0; l < 9; ++l) {
-    if (wdet) {
-      const bool in = ((c.vl[0] >> (g1 / 3)) & 1) && ((c.vl[1] >> (g2 / 3)) & 1) && ((c.vl[2] >> (l / 3)) & 1);
-      w[l] = in ? (real)(wq(g1 % 3) * wq(g2 % 3) * wq(l % 3) * L.hx * L.hy * L.hz) : (real)0;
-    } else {
-      w[l] = Wc[(l * 9 + g2) * 9 + g1];
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    real acc = 0;
-#pragma unroll
-    for (int t = 0; t < 6; ++t)
-      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TZ, r, t), w[vrow_g0(r) + t], acc);
-    U1[(r * 9 + g2) * 9 + g1] = acc;
-  }
-}
-
-template <int TY, typename real>
-__device__ __forceinline__ void vstage2(const real* __restrict__ U1, real* __restrict__ U2, int task) {
-  const int g1 = task % 9, r3 = task / 9;
-  real w[9];
-#pragma unroll
-  for (int l = 0; l < 9; ++l) w[l] = U1[(r3 * 9 + l) * 9 + g1];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    real acc = 0;
-#pragma unroll
-    for (int t = 0; t < 6; ++t)
-      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TY, r, t), w[vrow_g0(r) + t], acc);
-    U2[(r3 * 4 + r) * 9 + g1] = acc;
-  }
-}
-
-template <int TX, typename real>
-__device__ __forceinline__ void vstage3(const real* __restrict__ U2, real (&y)[4], int r2, int r3, real scale) {
-  real w[9];
-#pragma unroll
-  for (int l = 0; l < 9; ++l) w[l] = U2[(r3 * 4 + r2) * 9 + l];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    real acc = 0;
-#pragma unroll
-    for (int t = 0; t < 6; ++t)
-      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TX, r, t), w[vrow_g0(r) + t], acc);
-    y[r] = fma(scale, acc, y[r]);
-  }
-}
-
-// the 8 vector terms: (weight, x/y/z tables); term 3 is the source (w|J|, scaled -f)
-struct VTerm { int w, tx, ty, tz; };
-__device__ __constant__ VTerm c_vterms[8] = {
-    {1, VD, VB, VB}, {2, VB, VD, VB}, {3, VB, VB, VD}, {-1, VB, VB, VB},   // dR/dp
-    {4, VD, VB, VB}, {5, VB, VD, VB}, {6, VB, VB, VD},                     // dR/du
-    {7, VB, VB, VB}};                                                       // dR/dm
-
-template <typename real>
-__device__ __forceinline__ void tile_vectors(TileSmem<real>& S, const Lattice& L, const TileCtx& c,
-                                             double f, double* __restrict__ vstate,
-                                             double* __restrict__ vparam,
-                                             double* __restrict__ vadj, bool zero_ess) {
-  real* U1 = S.T1;            // 8 terms x [4][9][9]  (spans T1 and T2)
-  real* U2 = &S.O[0];         // 8 terms x [4][4][9]
-  const int tid = threadIdx.x;
-  for (int task = tid; task < 8 * 81; task += blockDim.x) {
-    const int term = task / 81, tt = task % 81;
-    const VTerm vt = c_vterms[term];
-    const real* Wc = vt.w >= 0 ? &S.W[vt.w][0][0][0] : nullptr;
-    real* out = U1 + term * 324;
-    if (vt.tz == VB) vstage1<VB>(Wc, out, tt, vt.w < 0, L, c);
-    else vstage1<VD>(Wc, out, tt, vt.w < 0, L, c);
-  }
-  __syncthreads();
-  for (int task = tid; task < 8 * 36; task += blockDim.x) {
-    const int term = task / 36, tt = task % 36;
-    const VTerm vt = c_vterms[term];
-    if (vt.ty == VB) vstage2<VB>(U1 + term * 324, U2 + term * 144, tt);
-    else vstage2<VD>(U1 + term * 324, U2 + term * 144, tt);
-  }
-  __syncthreads();
-  // 3 slots x 16 (r2, r3): each sums its terms over r1
-  if (tid < 48) {
-    const int slot = tid / 16, r2 = tid % 4, r3 = (tid / 4) % 4;
-    real y[4] = {0, 0, 0, 0};
-    const int t0 = slot == 0 ? 0 : slot == 1 ? 4 : 7;
-    const int t1 = slot == 0 ? 4 : slot == 1 ? 7 : 8;
-    const real sc[3] = {(real)(1.0 / L.hx), (real)(1.0 / L.hy), (real)(1.0 / L.hz)};
-    for (int term = t0; term < t1; ++term) {
-      const VTerm vt = c_vterms[term];
-      const real scale = term == 3 ? (real)(-f) : term == 7 ? (real)1 : sc[(term - t0) % 3];
-      if (vt.tx == VB) vstage3<VB>(U2 + term * 144, y, r2, r3, scale);
-      else vstage3<VD>(U2 + term * 144, y, r2, r3, scale);
-    }
-    double* dst = slot == 0 ? vadj : slot == 1 ? vstate : vparam;
-    const int gy = 4 * c.t2 + r2, gz = 4 * c.t3 + r3;
-    if (dst != nullptr && gy < L.Ny && gz < L.Nz) {
-#pragma unroll
-      for (int r1 = 0; r1 < 4; ++r1) {
-        const int gx = 4 * c.t1 + r1;
-        if (gx >= L.Nx) continue;
-        double v = (double)y[r1];
-        if (zero_ess && slot != 2 && S.ess[r3 + 2][r2 + 2][r1 + 2]) v = 0.0;
-        dst[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] = v;
-      }
-    }
-  }
-}
-
-template <typename real>
-__device__ __forceinline__ void tile_load(TileSmem<real>& S, const Lattice& L, TileCtx& c,
-                                          const real* __restrict__ quad,
-                                          const uint8_t* __restrict__ ess,
-                                          const int32_t* __restrict__ indptr) {
-  const int tid = threadIdx.x;
-  c.t1 = blockIdx.x; c.t2 = blockIdx.y; c.t3 = blockIdx.z;
-  const int tt[3] = {c.t1, c.t2, c.t3};
-  const int eb[3] = {2 * c.t1 - 1, 2 * c.t2 - 1, 2 * c.t3 - 1};
-  const int ne[3] = {L.nx, L.ny, L.nz};
-  const int Nn[3] = {L.Nx, L.Ny, L.Nz};
-  bool clipped = false;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    c.vl[d] = 0;
-#pragma unroll
-    for (int l = 0; l < 3; ++l)
-      if (eb[d] + l >= 0 && eb[d] + l < ne[d]) c.vl[d] |= 1 << l;
-    // the first tile clips row 0's stencil; the last holds the last node (clipped) and
-    // may hold rows outside the mesh
-    clipped |= tt[d] == 0 || 4 * tt[d] + 4 > Nn[d] - 1;
-  }
-  c.clipped = clipped;
-  // pointwise data: thread (component, point) walks the 27 halo'd elements
-  if (tid < 216) {
-    const int q = tid % 27, comp = tid / 27;
-    real* dst = &S.W[comp][q / 9][(q / 3) % 3][q % 3];
-    const int64_t sy = L.nx, sz = (int64_t)L.nx * L.ny;
-    const int64_t e0 = eb[0] + sy * eb[1] + sz * eb[2];
-    real v[27];
-#pragma unroll
-    for (int l = 0; l < 27; ++l) {
-      const int l1 = l % 3, l2 = (l / 3) % 3, l3 = l / 9;
-      const bool in = ((c.vl[0] >> l1) & 1) && ((c.vl[1] >> l2) & 1) && ((c.vl[2] >> l3) & 1);
-      v[l] = in ? quad[(e0 + l1 + sy * l2 + sz * l3) * 216 + tid] : (real)0;
-    }
-#pragma unroll
-    for (int l = 0; l < 27; ++l) dst[(3 * (l / 9)) * 81 + (3 * ((l / 3) % 3)) * 9 + 3 * (l % 3)] = v[l];
-  }
-  int any = 0;
-  for (int i = tid; i < 343; i += blockDim.x) {
-    const int s1 = i % 7, s2 = (i / 7) % 7, s3 = i / 49;
-    const int gx = 4 * c.t1 - 2 + s1, gy = 4 * c.t2 - 2 + s2, gz = 4 * c.t3 - 2 + s3;
-    uint8_t m = 0;
-    if (ess != nullptr && gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 && gz < L.Nz)
-      m = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
-    S.ess[s3][s2][s1] = m;
-    any |= m;
-  }
-  if (indptr != nullptr && tid < 64) {
-    const int r1 = tid % 4, r2 = (tid / 4) % 4, r3 = tid / 16;
-    const int gx = 4 * c.t1 + r1, gy = 4 * c.t2 + r2, gz = 4 * c.t3 + r3;
-    int32_t v = 0;
-    if (gx < L.Nx && gy < L.Ny && gz < L.Nz) v = indptr[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
-    S.rowptr[r3][r2][r1] = v;
-  }
-  if (clipped && tid < 12) {
-    // per axis and owned row: clipped stencil size, low-end clip, own place
-    const int d = tid / 4, r = tid % 4;
-    const int g = 4 * tt[d] + r;
-    if (g < Nn[d]) {
-      const int lo = stencil_lo(g);
-      S.nst[d][r] = (int8_t)stencil_n(g, Nn[d]);
-      S.clip[d][r] = (int8_t)(lo - (4 * tt[d] - 2 + row_col_start(r)));
-      S.dk[d][r] = (int8_t)(g - lo);
-    } else {
-      S.nst[d][r] = 0; S.clip[d][r] = 0; S.dk[d][r] = 0;
-    }
-  }
-  c.has_ess = __syncthreads_or(any) != 0;
-  if (clipped && tid < 16) {
-    // O layout of a clipped tile: run r2 + 4 r3, rows r1 inside, clipped lengths
-    const int r2 = tid & 3, r3 = tid >> 2;
-    int off = 0;
-    for (int run = 0; run < tid; ++run) {
-      const int a2 = run & 3, a3 = run >> 2;
-      for (int r1 = 0; r1 < 4; ++r1) off += S.nst[0][r1] * S.nst[1][a2] * S.nst[2][a3];
-    }
-    S.runoff[tid] = off;
-    for (int r1 = 0; r1 < 4; ++r1) {
-      S.rowoff[r3][r2][r1] = off;
-      off += S.nst[0][r1] * S.nst[1][r2] * S.nst[2][r3];
-    }
-    if (tid == 15) S.runoff[16] = off;
-  }
-  __syncthreads();
-}
-
-struct AssembleOut {
-  double* vals[4];
-  double* vec_state;
-  double* vec_param;
-  double* vec_adj;
-  double f;
-  int zero_ess;
-};
-
-// The fused assembly: one CTA per tile of 4 x 4 x 4 node rows, all pointwise data of
-// the 27 halo'd elements resident, the blocks one after the other, each streamed out
-// as soon as it is complete, then the vectors.
-template <typename real>
-__global__ void __launch_bounds__(256, 2)
-    k_tile_assemble(Lattice L, const real* __restrict__ quad, const uint8_t* __restrict__ ess,
-                    const int32_t* __restrict__ indptr, AssembleOut o) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  TileSmem<real>& S = *reinterpret_cast<TileSmem<real>*>(smem_raw);
-  TileCtx c;
-  tile_load(S, L, c, quad, ess, indptr);
-#pragma unroll 1
-  for (int blk = 0; blk < 4; ++blk) {
-    if (o.vals[blk] == nullptr) continue;
-    tile_block(blk, S, L, c);
-    tile_write(S, c, o.vals[blk]);
-  }
-  if (o.vec_state || o.vec_param || o.vec_adj) {
-    __syncthreads();
-    tile_vectors(S, L, c, o.f, o.vec_state, o.vec_param, o.vec_adj, o.zero_ess != 0);
-  }
 }
 
 // ====================================================== matrix-free Jacobian apply
@@ -941,34 +443,6 @@ int hm_launch_quad(const Lattice& L, const double* u, const double* m, const dou
   else
     k_quad<double><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, (double*)quad, status);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
-}
-
-template <typename real>
-static int launch_assemble_t(const Lattice& L, const void* quad, const int32_t* indptr,
-                             const uint8_t* ess, const AssembleOut& o, void* stream) {
-  const size_t smem = sizeof(TileSmem<real>);
-  static bool configured[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !configured[dev]) {
-    if (cudaFuncSetAttribute(k_tile_assemble<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-      return HM_ERR_CUDA;
-    configured[dev] = true;
-  }
-  dim3 grid(L.tx, L.ty, L.tz);
-  k_tile_assemble<real><<<grid, 256, smem, S_(stream)>>>(L, (const real*)quad, ess, indptr, o);
-  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
-}
-
-int hm_launch_assemble(const Lattice& L, const void* quad, int precision, const int32_t* indptr,
-                       const uint8_t* ess, double f, double* vA, double* vC, double* vWum,
-                       double* vWmm, double* vs, double* vp, double* va, int zero_ess, void* stream) {
-  AssembleOut o;
-  o.vals[0] = vA; o.vals[1] = vC; o.vals[2] = vWum; o.vals[3] = vWmm;
-  o.vec_state = vs; o.vec_param = vp; o.vec_adj = va; o.f = f; o.zero_ess = zero_ess;
-  if (precision == HM_FP32) return launch_assemble_t<float>(L, quad, indptr, ess, o, stream);
-  return launch_assemble_t<double>(L, quad, indptr, ess, o, stream);
 }
 
 int hm_launch_jacobian_prepare(const Lattice& L, const void* quad, int quad_precision, void* jac,

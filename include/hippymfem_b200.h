@@ -39,6 +39,7 @@ extern "C" {
 /* bits of the device status word */
 #define HM_STATUS_NONFINITE 1u
 #define HM_STATUS_RANGE 2u
+#define HM_STATUS_TIMEOUT 4u  /* a bounded wait in a kernel gave up: its outputs are invalid */
 
 /* arithmetic of the element contractions; CSR values are always FP64 */
 #define HM_FP64 0
@@ -46,6 +47,12 @@ extern "C" {
 
 const char* hm_error_string(int code);
 int hm_version(void);
+
+/* The library's own device status word on the current device: bits (HM_STATUS_*) that
+ * kernels without a d_status argument set -- HM_STATUS_TIMEOUT when the assembly's
+ * wait for its staged data gave up.  Synchronises the device; with clear != 0 the word
+ * is reset.  No counterpart in the reference (its host kernels cannot time out). */
+int hm_device_status(uint32_t* out, int clear);
 
 /* ------------------------------------------------------------------ sparsity pattern
  * hm_pattern_build: CSR graph and entry->slot map of the element-assembly map of one
