@@ -31,17 +31,25 @@ __device__ unsigned int g_device_status = 0;
 // ------------------------------------------------------------------ tile tables
 // Position of every (p1, p2, p3) output of an interior tile (no stencil clipped) in the
 // tile's CSR-ordered image: runs (r2, r3) of four consecutive rows r1, each row
-// diagonal first and then its columns ascending (z, then y, then x rank).
-struct TileTabs {
+// diagonal first and then its columns ascending (z, then y, then x rank).  Runs start
+// after an even pad (chosen to spread the image stores over the shared-memory banks;
+// at least 2 after the first run), and a tile may shift a run by one more slot so that
+// it has the parity of its CSR offset (the bulk copy-out wants 16-byte alignment on
+// both sides) without reaching the next run.
+constexpr int kRunPad[16] = {10, 10, 14, 10, 10, 2, 8, 2, 2, 10, 14, 10, 4, 6, 2, 12};
+struct alignas(16) TileTabs {
   uint16_t inv[16][16][16];  // [p3][p2][p1] -> position in the tile image
-  uint16_t runoff[17];       // start of run r2 + 4 r3
+  uint16_t runoff[16];       // start of run r2 + 4 r3 (before the tile's parity shift)
+  uint16_t runlen[16];       // its length
 };
 HM_HD constexpr TileTabs make_tile_tabs() {
   TileTabs t{};
   int off = 0;
   for (int run = 0; run < 16; ++run) {
     const int r2 = run & 3, r3 = run >> 2;
+    off += kRunPad[run];
     t.runoff[run] = (uint16_t)off;
+    const int start = off;
     const int n2 = row_stencil(r2), n3 = row_stencil(r3);
     const int d2 = (r2 & 1) ? 1 : 2, d3 = (r3 & 1) ? 1 : 2;
     for (int r1 = 0; r1 < 4; ++r1) {
@@ -57,18 +65,29 @@ HM_HD constexpr TileTabs make_tile_tabs() {
           }
       off += n1 * n2 * n3;
     }
+    t.runlen[run] = (uint16_t)(off - start);
   }
-  t.runoff[16] = (uint16_t)off;
   return t;
 }
 __device__ const TileTabs kTileTabs = make_tile_tabs();
+HM_HD constexpr int run_pad_total() {
+  int s = 0;
+  for (int i = 0; i < 16; ++i) s += kRunPad[i];
+  return s;
+}
+HM_HD constexpr bool run_pads_ok() {
+  for (int i = 1; i < 16; ++i)
+    if (kRunPad[i] < 2 || (kRunPad[i] & 1)) return false;
+  return (kRunPad[0] & 1) == 0;
+}
+static_assert(run_pads_ok(), "even pads, at least 2 between runs");
 
 // Geometry of the field buffers.  A phase's TMA box is [ez 3][ey 3][ex 3][BI] reals:
 // BI consecutive reals of each element's 216 (8 fields x 27 points) from x0 on, which
 // covers the phase's (up to) three fields; x0 keeps the copy 16-byte aligned and the
 // fields start `off` reals into each element's row.
 template <typename real> struct TileCfg;
-template <> struct TileCfg<double> { static constexpr int BI = 82, AL = 2; };
+template <> struct TileCfg<double> { static constexpr int BI = 86, AL = 2; };
 template <> struct TileCfg<float> { static constexpr int BI = 84, AL = 4; };
 
 enum Phase { PH_A = 0, PH_C = 1, PH_WUM = 2, PH_WMM = 3 };
@@ -84,17 +103,19 @@ template <typename real> HM_HD constexpr int phase_off(int ph) {
 // a half-warp (9 consecutive g1 of one p3 and 7 of the next) hit 16 distinct banks.
 constexpr int kT1P = 89;    // T1[p3 * kT1P + g2 * 9 + g1]
 constexpr int kT2P = 153;   // T2[p3 * kT2P + p2 * 9 + g1]
-constexpr int kImage = 4096;  // reals of a tile image; position kImage is the sink
+constexpr int kSink = 16 * kT1P * 3 - 1;   // the image's sink slot (outputs outside the mesh)
+static_assert(4096 + run_pad_total() + 16 <= kSink, "the padded image fits in T1");
 
 template <typename real>
 struct TileSmem {
   static constexpr int kBuf = ((27 * TileCfg<real>::BI * (int)sizeof(real) + 127) / 128) * 128;
   unsigned char wbuf[2][kBuf];   // the two field buffers (TMA destinations)
-  real T1[3][16 * kT1P];         // z-contracted; the tile image (kImage + 1) aliases it
+  real T1[3][16 * kT1P];         // z-contracted; the tile image (to kSink) aliases it
   real T2[2][16 * kT2P];         // y-contracted; the vector scratch aliases it
   unsigned long long mbar[2];    // completion of the two buffers' copies
   int32_t rowptr[16];            // CSR offset of row (0, r2, r3), [r2 + 4 r3]
-  int32_t runoff[17];            // image offsets of the runs (clipped tiles)
+  int32_t runstart[16];          // image offset of each run
+  int32_t runlen[16];            // and its length
   int32_t rowoff[64];            // image offsets of the rows (clipped tiles)
   uint8_t ess[7][7][7];          // Dirichlet markers of the halo'd nodes [s3][s2][s1]
   int8_t nst[3][4];              // stencil size of each owned row, per axis (0: no row)
@@ -102,7 +123,6 @@ struct TileSmem {
   int8_t dk[3][4];               // the row's own place in its (clipped) stencil
 };
 static_assert(sizeof(TileSmem<double>) <= 113 * 1024, "two CTAs per SM");
-static_assert(16 * kT1P * 3 >= kImage + 1, "the image fits in T1");
 
 // ------------------------------------------------------------- TMA + mbarrier
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -149,6 +169,19 @@ __device__ __forceinline__ void issue_fields(const CUtensorMap* tmap, TileSmem<r
       "r"(smem_u32(b))
       : "memory");
 }
+
+// bulk copy of a stretch of the image to global memory (both ends 16-byte aligned,
+// size a multiple of 16), and the waits on this thread's copies
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
+               "r"(smem_u32(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // ------------------------------------------------------------ 1D contractions
 // sum over pair p's support of table TAB times the window w (zero coefficients skipped)
@@ -254,31 +287,43 @@ __device__ __forceinline__ void x_task(const real* __restrict__ row1, const real
 
 // ------------------------------------------------------------ vector stages
 // dR/dp = sum_g E.grad phi - f w|J| phi,  dR/du = sum_g F.grad phi,  dR/dm = sum_g W psi,
-// by the same sum factorisation with single-index tables of the owned rows.
-// Terms of a phase: (field or -1 for the weights alone, x/y/z tables)
-struct VTerm { int f, tx, ty, tz; };
-HM_HD constexpr int phase_nterms(int ph) { return ph == PH_C ? 4 : ph == PH_WUM ? 3 : ph == PH_WMM ? 1 : 0; }
-HM_HD constexpr VTerm phase_term(int ph, int j) {
-  return ph == PH_WMM ? VTerm{0, VB, VB, VB}
-       : j == 0 ? VTerm{0, VD, VB, VB}
-       : j == 1 ? VTerm{1, VB, VD, VB}
-       : j == 2 ? VTerm{2, VB, VB, VD}
-                : VTerm{-1, VB, VB, VB};
+// by the same sum factorisation with single-index tables of the owned rows.  The terms
+// of a phase: field j with table VD on axis j (the gradient terms of C and Wum phases),
+// or VB everywhere (Wmm).  The source term -f w|J| phi separates into three 1D sums.
+template <int PH> HM_HD constexpr int vec_nterms() { return PH == PH_WMM ? 1 : 3; }
+template <int PH, int J, int AXIS> HM_HD constexpr int vec_tab() {
+  return PH == PH_WMM ? VB : (J == AXIS ? VD : VB);
 }
 
-template <int TZ, typename real>
-__device__ __forceinline__ void v1_task(const real (&w)[9], real* __restrict__ u1) {
+// z: the (g1, g2) column of field J -> U1[J][r3][g2][g1]
+template <int PH, int J, int BI, typename real>
+__device__ __forceinline__ void vz_task(const real* __restrict__ col, real* __restrict__ u1) {
+  real w[9];
+#pragma unroll
+  for (int g = 0; g < 9; ++g) w[g] = col[(g / 3) * 9 * BI + (g % 3) * 9];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     real acc = 0;
 #pragma unroll
     for (int t = 0; t < 6; ++t)
-      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TZ, r, t), w[vrow_g0(r) + t], acc);
+      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(vec_tab<PH, J, 2>(), r, t), w[vrow_g0(r) + t], acc);
     u1[r * 81] = acc;
   }
 }
-template <int TY, typename real>
-__device__ __forceinline__ void v2_task(const real* __restrict__ u1, real* __restrict__ u2) {
+template <int PH, int BI, typename real>
+__device__ __forceinline__ void vec_z(const real* __restrict__ W, real* __restrict__ U1, int tid) {
+  if (tid >= 81 * vec_nterms<PH>()) return;
+  const int j = tid / 81, i = tid % 81;
+  const int g1 = i % 9, g2 = i / 9;
+  const real* col = W + 27 * j + ((g2 / 3) * 3 + g1 / 3) * BI + g1 % 3 + 3 * (g2 % 3);
+  real* u1 = U1 + j * 324 + g2 * 9 + g1;
+  if (j == 0) vz_task<PH, 0, BI>(col, u1);
+  else if (j == 1) vz_task<PH, 1, BI>(col, u1);
+  else vz_task<PH, 2, BI>(col, u1);
+}
+// y: (g1, r3) of term J -> U2[J][r3][r2][g1]
+template <int PH, int J, typename real>
+__device__ __forceinline__ void vy_task(const real* __restrict__ u1, real* __restrict__ u2) {
   real w[9];
 #pragma unroll
   for (int l = 0; l < 9; ++l) w[l] = u1[l * 9];
@@ -287,23 +332,64 @@ __device__ __forceinline__ void v2_task(const real* __restrict__ u1, real* __res
     real acc = 0;
 #pragma unroll
     for (int t = 0; t < 6; ++t)
-      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TY, r, t), w[vrow_g0(r) + t], acc);
+      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(vec_tab<PH, J, 1>(), r, t), w[vrow_g0(r) + t], acc);
     u2[r * 9] = acc;
   }
 }
-template <int TX, typename real>
-__device__ __forceinline__ void v3_task(const real* __restrict__ u2, real (&y)[4], real scale) {
-  real w[9];
+template <int PH, typename real>
+__device__ __forceinline__ void vec_y(const real* __restrict__ U1, real* __restrict__ U2, int tid) {
+  if (tid >= 36 * vec_nterms<PH>()) return;
+  const int j = tid / 36, i = tid % 36;
+  const int g1 = i % 9, r3 = i / 9;
+  const real* u1 = U1 + j * 324 + r3 * 81 + g1;
+  real* u2 = U2 + j * 144 + r3 * 36 + g1;
+  if (j == 0) vy_task<PH, 0>(u1, u2);
+  else if (j == 1) vy_task<PH, 1>(u1, u2);
+  else vy_task<PH, 2>(u1, u2);
+}
+// x: output row r1 of (r2, r3): sum of the terms, scaled, plus the source
+template <int PH, int J, int R1, typename real>
+__device__ __forceinline__ real vx_term(const real* __restrict__ u2) {
+  real acc = 0;
 #pragma unroll
-  for (int l = 0; l < 9; ++l) w[l] = u2[l];
+  for (int t = 0; t < 6; ++t)
+    if (t < vrow_cnt(R1)) acc = fma((real)vrow_coef(vec_tab<PH, J, 0>(), R1, t), u2[vrow_g0(R1) + t], acc);
+  return acc;
+}
+// sum_t B(r, g0 + t) w(g0 + t) over the points of elements inside the mesh (bits vl)
+template <int R, typename real>
+__device__ __forceinline__ real src_1d(int vl) {
+  real acc = 0;
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    real acc = 0;
-#pragma unroll
-    for (int t = 0; t < 6; ++t)
-      if (t < vrow_cnt(r)) acc = fma((real)vrow_coef(TX, r, t), w[vrow_g0(r) + t], acc);
-    y[r] = fma(scale, acc, y[r]);
+  for (int t = 0; t < 6; ++t)
+    if (t < vrow_cnt(R) && ((vl >> ((vrow_g0(R) + t) / 3)) & 1))
+      acc = fma((real)vrow_coef(VB, R, t), (real)wq((vrow_g0(R) + t) % 3), acc);
+  return acc;
+}
+template <typename real>
+__device__ __forceinline__ real src_1d_rt(int r, int vl) {
+  return r == 0 ? src_1d<0, real>(vl) : r == 1 ? src_1d<1, real>(vl) : r == 2 ? src_1d<2, real>(vl)
+                                                                              : src_1d<3, real>(vl);
+}
+template <int PH, int R1, typename real>
+__device__ __forceinline__ real vx_row(const real* __restrict__ U2, int r2, int r3, real ihx,
+                                       real ihy, real ihz) {
+  const int o = r3 * 36 + r2 * 9;
+  if constexpr (PH == PH_WMM) {
+    return vx_term<PH, 0, R1>(U2 + o);
+  } else {
+    real y = ihx * vx_term<PH, 0, R1>(U2 + o);
+    y = fma(ihy, vx_term<PH, 1, R1>(U2 + 144 + o), y);
+    return fma(ihz, vx_term<PH, 2, R1>(U2 + 288 + o), y);
   }
+}
+template <int PH, typename real>
+__device__ __forceinline__ real vec_x(const real* __restrict__ U2, int r1, int r2, int r3, real ihx,
+                                      real ihy, real ihz) {
+  return r1 == 0 ? vx_row<PH, 0>(U2, r2, r3, ihx, ihy, ihz)
+       : r1 == 1 ? vx_row<PH, 1>(U2, r2, r3, ihx, ihy, ihz)
+       : r1 == 2 ? vx_row<PH, 2>(U2, r2, r3, ihx, ihy, ihz)
+                 : vx_row<PH, 3>(U2, r2, r3, ihx, ihy, ihz);
 }
 
 struct AssembleOut {
@@ -394,18 +480,30 @@ __global__ void __launch_bounds__(256, 2)
     }
   }
   const bool has_ess = __syncthreads_or(any) != 0;
-  if (clipped && tid < 16) {
-    // image layout of a clipped tile: run r2 + 4 r3, its rows r1, clipped lengths
-    const int r2 = tid & 3, r3 = tid >> 2;
-    int off = 0;
-    for (int run = 0; run < tid; ++run)
-      for (int r1 = 0; r1 < 4; ++r1) off += S.nst[0][r1] * S.nst[1][run & 3] * S.nst[2][run >> 2];
-    S.runoff[tid] = off;
-    for (int r1 = 0; r1 < 4; ++r1) {
-      S.rowoff[tid * 4 + r1] = off;
-      off += S.nst[0][r1] * S.nst[1][r2] * S.nst[2][r3];
+  // image layout: run starts (with the parity of the run's CSR offset when the copy-out
+  // is a bulk copy) and lengths; a clipped tile packs its clipped rows
+  constexpr bool kBulk = sizeof(real) == 8;
+  if (tid < 16) {
+    const int run = tid;
+    const int want = kBulk ? (S.rowptr[run] & 1) : 0;
+    if (!clipped) {
+      const int a0 = kTileTabs.runoff[run];
+      S.runstart[run] = a0 + ((want - a0) & 1);
+      S.runlen[run] = kTileTabs.runlen[run];
+    } else {
+      int off = 0;
+      for (int q = 0; q <= run; ++q) {
+        const int wq_ = kBulk ? (S.rowptr[q] & 1) : 0;
+        off += (wq_ - off) & 1;
+        int len = 0;
+        for (int r1 = 0; r1 < 4; ++r1) {
+          if (q == run) S.rowoff[run * 4 + r1] = off + len;
+          len += S.nst[0][r1] * S.nst[1][q & 3] * S.nst[2][q >> 2];
+        }
+        if (q == run) { S.runstart[run] = off; S.runlen[run] = len; }
+        off += len;
+      }
     }
-    if (tid == 15) S.runoff[16] = off;
   }
   __syncthreads();
 
@@ -414,11 +512,14 @@ __global__ void __launch_bounds__(256, 2)
   uint32_t pk[8];
   {
     if (!clipped) {
+      const int run = pair_row_of(xp2) + 4 * pair_row_of(xp3);
+      const uint32_t shift = (uint32_t)(S.runstart[run] - kTileTabs.runoff[run]);   // 0 or 1
       const uint4* src = reinterpret_cast<const uint4*>(&kTileTabs.inv[xp3][xp2][0]);
       const uint4 a = __ldg(src), b = __ldg(src + 1);
       const uint32_t v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-      for (int i = 0; i < 8; ++i) pk[i] = v[i] * (uint32_t)sizeof(real);   // both halves < 2^13
+      for (int i = 0; i < 8; ++i)   // both halves stay below 2^16
+        pk[i] = (v[i] + shift * 0x10001u) * (uint32_t)sizeof(real);
     } else {
       const int r2 = pair_row_of(xp2), r3 = pair_row_of(xp3);
       const int n2 = S.nst[1][r2], n3 = S.nst[2][r3];
@@ -432,7 +533,7 @@ __global__ void __launch_bounds__(256, 2)
         const int r1 = pair_row_of(p1);
         const int n1 = S.nst[0][r1];
         const int k1 = p1 - row_pair_base(r1) - S.clip[0][r1];
-        int pos = kImage;
+        int pos = kSink;
         if (ok23 && n1 > 0 && k1 >= 0 && k1 < n1) {
           const int rank = (k3 * n2 + k2) * n1 + k1;
           const int kd = (S.dk[2][r3] * n2 + S.dk[1][r2]) * n1 + S.dk[0][r1];
@@ -461,15 +562,17 @@ __global__ void __launch_bounds__(256, 2)
     }
   }
 
-  // ---- per-thread addresses of the z and y tasks
+  // ---- per-thread addresses of the z tasks
   const int zi = tid % 81;                     // (g1, g2) of the z task
   const int zg1 = zi % 9, zg2 = zi / 9;
   const int zbase = ((zg2 / 3) * 3 + zg1 / 3) * BI + zg1 % 3 + 3 * (zg2 % 3);
   const int zt1 = zg2 * 9 + zg1;
+  // the source term's 1D factors for this thread's vector output (r1, r2, r3)
+  const int vr1 = tid >> 4, vr2 = tid & 3, vr3 = (tid >> 2) & 3;
 
   unsigned char* const img = reinterpret_cast<unsigned char*>(&S.T1[0][0]);
   real* const U1 = &S.T2[0][0];               // vector scratch: [term][r3][g2][g1]
-  real* const U2 = U1 + 4 * 324;              // [term][r3][r2][g1]
+  real* const U2 = U1 + 3 * 324;              // [term][r3][r2][g1]
   const real ihx = (real)(1.0 / L.hx), ihy = (real)(1.0 / L.hy), ihz = (real)(1.0 / L.hz);
 
   int k = 0;
@@ -478,6 +581,8 @@ __global__ void __launch_bounds__(256, 2)
     if (!((pm >> ph) & 1u)) continue;
     const int buf = k & 1;
     const bool ok = mbar_wait(&S.mbar[buf], (uint32_t)(k >> 1) & 1u);
+    // the previous phase's image copies must have left the image before it is rewritten
+    if (kBulk && tid < 16) bulk_wait_read();
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicOr(&g_device_status, HM_STATUS_TIMEOUT);
@@ -485,6 +590,7 @@ __global__ void __launch_bounds__(256, 2)
         const int nx = next_phase(ph);
         if (nx >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
       }
+      if (kBulk && tid < 16) bulk_wait_all();
       return;
     }
     const real* W = reinterpret_cast<const real*>(S.wbuf[buf]) + phase_off<real>(ph);
@@ -538,84 +644,68 @@ __global__ void __launch_bounds__(256, 2)
         else if (ph == PH_WMM) x_task<TM, TM, false>(&S.T2[0][r], (const real*)nullptr, img, pk, false, 0u, 0u);
         else x_task<TR, TM, true>(&S.T2[0][r], &S.T2[1][r], img, pk, has_ess, zC, 0u);
       }
+      if (kBulk) fence_proxy_async();   // the image stores, before the async copies read them
       __syncthreads();
-      // stream the image out: a warp per run of four consecutive rows
+      // stream the image out, run by run (four consecutive rows, one stretch of CSR)
       const real* O = reinterpret_cast<const real*>(img);
+      if constexpr (kBulk) {
+        if (tid < 16) {
+          const int run = tid, a0 = S.runstart[run], len = S.runlen[run];
+          if (len > 0) {
+            double* dst = vals + (int64_t)S.rowptr[run];
+            const int h = S.rowptr[run] & 1;   // the values are 16-byte aligned
+            if (h) dst[0] = (double)O[a0];
+            const int body = (len - h) & ~1;
+            if (body > 0) bulk_store(dst + h, O + a0 + h, (uint32_t)body * 8u);
+            if ((len - h) & 1) dst[len - 1] = (double)O[a0 + len - 1];
+          }
+          bulk_commit();
+        }
+      } else {
 #pragma unroll 1
-      for (int run = warp; run < 16; run += 8) {
-        const int a = clipped ? S.runoff[run] : (int)kTileTabs.runoff[run];
-        const int b = clipped ? S.runoff[run + 1] : (int)kTileTabs.runoff[run + 1];
-        double* dst = vals + (int64_t)S.rowptr[run];
-        for (int j = lane; j < b - a; j += 32) dst[j] = (double)O[a + j];
+        for (int run = warp; run < 16; run += 8) {
+          const int a0 = S.runstart[run], len = S.runlen[run];
+          double* dst = vals + (int64_t)S.rowptr[run];
+          for (int j = lane; j < len; j += 32) dst[j] = (double)O[a0 + j];
+        }
       }
     }
     if (vec != nullptr) {
-      // vector z stage (fields still resident)
-      const int nt = phase_nterms(ph);
-      for (int task = tid; task < nt * 81; task += 256) {
-        const int j = task / 81, i = task % 81;
-        const VTerm vt = phase_term(ph, j);
-        const int g1 = i % 9, g2 = i / 9;
-        real w[9];
-        if (vt.f >= 0) {
-          const real* col = W + 27 * vt.f + ((g2 / 3) * 3 + g1 / 3) * BI + g1 % 3 + 3 * (g2 % 3);
-#pragma unroll
-          for (int g = 0; g < 9; ++g) w[g] = col[(g / 3) * 9 * BI + (g % 3) * 9];
-        } else {
-          const bool in12 = ((vl[0] >> (g1 / 3)) & 1) && ((vl[1] >> (g2 / 3)) & 1);
-#pragma unroll
-          for (int g = 0; g < 9; ++g)
-            w[g] = (in12 && ((vl[2] >> (g / 3)) & 1))
-                       ? (real)(wq(g1 % 3) * wq(g2 % 3) * wq(g % 3) * L.hx * L.hy * L.hz)
-                       : (real)0;
-        }
-        real* u1 = U1 + j * 324 + g2 * 9 + g1;
-        if (vt.tz == VD) v1_task<VD>(w, u1);
-        else v1_task<VB>(w, u1);
-      }
+      // the vector: z (fields still resident), y, x
+      if (ph == PH_C) vec_z<PH_C, BI>(W, U1, tid);
+      else if (ph == PH_WUM) vec_z<PH_WUM, BI>(W, U1, tid);
+      else vec_z<PH_WMM, BI>(W, U1, tid);
       __syncthreads();
       if (tid == 0 && after2 >= 0) {
         fence_proxy_async();
         issue_fields(&tmap, S, buf, after2, e1, e2, e3);
       }
-      for (int task = tid; task < nt * 36; task += 256) {
-        const int j = task / 36, i = task % 36;
-        const int g1 = i % 9, r3 = i / 9;
-        const VTerm vt = phase_term(ph, j);
-        const real* u1 = U1 + j * 324 + r3 * 81 + g1;
-        real* u2 = U2 + j * 144 + r3 * 36 + g1;
-        if (vt.ty == VD) v2_task<VD>(u1, u2);
-        else v2_task<VB>(u1, u2);
-      }
+      if (ph == PH_C) vec_y<PH_C>(U1, U2, tid);
+      else if (ph == PH_WUM) vec_y<PH_WUM>(U1, U2, tid);
+      else vec_y<PH_WMM>(U1, U2, tid);
       __syncthreads();
-      if (tid < 16) {
-        const int r2 = tid & 3, r3 = tid >> 2;
-        real y[4] = {0, 0, 0, 0};
-        for (int j = 0; j < nt; ++j) {
-          const VTerm vt = phase_term(ph, j);
-          const real scale = vt.f < 0 ? (real)(-o.f)
-                           : ph == PH_WMM ? (real)1 : (j == 0 ? ihx : j == 1 ? ihy : ihz);
-          const real* u2 = U2 + j * 144 + r3 * 36 + r2 * 9;
-          if (vt.tx == VD) v3_task<VD>(u2, y, scale);
-          else v3_task<VB>(u2, y, scale);
+      if (tid < 64) {
+        real y = ph == PH_C ? vec_x<PH_C>(U2, vr1, vr2, vr3, ihx, ihy, ihz)
+               : ph == PH_WUM ? vec_x<PH_WUM>(U2, vr1, vr2, vr3, ihx, ihy, ihz)
+                              : vec_x<PH_WMM>(U2, vr1, vr2, vr3, ihx, ihy, ihz);
+        if (ph == PH_C) {
+          const real src = (real)(L.hx * L.hy * L.hz) * src_1d_rt<real>(vr1, vl[0]) *
+                           src_1d_rt<real>(vr2, vl[1]) * src_1d_rt<real>(vr3, vl[2]);
+          y = fma((real)(-o.f), src, y);
         }
-        const int gy = 4 * t2 + r2, gz = 4 * t3 + r3;
-        if (gy < L.Ny && gz < L.Nz) {
-#pragma unroll
-          for (int r1 = 0; r1 < 4; ++r1) {
-            const int gx = 4 * t1 + r1;
-            if (gx >= L.Nx) continue;
-            double v = (double)y[r1];
-            if (o.zero_ess && ph != PH_WMM && S.ess[r3 + 2][r2 + 2][r1 + 2]) v = 0.0;
-            vec[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] = v;
-          }
+        const int gx = 4 * t1 + vr1, gy = 4 * t2 + vr2, gz = 4 * t3 + vr3;
+        if (gx < L.Nx && gy < L.Ny && gz < L.Nz) {
+          double v = (double)y;
+          if (o.zero_ess && ph != PH_WMM && S.ess[vr3 + 2][vr2 + 2][vr1 + 2]) v = 0.0;
+          vec[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] = v;
         }
       }
     }
-    // the image (T1) and the y buffers are rewritten by the next phase
+    // the y buffers are rewritten by the next phase
     __syncthreads();
     ++k;
   }
+  if (kBulk && tid < 16) bulk_wait_all();
 }
 
 // ------------------------------------------------------------ host side
@@ -691,6 +781,9 @@ int hm_launch_assemble(const Lattice& L, const void* quad, int precision, const 
   o.vals[0] = vA; o.vals[1] = vC; o.vals[2] = vWum; o.vals[3] = vWmm;
   o.vec_state = vs; o.vec_param = vp; o.vec_adj = va; o.f = f; o.zero_ess = zero_ess;
   if ((vA || vC || vWum || vWmm) && indptr == nullptr) return HM_ERR_ARG;
+  // the copy-out moves 16-byte aligned stretches of the value arrays
+  for (double* v : {vA, vC, vWum, vWmm})
+    if ((reinterpret_cast<uintptr_t>(v) & 15u) != 0) return HM_ERR_ARG;
   if (precision == HM_FP32) return launch_assemble_t<float>(L, quad, indptr, ess, o, stream);
   return launch_assemble_t<double>(L, quad, indptr, ess, o, stream);
 }

@@ -120,8 +120,9 @@ int hm_lattice_quadrature(const hm_lattice* h, const double* d_u, const double* 
  * (uint8 per dof, NULL: none): A rows and columns zeroed with a unit diagonal, C and
  * Wum rows zeroed, Wmm untouched.  And the assembled vectors whose pointer is not
  * NULL: dR/du (STATE), dR/dm (PARAMETER), dR/dp (ADJOINT, the residual with source f);
- * with zero_ess_vectors the STATE and ADJOINT ones are zeroed on d_ess.
- * Replaces setLinearizationPoint's shared pass (modeling/PDEVariationalProblem.py:
+ * with zero_ess_vectors the STATE and ADJOINT ones are zeroed on d_ess.  The value
+ * arrays and d_quad must be 16-byte aligned (HM_ERR_ARG otherwise; cudaMalloc and
+ * torch allocations are).  Replaces setLinearizationPoint's shared pass (modeling/PDEVariationalProblem.py:
  * 1372-1482), _jacobian (:542), _residual (:423), element_matrices_many /
  * element_vectors (hippymfem/fem/kernel.py:2048,2070) and the scatter
  * ScatterPattern.data (hippymfem/fem/pattern.py:749-791). */
