@@ -37,6 +37,9 @@ if ROOT not in sys.path:
 
 METRIC = "Q2 elems/s, H-applies/s at 64^3 vs plain FP64; p50/p99 batched-solve latency"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes per algorithmic byte of k_tile_assemble<double>, from one ncu capture at 48^3
+# (profiles/k_tile_assemble_48cube.md)
+TRAFFIC_PER_ALG_BYTE = 2030.9 / 2043.7
 
 
 def parse():
@@ -48,6 +51,8 @@ def parse():
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--happly", type=int, default=5, help="timed Hessian actions")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving", type=int, default=2000,
+                    help="requests of the serving trace (0: skip)")
     return ap.parse_args()
 
 
@@ -74,6 +79,13 @@ class Clocks:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # wait (at most 5 s) for the first sample, so the timed region is covered
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -201,6 +213,58 @@ def run_reference(a):
 
 
 # ------------------------------------------------------------------------- ours
+def run_serving(nreq, dev, sizes=(8, 12, 16, 24, 32, 48), slots=4, plain_sample=200):
+    """The serving configuration: requests on n^3 meshes, n uniform over ``sizes``, 70%
+    forward solves (Jacobi-PCG to rtol 1e-8) / 30% Hessian actions, Poisson arrivals at
+    80% of the measured capacity, through the request loop (4 slots, FP32 operator and
+    recurrence with FP64 reliable updates, graph-captured iteration batches); beside it
+    the plain FP64 per-request path on a sample of the same trace, one request at a time."""
+    import torch
+
+    from hippymfem_b200.serving import Server, latency_stats, plain_fp64, poisson_trace
+
+    srv = Server(slots=slots, precision="mixed", rel_tolerance=1e-8, device=dev,
+                 keep_results=False)
+    tuned = srv.autotune(sizes, candidates=(8, 16, 32), reps=2)
+    # capacity: a burst of requests from the same mix, all arriving at once
+    burst = poisson_trace(120, 1e9, sizes, seed=11)
+    for r in burst:
+        r.arrival = 0.0
+    srv.run(burst)
+    capacity = latency_stats(burst)["requests_per_s"]
+    trace = poisson_trace(nreq, 0.8 * capacity, sizes, seed=12)
+    srv.run(trace)
+    st = latency_stats(trace)
+    st.update({"capacity_requests_per_s": capacity, "arrival_rate": 0.8 * capacity,
+               "slots": slots, "peak_workspace_bytes": srv.peak_resident,
+               "graph_batch_by_n": {str(k): v for k, v in tuned.items()},
+               "solves_per_s": sum(len(r.iterations) for r in trace) / (
+                   max(r.t_done for r in trace) - min(r.arrival for r in trace))})
+    srv.close()
+    # the plain FP64 path, request by request (no overlap, no resident workspace)
+    cache = {}
+    sample = trace[:plain_sample]
+    for r in sample[:6]:
+        plain_fp64(r, dev, cache=cache)
+    lat = []
+    for r in sample:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plain_fp64(r, dev, cache=cache)
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    st["plain_fp64"] = {"p50_ms": float(np.percentile(lat, 50)),
+                        "p99_ms": float(np.percentile(lat, 99)),
+                        "requests_per_s": 1000.0 * len(lat) / float(np.sum(lat)),
+                        "sample": len(lat),
+                        "what": "service time of each request alone (no queueing), FP64, "
+                                "fresh problem objects, default stream"}
+    st["what"] = ("%d-request Poisson trace at 80%% of capacity, n in %s, 70%% forward / 30%% "
+                  "Hessian actions, rtol 1e-8; latency = completion - arrival" % (nreq, list(sizes)))
+    return st
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -252,13 +316,13 @@ def run_ours(a):
             ev_k1[i].record(stream)
 
     launches_per_step = 2
+    clocks = Clocks(local)
+    clocks.start()
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = Clocks(local)
-    clocks.start()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -267,7 +331,6 @@ def run_ours(a):
         step(i)
     t1.record(stream)
     torch.cuda.synchronize()
-    ck = clocks.stop()
     ms = t0.elapsed_time(t1)
     k_ms = statistics.mean(ev_k0[i].elapsed_time(ev_k1[i]) for i in range(a.steps))
     if world > 1:
@@ -379,6 +442,13 @@ def run_ours(a):
         lat32.append(h0.elapsed_time(h1))
     mixed_err = float((y - y64).norm() / y64.norm())
     iters32 = list(H.iterations)
+    ck = clocks.stop()
+    del H, model, prob
+    torch.cuda.empty_cache()
+
+    serving = None
+    if a.serving > 0 and world == 1:
+        serving = run_serving(a.serving, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -397,7 +467,11 @@ def run_ours(a):
                        "l2": "inputs and outputs larger than L2 (4.3 GB written per step)"},
             "dofs_per_s": world * nd * a.steps / (ms / 1000.0),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": alg_bytes * TRAFFIC_PER_ALG_BYTE,
+                         "traffic_source": "ncu dram__bytes_read+write of one 48^3 launch "
+                                           "(2030.9 MB for 2043.7 algorithmic MB), scaled "
+                                           "by the algorithmic bytes",
                          "kernel": "k_tile_assemble<double>", "kernel_ms": k_ms,
                          "alg_bytes_per_launch": alg_bytes,
                          "step_alg_bytes": step_bytes,
@@ -419,6 +493,7 @@ def run_ours(a):
                     "h2d_bytes_per_step": 3 * 8 * nd, "d2h_bytes_per_step": 8 * nd,
                     "steps": e_steps},
             "clocks": ck,
+            "serving": serving,
             "gpu_launches": launches_per_step * a.steps,
             "cpu_baseline": cpu,
         }

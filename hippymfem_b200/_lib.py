@@ -65,6 +65,10 @@ SIGNATURES = {
     "hm_pcg_mixed": (_i32, [_p, _p, _p, _p, _p, _p, _p, _d, _d, _i32, _i32, _i32, _p, _p, _p, _p,
                             _p]),
     "hm_device_status": (_i32, [_p, _i32]),
+    "hm_pcg_plan_create": (_i32, [_p, _p, _p, _p, _p, _p, _p, _p, _i32, _p]),
+    "hm_pcg_plan_solve": (_i32, [_p, _d, _d, _i32, _i32, _p, _p, _p, _p]),
+    "hm_pcg_plan_destroy": (_i32, [_p]),
+    "hm_lattice_quadrature_dir": (_i32, [_p, _p, _p, _p, _p, _i32, _p, _p, _p]),
     "hm_dot_workspace_bytes": (_i64, [_i64]),
     "hm_dot": (_i32, [_i64, _p, _p, _p, _p, _p]),
 }

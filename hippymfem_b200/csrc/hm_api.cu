@@ -88,6 +88,16 @@ extern "C" int hm_lattice_quadrature(const hm_lattice* h, const double* u, const
   return hm_launch_quad(h->L, u, m, p, precision, quad, status, stream);
 }
 
+extern "C" int hm_lattice_quadrature_dir(const hm_lattice* h, const double* u, const double* m,
+                                         const double* p, const double* mhat, int precision,
+                                         void* quad, uint32_t* status, void* stream) {
+  if (!h || !u || !m || !p || !mhat || !quad || !status) return HM_ERR_ARG;
+  if (precision != HM_FP64 && precision != HM_FP32) return HM_ERR_ARG;
+  if (!aligned8(u) || !aligned8(m) || !aligned8(p) || !aligned8(mhat) || !aligned8(quad))
+    return HM_ERR_ARG;
+  return hm_launch_quad(h->L, u, m, p, precision, quad, status, stream, mhat);
+}
+
 extern "C" int hm_lattice_assemble(const hm_lattice* h, const void* quad, int precision,
                                    const int32_t* indptr, const uint8_t* ess, double f,
                                    double* vA, double* vC, double* vWum, double* vWmm,

@@ -16,7 +16,8 @@ int hm_launch_pattern(const hm::Lattice& L, int32_t* indptr, int32_t* indices, i
                       void* stream);
 int hm_launch_tpos(const hm::Lattice& L, const int32_t* indptr, int32_t* tpos, void* stream);
 int hm_launch_quad(const hm::Lattice& L, const double* u, const double* m, const double* p,
-                   int precision, void* quad, uint32_t* status, void* stream);
+                   int precision, void* quad, uint32_t* status, void* stream,
+                   const double* mhat = nullptr);
 int hm_launch_assemble(const hm::Lattice& L, const void* quad, int precision,
                        const int32_t* indptr, const uint8_t* ess, double f, double* vA,
                        double* vC, double* vWum, double* vWmm, double* vs, double* vp,

@@ -108,13 +108,16 @@ __global__ void k_pattern_tpos(Lattice L, const int32_t* __restrict__ indptr,
 // ============================================================ quadrature data
 // One thread per (element, Gauss point), 8 elements per 216-thread block.  Layout:
 // quad[e][c][q], c = 0 D, 1-3 E, 4-6 F, 7 W (each element's 216 values contiguous).
+// With mhat, D = w|J| e^m mhat: the data of the directional derivative along mhat
+// (the second-order products of the assembled vectors, with f = 0).
 template <typename real>
 __global__ void __launch_bounds__(216) k_quad(Lattice L, const double* __restrict__ u,
                                               const double* __restrict__ m,
                                               const double* __restrict__ p,
+                                              const double* __restrict__ mhat,
                                               real* __restrict__ quad,
                                               uint32_t* __restrict__ status) {
-  __shared__ real sv[8][3][27];
+  __shared__ real sv[8][4][27];
   const int le = threadIdx.x / 27, q = threadIdx.x % 27;
   const int64_t e = blockIdx.x * 8LL + le;
   const bool live = e < L.ne;
@@ -125,6 +128,7 @@ __global__ void __launch_bounds__(216) k_quad(Lattice L, const double* __restric
     sv[le][0][a] = (real)u[node];
     sv[le][1][a] = (real)m[node];
     sv[le][2][a] = (real)p[node];
+    if (mhat) sv[le][3][a] = (real)mhat[node];
   }
   __syncthreads();
   if (!live) return;
@@ -166,7 +170,25 @@ __global__ void __launch_bounds__(216) k_quad(Lattice L, const double* __restric
     gz[f] = vz / (real)L.hz;
   }
   const real wdet = (real)(wq(q1) * wq(q2) * wq(q3) * L.hx * L.hy * L.hz);
-  const real D = wdet * exp(val[1]);
+  real D = wdet * exp(val[1]);
+  if (mhat) {
+    // mhat at the point (value only)
+    const real* x = sv[le][3];
+    real vb = 0;
+#pragma unroll
+    for (int a3 = 0; a3 < 3; ++a3) {
+      real sbb = 0;
+#pragma unroll
+      for (int a2 = 0; a2 < 3; ++a2) {
+        real xb = 0;
+#pragma unroll
+        for (int a1 = 0; a1 < 3; ++a1) xb = fma(b1[a1], x[a1 + 3 * a2 + 9 * a3], xb);
+        sbb = fma(b2[a2], xb, sbb);
+      }
+      vb = fma(b3[a3], sbb, vb);
+    }
+    D *= vb;
+  }
   const real E[3] = {D * gx[0], D * gy[0], D * gz[0]};
   const real F[3] = {D * gx[2], D * gy[2], D * gz[2]};
   const real W = D * (gx[0] * gx[2] + gy[0] * gy[2] + gz[0] * gz[2]);
@@ -436,12 +458,12 @@ int hm_launch_tpos(const Lattice& L, const int32_t* indptr, int32_t* tpos, void*
 }
 
 int hm_launch_quad(const Lattice& L, const double* u, const double* m, const double* p,
-                   int precision, void* quad, uint32_t* status, void* stream) {
+                   int precision, void* quad, uint32_t* status, void* stream, const double* mhat) {
   const int blocks = grid1(L.ne, 8);
   if (precision == HM_FP32)
-    k_quad<float><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, (float*)quad, status);
+    k_quad<float><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, mhat, (float*)quad, status);
   else
-    k_quad<double><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, (double*)quad, status);
+    k_quad<double><<<blocks, 216, 0, S_(stream)>>>(L, u, m, p, mhat, (double*)quad, status);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 

@@ -6,6 +6,7 @@
 // launches and, every check_every iterations, reads one flag.  After convergence the
 // step length is frozen at zero, so the result is that of the exact iteration count
 // whatever check_every is.
+#include <new>
 #include <cmath>
 
 #include "hm_common.cuh"
@@ -86,7 +87,7 @@ __global__ void k_reduce_final(const double* __restrict__ part, int nq, double* 
 
 // ----------------------------------------------------------------------- PCG
 // device scalars
-enum { SC_RZ = 0, SC_PQ, SC_ALPHA, SC_BETA, SC_RR, SC_BB, SC_TOL2, SC_CONV, SC_TMP0, SC_TMP1, SC_TMP2, SC_N };
+enum { SC_RZ = 0, SC_PQ, SC_ALPHA, SC_BETA, SC_RR, SC_BB, SC_TOL2, SC_CONV, SC_TMP0, SC_TMP1, SC_TMP2, SC_IT, SC_N };
 
 // Vector kernels, templated on the vector type T (double, or float for the inner solves
 // of the mixed-precision PCG); sums are accumulated in double.
@@ -131,6 +132,7 @@ __global__ void k_pcg_init_final(const double* __restrict__ part, double* __rest
     sc[SC_BB] = v[2];
     sc[SC_TOL2] = rtol * rtol;
     sc[SC_CONV] = (v[1] <= rtol * rtol * v[2]) ? 0.0 : -1.0;
+    sc[SC_IT] = 0.0;
   }
 }
 
@@ -171,7 +173,9 @@ __global__ void __launch_bounds__(kReduceThreads)
   }
 }
 
-__global__ void k_pcg_beta(const double* __restrict__ part, double* __restrict__ sc, int it) {
+// the iteration count lives on the device (sc[SC_IT]), so that every batch of
+// iterations launches the same kernels with the same arguments (a graph replays it)
+__global__ void k_pcg_beta(const double* __restrict__ part, double* __restrict__ sc) {
   __shared__ double sh[32];
   double v[2];
   for (int q = 0; q < 2; ++q) {
@@ -182,8 +186,10 @@ __global__ void k_pcg_beta(const double* __restrict__ part, double* __restrict__
   if (threadIdx.x == 0) {
     const bool was = sc[SC_CONV] >= 0.0;
     if (!was) {
+      const double it = sc[SC_IT] + 1.0;
+      sc[SC_IT] = it;
       sc[SC_RR] = v[1];
-      if (v[1] <= sc[SC_TOL2] * sc[SC_BB]) sc[SC_CONV] = (double)it;
+      if (v[1] <= sc[SC_TOL2] * sc[SC_BB]) sc[SC_CONV] = it;
       const double beta = sc[SC_RZ] == 0.0 ? 0.0 : v[0] / sc[SC_RZ];
       sc[SC_BETA] = isfinite(beta) ? beta : 0.0;
       sc[SC_RZ] = v[0];
@@ -397,11 +403,66 @@ int op_apply(const PcgOp& o, const float* x, float* y, double* part, int64_t* np
   return hm_launch_apply_A32_dot(*o.L, o.jac, o.ess, x, y, part, stream);
 }
 
+// `count` PCG iterations (operator + fused p.q, alpha, update with r.z and r.r, beta,
+// direction); nothing in it synchronises with the host
+template <typename T>
+int pcg_batch(const PcgOp& o, const double* diag, T* x, T* r, T* z, T* p, T* q, double* pq_part,
+              double* sc, double* part, int count, cudaStream_t s) {
+  int64_t np = 0;
+  for (int j = 0; j < count; ++j) {
+    const int rc = op_apply(o, p, q, pq_part, &np, (void*)s);
+    if (rc) return rc;
+    k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
+    k_pcg_update<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(o.n, sc, x, r, z, p, q, diag, part);
+    k_pcg_beta<<<1, 1024, 0, s>>>(part, sc);
+    k_pcg_pupdate<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(o.n, sc, z, p);
+  }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+}  // namespace
+
+// A full batch of iterations captured once as a CUDA graph and replayed (a solve plan
+// owns one per precision); partial batches, and streams that cannot be captured (the
+// legacy default stream), launch directly.
+struct HmBatchGraph {
+  cudaGraphExec_t exec = nullptr;
+  ~HmBatchGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+namespace {
+
+template <typename F>
+int run_batch(HmBatchGraph* g, bool full, cudaStream_t s, F&& launch) {
+  if (g == nullptr || s == nullptr || !full) return launch();
+  if (g->exec == nullptr) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HM_ERR_CUDA;
+    const int rc = launch();
+    const cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (rc != HM_OK || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      return rc != HM_OK ? rc : HM_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      g->exec = nullptr;
+      return HM_ERR_CUDA;
+    }
+  }
+  return cudaGraphLaunch(g->exec, s) == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
 // Jacobi-PCG on vectors of type T from initial guess x; work holds r, z, p, q (T), the
 // p.q partials (n doubles), the scalars and the partials.  Returns HM_OK / HM_ERR_NOCONV.
 template <typename T>
 int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, int maxiter,
-            int check_every, double* wd, T* wt, int* iterations, double* relres, void* stream) {
+            int check_every, double* wd, T* wt, int* iterations, double* relres, void* stream,
+            HmBatchGraph* graph = nullptr) {
   const int64_t n = o.n;
   cudaStream_t s = S_(stream);
   T* r = wt;
@@ -423,17 +484,12 @@ int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, i
     if (cudaMemcpyAsync(host, sc, sizeof(host), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HM_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return HM_ERR_CUDA;
     if (host[SC_CONV] >= 0.0 || it >= maxiter) break;
-    const int stop = it + check_every < maxiter ? it + check_every : maxiter;
-    for (; it < stop;) {
-      ++it;
-      rc = op_apply(o, p, q, pq_part, &nparts, stream);
-      if (rc) return rc;
-      k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, nparts, sc);
-      k_pcg_update<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, z, p, q, diag, part);
-      k_pcg_beta<<<1, 1024, 0, s>>>(part, sc, it);
-      k_pcg_pupdate<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z, p);
-    }
-    if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
+    const int count = it + check_every < maxiter ? check_every : maxiter - it;
+    rc = run_batch(graph, count == check_every, s, [&] {
+      return pcg_batch<T>(o, diag, x, r, z, p, q, pq_part, sc, part, count, s);
+    });
+    if (rc) return rc;
+    it += count;
   }
   const bool conv = host[SC_CONV] >= 0.0;
   if (iterations) *iterations = conv ? (int)host[SC_CONV] : it;
@@ -471,11 +527,11 @@ extern "C" int64_t hm_pcg_mixed_workspace_bytes(int64_t n) {
 // reference's refined solves (modeling/PDEVariationalProblem.py:1236-1237, :1299): a
 // residual that no longer halves between anchors is at its rounding floor; it counts as
 // converged within 10 rtol.
-extern "C" int hm_pcg_mixed_impl(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t* ess,
-                                 const double* diag, const double* b, double* x, double rtol,
-                                 double delta, int max_updates, int maxiter, int check_every,
-                                 void* work, int* iterations, int* updates, double* relres,
-                                 void* stream) {
+namespace {
+int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t* ess,
+                  const double* diag, const double* b, double* x, double rtol, double delta,
+                  int max_updates, int maxiter, int check_every, void* work, int* iterations,
+                  int* updates, double* relres, void* stream, HmBatchGraph* graph) {
   if (!L || !jac64 || !jac32 || !diag || !b || !x || !work || max_updates <= 0 || maxiter < 0 ||
       !(delta > 0.0 && delta < 1.0) || !(rtol >= 0.0))
     return HM_ERR_ARG;
@@ -531,18 +587,12 @@ extern "C" int hm_pcg_mixed_impl(const hm::Lattice* L, void* jac64, void* jac32,
   int it = 0, nup = 0, stalls = 0;
   bool conv = tr <= tol2;
   while (!conv) {
-    const int stop = it + check_every < maxiter ? it + check_every : maxiter;
-    int64_t np = 0;
-    for (; it < stop;) {
-      ++it;
-      rc = op_apply(o32, p32, q32, pq_part, &np, stream);
-      if (rc) return rc;
-      k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
-      k_pcg_update<float><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x32, r32, z32, p32, q32, diag, part);
-      k_pcg_beta<<<1, 1024, 0, s>>>(part, sc, it);
-      k_pcg_pupdate<float><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z32, p32);
-    }
-    if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
+    const int count = it + check_every < maxiter ? check_every : maxiter - it;
+    rc = run_batch(graph, count == check_every, s, [&] {
+      return pcg_batch<float>(o32, diag, x32, r32, z32, p32, q32, pq_part, sc, part, count, s);
+    });
+    if (rc) return rc;
+    it += count;
     if ((rc = read())) return rc;
     const bool claim = h[SC_CONV] >= 0.0;
     if (!claim && h[SC_RR] > delta * delta && it < maxiter) continue;
@@ -562,4 +612,71 @@ extern "C" int hm_pcg_mixed_impl(const hm::Lattice* L, void* jac64, void* jac32,
   if (updates) *updates = nup;
   if (relres) *relres = bb > 0.0 ? std::sqrt(tr / bb) : 0.0;
   return conv ? HM_OK : HM_ERR_NOCONV;
+}
+}  // namespace
+
+extern "C" int hm_pcg_mixed_impl(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t* ess,
+                                 const double* diag, const double* b, double* x, double rtol,
+                                 double delta, int max_updates, int maxiter, int check_every,
+                                 void* work, int* iterations, int* updates, double* relres,
+                                 void* stream) {
+  return pcg_mixed_run(L, jac64, jac32, ess, diag, b, x, rtol, delta, max_updates, maxiter,
+                       check_every, work, iterations, updates, relres, stream, nullptr);
+}
+
+// ------------------------------------------------------------------ solve plans
+struct hm_pcg_plan {
+  hm::Lattice L;
+  void* jac64;
+  void* jac32;          // NULL: an FP64 solve
+  const uint8_t* ess;
+  const double* diag;
+  double* b;
+  double* x;
+  void* work;
+  int check_every;
+  HmBatchGraph graph;
+};
+
+extern "C" int hm_pcg_plan_create(const hm_lattice* h, void* jac64, void* jac32,
+                                  const uint8_t* ess, const double* diag, double* b, double* x,
+                                  void* work, int check_every, hm_pcg_plan** plan) {
+  const hm::Lattice* L = hm_lattice_geometry(h);
+  if (!L || !jac64 || !diag || !b || !x || !work || !plan || check_every <= 0) return HM_ERR_ARG;
+  hm_pcg_plan* p = new (std::nothrow) hm_pcg_plan();
+  if (!p) return HM_ERR_NOMEM;
+  p->L = *L;
+  p->jac64 = jac64;
+  p->jac32 = jac32;
+  p->ess = ess;
+  p->diag = diag;
+  p->b = b;
+  p->x = x;
+  p->work = work;
+  p->check_every = check_every;
+  *plan = p;
+  return HM_OK;
+}
+
+extern "C" int hm_pcg_plan_solve(hm_pcg_plan* p, double rtol, double delta, int max_updates,
+                                 int maxiter, int* iterations, int* updates, double* relres,
+                                 void* stream) {
+  if (!p || maxiter < 0) return HM_ERR_ARG;
+  if (p->jac32 != nullptr)
+    return pcg_mixed_run(&p->L, p->jac64, p->jac32, p->ess, p->diag, p->b, p->x, rtol, delta,
+                         max_updates, maxiter, p->check_every, p->work, iterations, updates,
+                         relres, stream, &p->graph);
+  const int64_t n = p->L.ndof;
+  cudaStream_t s = S_(stream);
+  if (cudaMemsetAsync(p->x, 0, sizeof(double) * n, s) != cudaSuccess) return HM_ERR_CUDA;
+  PcgOp o{n, nullptr, nullptr, nullptr, &p->L, p->jac64, HM_FP64, p->ess};
+  double* w = static_cast<double*>(p->work);
+  if (updates) *updates = 0;
+  return pcg_run<double>(o, p->diag, p->b, p->x, rtol, maxiter, p->check_every, w + 4 * n, w,
+                         iterations, relres, stream, &p->graph);
+}
+
+extern "C" int hm_pcg_plan_destroy(hm_pcg_plan* p) {
+  delete p;
+  return HM_OK;
 }

@@ -35,8 +35,19 @@ _BLOCKS = {(ADJOINT, STATE): "A", (ADJOINT, PARAMETER): "C", (STATE, PARAMETER):
            (PARAMETER, PARAMETER): "Wmm"}
 
 
-def _key(t):
-    return None if t is None else (id(t), t.data_ptr(), t._version)
+class _Snapshot:
+    """A copy of a vector, to recognise it again by its values (object identity and
+    storage addresses are reused once a tensor is freed)."""
+
+    __slots__ = ("t",)
+
+    def __init__(self, t):
+        self.t = None if t is None else t.detach().clone()
+
+    def matches(self, t):
+        if self.t is None or t is None:
+            return self.t is None and t is None
+        return self.t.shape == t.shape and bool(torch.equal(self.t, t))
 
 
 class PDEVariationalProblem:
@@ -89,6 +100,7 @@ class PDEVariationalProblem:
         self._pattern = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.mesh.device)
         self._quad = {}
+        self._dir_cache = None
         self._jac_cache = None
         self.A = self.At = self.C = self.Wuu = self.Wum = self.Wmm = self.Ct = self.Wmu = None
         self._lin_point = None
@@ -125,8 +137,9 @@ class PDEVariationalProblem:
             out.append(v if v is not None else self.Vh[i].vector())
         return out
 
-    def _quadrature(self, x, slot="point"):
-        """Quadrature data of ``x`` into the buffer named ``slot`` (kept for reuse)."""
+    def _quadrature(self, x, slot="point", mhat=None):
+        """Quadrature data of ``x`` into the buffer named ``slot`` (kept for reuse); with
+        ``mhat`` the data of the directional derivative along ``mhat``."""
         u, m, p = self._locals(x)
         nbytes = self.mesh.quad_bytes(self.precision)
         buf = self._quad.get(slot)
@@ -135,24 +148,31 @@ class PDEVariationalProblem:
                                                  device=self.mesh.device)
         if self.check_finite:
             self._status.zero_()
-        check(lib.hm_lattice_quadrature(self.mesh.handle, ptr(u), ptr(m), ptr(p), self.precision,
-                                        ptr(buf), ptr(self._status), stream_ptr()),
-              "hm_lattice_quadrature")
+        if mhat is None:
+            check(lib.hm_lattice_quadrature(self.mesh.handle, ptr(u), ptr(m), ptr(p),
+                                            self.precision, ptr(buf), ptr(self._status),
+                                            stream_ptr()), "hm_lattice_quadrature")
+        else:
+            check(lib.hm_lattice_quadrature_dir(self.mesh.handle, ptr(u), ptr(m), ptr(p),
+                                                ptr(mhat), self.precision, ptr(buf),
+                                                ptr(self._status), stream_ptr()),
+                  "hm_lattice_quadrature_dir")
         return buf
 
     def _require_finite(self, what):
         if self.check_finite and int(self._status.item()) & _lib.HM_STATUS_NONFINITE:
             raise RuntimeError("non-finite values in %s" % what)
 
-    def _assemble(self, quad, blocks=(), vectors=(), zero_ess_vectors=False):
+    def _assemble(self, quad, blocks=(), vectors=(), zero_ess_vectors=False, f=None):
         """One fused launch: the CSR values of ``blocks`` (names of ``_BLOCKS``) and the
-        assembled vectors of the slots in ``vectors``."""
+        assembled vectors of the slots in ``vectors`` (source ``f``: the problem's)."""
         pat = self.pattern if blocks else None
         vals = {b: pat.new_values() for b in blocks}
         vecs = {s: self.Vh[s].vector() for s in vectors}
         check(lib.hm_lattice_assemble(
             self.mesh.handle, ptr(quad), self.precision,
-            ptr(pat.indptr) if pat is not None else None, ptr(self.bc0.marker), self.f,
+            ptr(pat.indptr) if pat is not None else None, ptr(self.bc0.marker),
+            self.f if f is None else float(f),
             ptr(vals.get("A")), ptr(vals.get("C")), ptr(vals.get("Wum")), ptr(vals.get("Wmm")),
             ptr(vecs.get(STATE)), ptr(vecs.get(PARAMETER)), ptr(vecs.get(ADJOINT)),
             int(bool(zero_ess_vectors)), stream_ptr()), "hm_lattice_assemble")
@@ -184,12 +204,11 @@ class PDEVariationalProblem:
         """The assembled Jacobian ``A`` and its transpose (``A`` itself: the density is
         symmetric in u and p), reused while ``m`` has not moved (:542)."""
         m = x[PARAMETER]
-        key = _key(m)
-        if self._jac_cache is not None and self._jac_cache[0] == key:
+        if self._jac_cache is not None and self._jac_cache[0].matches(m):
             return self._jac_cache[1], self._jac_cache[1]
         quad = self._quadrature([None, m, None], "jacobian")
         A = self._make_jacobian(quad)
-        self._jac_cache = (key, A, quad)
+        self._jac_cache = (_Snapshot(m), A, quad)
         self.solver = None
         return A, A
 
@@ -254,7 +273,7 @@ class PDEVariationalProblem:
         self.gauss_newton_approx = bool(gauss_newton_approx)
         self._mf = bool(matrix_free)
         m = x[PARAMETER]
-        need_A = self._jac_cache is None or self._jac_cache[0] != _key(m)
+        need_A = self._jac_cache is None or not self._jac_cache[0].matches(m)
         quad = self._quadrature(self._lin_point, "linpoint")
         names = []
         if need_A and not self.matrix_free_solves:
@@ -267,7 +286,7 @@ class PDEVariationalProblem:
         self._require_finite("linearization point")
         if need_A:
             A = blocks["A"] if "A" in blocks else self._make_jacobian(quad)
-            self._jac_cache = (_key(m), A, quad)
+            self._jac_cache = (_Snapshot(m), A, quad)
             self.solver = None
         self.A, self.At = self._jac_cache[1], self._jac_cache[1]
         self.C = blocks.get("C")
@@ -332,10 +351,29 @@ class PDEVariationalProblem:
             mat.mult(dir, out)
         return out
 
+    def _dir_products(self, x, mhat):
+        """``C mhat``, ``W_um mhat`` and ``W_mm mhat`` at ``x`` from one pass of the
+        directional quadrature data (f = 0), with the row eliminations of C and W_um;
+        kept for the next products along the same ``mhat`` at the same point."""
+        c = self._dir_cache
+        if c is not None and all(a.matches(v) for a, v in zip(c[0], list(x) + [mhat])):
+            return c[1]
+        quad = self._quadrature(x, "dir", mhat=mhat)
+        _, vecs = self._assemble(quad, vectors=(ADJOINT, STATE, PARAMETER), f=0.0)
+        self._require_finite("the second-order products")
+        mask = self.bc0.mask
+        vecs[ADJOINT].masked_fill_(mask, 0.0)
+        vecs[STATE].masked_fill_(mask, 0.0)
+        self._dir_cache = (tuple(_Snapshot(v) for v in list(x) + [mhat]), vecs)
+        return vecs
+
     def apply_ij_at(self, i, j, x, dir, out):
-        """The ``(i, j)`` block at ``x`` applied to ``dir`` without keeping the block
-        (:1672): the Jacobian pair through the matrix-free operator; the others from a
-        block assembled for the product and dropped."""
+        """The ``(i, j)`` block at ``x`` applied to ``dir`` without forming the block
+        (:1672): the Jacobian pair through the matrix-free operator; the second-order
+        blocks from the vector kernels -- ``C``, ``W_um``, ``W_mm`` times a parameter
+        direction from the directional quadrature data, ``C^T p`` and ``W_mu u`` as
+        ``dR/dm`` with the direction in the adjoint or state slot (eliminated rows
+        zeroed first)."""
         if {i, j} == {STATE, ADJOINT}:
             quad = self._quadrature([None, x[PARAMETER], None], "apply")
             MatrixFreeJacobian(self.mesh, quad, self.bc0.marker, self.precision).mult(dir, out)
@@ -343,12 +381,18 @@ class PDEVariationalProblem:
         if (i, j) == (STATE, STATE) or (self.gauss_newton_approx and ADJOINT not in (i, j)):
             out.zero_()
             return out
-        transpose = (i, j) in ((PARAMETER, ADJOINT), (PARAMETER, STATE))
-        blk = self._block(j, i, x) if transpose else self._block(i, j, x)
-        if transpose:
-            if blk.pattern.tpos is None:
-                raise ValueError("transpose map missing")
-            blk.mult_transpose(dir, out)
-        else:
-            blk.mult(dir, out)
+        x = self._locals(x)
+        if j == PARAMETER:
+            if (i, j) not in ((ADJOINT, PARAMETER), (STATE, PARAMETER), (PARAMETER, PARAMETER)):
+                raise ValueError("no block (%d, %d)" % (i, j))
+            out.copy_(self._dir_products(x, dir)[i])
+            return out
+        if (i, j) not in ((PARAMETER, ADJOINT), (PARAMETER, STATE)):
+            raise ValueError("no block (%d, %d)" % (i, j))
+        d = dir.masked_fill(self.bc0.mask, 0.0)
+        y = [x[STATE], x[PARAMETER], d] if j == ADJOINT else [d, x[PARAMETER], x[ADJOINT]]
+        quad = self._quadrature(y, "transpose")
+        _, vecs = self._assemble(quad, vectors=(PARAMETER,))
+        self._require_finite("the second-order products")
+        out.copy_(vecs[PARAMETER])
         return out

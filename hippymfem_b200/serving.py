@@ -1,0 +1,433 @@
+"""A request loop for forward solves and Hessian-vector applies on meshes of several
+sizes -- the MCMC / forward-UQ pattern in which the reference's ``Model`` is called
+once per sample (modeling/model.py:139-261, modeling/reducedHessian.py:87-131).
+
+Continuous batching over CUDA streams.  ``Server`` owns ``slots`` worker threads, each
+with its own stream.  Requests wait in arrival order; a free slot takes the oldest one
+as soon as its working set fits the device-memory budget (``memory_budget`` bytes):
+workspaces stay resident per slot and mesh size between requests, and the least
+recently used idle ones are released when a new size needs room.  Requests on different
+slots run at the same time on the device (the library's calls release the GIL and
+synchronise only their own stream), so requests that arrive while others run are
+admitted as slots and memory free up.
+
+Per mesh size the server keeps, once for all slots: the lattice, its Dirichlet markers,
+the node coordinates and a misfit (pointwise observations).  Per slot and size: the
+quadrature buffers and a ``SolvePlan`` (operator storage, Jacobi diagonal, PCG workspace;
+its iteration batches replay a captured CUDA graph).  The batch length of the graph is
+picked per mesh size by ``autotune`` (timed solves over a few candidates; the result of
+a solve does not depend on it).
+
+Work of a request (FP64 outer loops; FP32 operator and recurrence with FP64 reliable
+updates when ``precision="mixed"``):
+
+* ``forward``: ``m`` from the request's seed (the benchmark's cosine field, computed on
+  the device), its quadrature data, the residual at ``u = 0`` (Dirichlet data 0), one
+  Jacobi-PCG solve to ``rel_tolerance`` -> ``u``;
+* ``hessian``: the forward solve, the adjoint solve of the misfit, then the true
+  (misfit-only) Hessian action on ``v`` from the seed: ``C v``, ``W_um v``, ``W_mm v``
+  from one directional quadrature pass, the two incremental solves, ``C^T p^`` and
+  ``W_mu u^`` from the vector kernels -> ``H v`` (as ``ReducedHessian.TrueHessian``).
+
+Every kernel is deterministic, so a request's result does not depend on what else runs.
+"""
+
+import math
+import threading
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_ptr
+from .mesh import BoxMesh, DirichletBC, Q2Space
+from .modeling import DiscreteStateObservation, PointwiseStateObservation
+from .problem import STATE
+from .sparse import SolvePlan
+from .synthetic import field_params, interior_points
+
+
+class Request:
+    """One request: ``kind`` "forward" or "hessian", mesh ``n`` (n^3 elements), the
+    ``seed`` of its parameter field (and of ``v``), arrival time in seconds."""
+
+    __slots__ = ("kind", "n", "seed", "arrival", "t_admit", "t_done", "result", "iterations",
+                 "slot")
+
+    def __init__(self, kind, n, seed, arrival=0.0):
+        if kind not in ("forward", "hessian"):
+            raise ValueError("kind must be 'forward' or 'hessian'")
+        self.kind, self.n, self.seed, self.arrival = kind, int(n), int(seed), float(arrival)
+        self.t_admit = self.t_done = None
+        self.result = None
+        self.iterations = []
+        self.slot = None
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.arrival
+
+
+class _MeshState:
+    """Read-only state of one mesh size, shared by the slots."""
+
+    def __init__(self, n, device, nobs=256, sigma=0.1):
+        self.n = n
+        self.mesh = BoxMesh(n, device=device)
+        self.V = Q2Space(self.mesh)
+        self.bc = DirichletBC(self.V)
+        self.coords = torch.as_tensor(self.mesh.node_coords(), device=device)
+        pts = interior_points(nobs, seed=7)
+        self.misfit = PointwiseStateObservation(self.V, pts, data=np.zeros(nobs),
+                                                noise_variance=1e-4)
+        self.sigma = sigma
+
+    def field(self, seed):
+        a, w, phi = field_params(seed, self.sigma)
+        a = torch.as_tensor(a, device=self.coords.device)
+        w = torch.as_tensor(w.astype(np.float64), device=self.coords.device)
+        phi = torch.as_tensor(phi, device=self.coords.device)
+        return torch.cos(2.0 * math.pi * (self.coords @ w.T) + phi) @ a
+
+    def direction(self, seed):
+        g = torch.Generator(device="cpu").manual_seed(int(seed) + 7919)
+        return torch.randn(self.mesh.ndof, dtype=torch.float64, generator=g).to(self.coords.device)
+
+    def footprint(self, precision):
+        """Bytes of one slot's workspace for this size."""
+        nd, q = self.mesh.ndof, self.mesh.quad_bytes(_lib.HM_FP64)
+        jac = lib.hm_lattice_jacobian_bytes(self.mesh.handle, _lib.HM_FP64)
+        if precision == "mixed":
+            jac += lib.hm_lattice_jacobian_bytes(self.mesh.handle, _lib.HM_FP32)
+            work = lib.hm_pcg_mixed_workspace_bytes(nd)
+        else:
+            work = lib.hm_pcg_workspace_bytes(nd)
+        return int(2 * q + jac + work + 14 * 8 * nd)
+
+
+class _Workspace:
+    """One slot's resident buffers for one mesh size."""
+
+    def __init__(self, ms, precision, rtol, check_every):
+        self.ms = ms
+        mesh, dev = ms.mesh, ms.mesh.device
+        nq = (mesh.quad_bytes(_lib.HM_FP64) + 7) // 8
+        self.quad = torch.empty(nq, dtype=torch.float64, device=dev)
+        self.quad2 = torch.empty(nq, dtype=torch.float64, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.plan = SolvePlan(mesh, ms.bc.marker, precision, rel_tolerance=rtol,
+                              check_every=check_every)
+        nd = mesh.ndof
+        self.vec = {k: torch.zeros(nd, dtype=torch.float64, device=dev)
+                    for k in ("u", "p", "uh", "ph", "zero", "r1", "r2", "r3", "y")}
+        # the misfit keeps scratch of its own: one per workspace (slots run concurrently)
+        mis = ms.misfit
+        self.misfit = DiscreteStateObservation(mis.Bh, mis.d.cpu().numpy(), mis.noise_variance,
+                                               device=dev)
+        self.nbytes = ms.footprint(precision)
+        self.in_use = False
+        self.last_used = 0.0
+
+    # -- kernels of the path -------------------------------------------------------
+    def _quad(self, buf, u, m, p, mhat=None):
+        h = self.ms.mesh.handle
+        if mhat is None:
+            check(lib.hm_lattice_quadrature(h, ptr(u), ptr(m), ptr(p), _lib.HM_FP64, ptr(buf),
+                                            ptr(self.status), stream_ptr()), "hm_lattice_quadrature")
+        else:
+            check(lib.hm_lattice_quadrature_dir(h, ptr(u), ptr(m), ptr(p), ptr(mhat), _lib.HM_FP64,
+                                                ptr(buf), ptr(self.status), stream_ptr()),
+                  "hm_lattice_quadrature_dir")
+
+    def _vectors(self, buf, f, state=None, param=None, adj=None, zero_ess=False):
+        check(lib.hm_lattice_assemble(self.ms.mesh.handle, ptr(buf), _lib.HM_FP64, None,
+                                      ptr(self.ms.bc.marker), float(f), None, None, None, None,
+                                      ptr(state), ptr(param), ptr(adj), int(bool(zero_ess)),
+                                      stream_ptr()), "hm_lattice_assemble")
+
+    def _solve(self, out, rhs, req):
+        self.plan.solve(out, rhs)
+        req.iterations.append(self.plan.last.iterations)
+
+    def forward(self, m, req):
+        v = self.vec
+        z = v["zero"]
+        self._quad(self.quad, z, m, z)
+        self.plan.set_point(self.quad)
+        self._vectors(self.quad, 1.0, adj=self.plan.b, zero_ess=True)
+        self.plan.b.neg_()
+        self._solve(v["u"], self.plan.b, req)
+        return v["u"]
+
+    def hessian(self, m, x, req):
+        v, mask, mis = self.vec, self.ms.bc.mask, self.misfit
+        u = self.forward(m, req)
+        # adjoint: A^T p = -B^T (B u - d) / sigma^2
+        mis.grad(STATE, [u, m, None], v["r1"])
+        v["r1"].neg_().masked_fill_(mask, 0.0)
+        self._solve(v["p"], v["r1"], req)
+        p = v["p"]
+        # C x, W_um x, W_mm x from one directional pass (f = 0)
+        self._quad(self.quad2, u, m, p, mhat=x)
+        self._vectors(self.quad2, 0.0, state=v["r2"], param=v["y"], adj=v["r1"])
+        v["r1"].masked_fill_(mask, 0.0)                       # C x, rows eliminated
+        v["r2"].masked_fill_(mask, 0.0)                       # W_um x
+        self._solve(v["uh"], v["r1"], req)                    # A u^ = C x
+        mis.apply_ij(STATE, STATE, v["uh"], v["r3"])          # W_uu u^
+        v["r3"].sub_(v["r2"]).masked_fill_(mask, 0.0)
+        self._solve(v["ph"], v["r3"], req)                    # A^T p^ = W_uu u^ - W_um x
+        # y = W_mm x + C^T p^ - W_mu u^
+        self._quad(self.quad2, u, m, v["ph"].masked_fill_(mask, 0.0))
+        self._vectors(self.quad2, 0.0, param=v["r3"])
+        v["y"].add_(v["r3"])
+        self._quad(self.quad2, v["uh"].masked_fill_(mask, 0.0), m, p)
+        self._vectors(self.quad2, 0.0, param=v["r3"])
+        v["y"].sub_(v["r3"])
+        return v["y"]
+
+    def close(self):
+        self.plan.close()
+
+
+class Server:
+    """``Server(slots=4, precision="mixed", rel_tolerance=1e-8, memory_budget=None)``.
+
+    ``run(requests)`` feeds the requests at their arrival times (seconds from the call)
+    and returns when all are done; each request gets ``result`` (a host FP64 array),
+    ``t_admit``, ``t_done`` (seconds from the call), ``iterations`` and ``slot``.
+    ``memory_budget``: bytes the slots' workspaces may hold (default: half of the free
+    device memory)."""
+
+    def __init__(self, slots=4, precision="mixed", rel_tolerance=1e-8, memory_budget=None,
+                 device=None, check_every=None, keep_results=True):
+        self.device = torch.device(device if device is not None else "cuda")
+        self.slots = int(slots)
+        self.precision = precision
+        self.rtol = float(rel_tolerance)
+        if memory_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            memory_budget = free // 2
+        self.budget = int(memory_budget)
+        self.fixed_check_every = check_every
+        self.keep_results = keep_results
+        self.meshes = {}
+        self.tuned = {}
+        self._ws = {}            # (slot, n) -> _Workspace
+        self._resident = 0
+        self.peak_resident = 0
+        self._lock = threading.Condition()
+        self._streams = [torch.cuda.Stream(device=self.device) for _ in range(self.slots)]
+
+    # -- per-size state ------------------------------------------------------------
+    def mesh_state(self, n):
+        with self._lock:
+            ms = self.meshes.get(n)
+        if ms is None:
+            ms = _MeshState(n, self.device)
+            with self._lock:
+                ms = self.meshes.setdefault(n, ms)
+        return ms
+
+    def check_every(self, n):
+        if self.fixed_check_every is not None:
+            return int(self.fixed_check_every)
+        return self.tuned.get(n, 16)
+
+    def autotune(self, sizes, candidates=(4, 8, 16, 32), reps=3):
+        """Pick the graph batch length per mesh size: the fastest forward solve (CUDA
+        events, in a side stream, after one warm-up that captures the graph)."""
+        stream = torch.cuda.Stream(device=self.device)
+        for n in sizes:
+            ms = self.mesh_state(n)
+            best = None
+            for ce in candidates:
+                ws = _Workspace(ms, self.precision, self.rtol, ce)
+                req = Request("forward", n, 0)
+                with torch.cuda.stream(stream):
+                    m = ms.field(0)
+                    ws.forward(m, req)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for _ in range(reps):
+                        ws.forward(m, req)
+                    e1.record(stream)
+                stream.synchronize()
+                t = e0.elapsed_time(e1) / reps
+                ws.close()
+                del ws
+                if best is None or t < best[0]:
+                    best = (t, ce)
+            self.tuned[n] = best[1]
+        return dict(self.tuned)
+
+    # -- admission -------------------------------------------------------------------
+    def _acquire(self, slot, n):
+        """The slot's workspace for size n, created (and room made) when missing; blocks
+        while the budget has no room.  Under the lock."""
+        ws = self._ws.get((slot, n))
+        if ws is not None:
+            ws.in_use = True
+            return ws, None
+        need = self.mesh_state_locked(n).footprint(self.precision)
+        while self._resident + need > self.budget:
+            idle = [(w.last_used, k) for k, w in self._ws.items() if not w.in_use]
+            if idle:
+                _, k = min(idle)
+                w = self._ws.pop(k)
+                self._resident -= w.nbytes
+                w.close()
+                continue
+            if self._resident == 0:
+                raise MemoryError("a workspace for n=%d needs %d bytes, more than the budget"
+                                  % (n, need))
+            self._lock.wait()
+        self._resident += need
+        self.peak_resident = max(self.peak_resident, self._resident)
+        return None, need
+
+    def mesh_state_locked(self, n):
+        ms = self.meshes.get(n)
+        if ms is None:
+            self._lock.release()
+            try:
+                ms = self.mesh_state(n)
+            finally:
+                self._lock.acquire()
+        return ms
+
+    def _worker(self, slot, pending, t0, done):
+        stream = self._streams[slot]
+        while True:
+            with self._lock:
+                while not pending and not done["fed"]:
+                    self._lock.wait()
+                if not pending:
+                    return
+                req = pending.popleft()
+                ws, reserved = self._acquire(slot, req.n)
+            if ws is None:
+                ms = self.mesh_state(req.n)
+                with torch.cuda.stream(stream):
+                    ws = _Workspace(ms, self.precision, self.rtol, self.check_every(req.n))
+                ws.nbytes = reserved
+                ws.in_use = True
+                with self._lock:
+                    self._ws[(slot, req.n)] = ws
+            req.t_admit = time.perf_counter() - t0
+            req.slot = slot
+            ms = ws.ms
+            with torch.cuda.stream(stream):
+                m = ms.field(req.seed)
+                if req.kind == "forward":
+                    out = ws.forward(m, req)
+                else:
+                    out = ws.hessian(m, ms.direction(req.seed), req)
+                res = out.to("cpu", non_blocking=False) if self.keep_results else None
+                stream.synchronize()
+            req.result = res.numpy() if res is not None else None
+            req.t_done = time.perf_counter() - t0
+            with self._lock:
+                ws.in_use = False
+                ws.last_used = req.t_done
+                self._lock.notify_all()
+
+    def run(self, requests):
+        """Serve ``requests`` (arrival times in seconds from now); returns them."""
+        import collections
+
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for n in sorted({r.n for r in reqs}):
+            self.mesh_state(n)
+        pending = collections.deque()
+        done = {"fed": False}
+        t0 = time.perf_counter()
+        errors = []
+
+        def guarded(slot):
+            try:
+                self._worker(slot, pending, t0, done)
+            except BaseException as e:                    # noqa: BLE001
+                errors.append(e)
+                with self._lock:
+                    done["fed"] = True
+                    pending.clear()
+                    self._lock.notify_all()
+
+        threads = [threading.Thread(target=guarded, args=(k,), daemon=True)
+                   for k in range(self.slots)]
+        for t in threads:
+            t.start()
+        for r in reqs:
+            delay = r.arrival - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            with self._lock:
+                if errors:
+                    break
+                pending.append(r)
+                self._lock.notify_all()
+        with self._lock:
+            done["fed"] = True
+            self._lock.notify_all()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+        return reqs
+
+    def close(self):
+        with self._lock:
+            for w in self._ws.values():
+                w.close()
+            self._ws.clear()
+            self._resident = 0
+
+
+def latency_stats(requests):
+    lat = np.array([r.latency for r in requests if r.latency is not None])
+    span = max(r.t_done for r in requests) - min(r.arrival for r in requests)
+    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3), "requests_per_s": len(lat) / span,
+            "n": int(len(lat))}
+
+
+def poisson_trace(nreq, rate, sizes=(8, 12, 16, 24, 32, 48), p_forward=0.7, seed=0):
+    """``nreq`` requests with Poisson arrivals at ``rate`` per second, sizes uniform over
+    ``sizes``, 70% forward solves / 30% Hessian actions, one parameter seed each."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    n = rng.choice(sizes, nreq)
+    kind = np.where(rng.random(nreq) < p_forward, "forward", "hessian")
+    return [Request(k, int(nn), 1000 + i, float(ti)) for i, (k, nn, ti) in enumerate(zip(kind, n, t))]
+
+
+def plain_fp64(req, device=None, rel_tolerance=1e-8, cache=None):
+    """The same request through the library's plain per-request path: a fresh
+    ``PDEVariationalProblem`` / ``Model`` / ``ReducedHessian`` in FP64 on the default
+    stream (no resident workspace, no graphs).  The reference for the server's results
+    and the baseline of the serving benchmark."""
+    from .modeling import Model, ReducedHessian
+    from .problem import PDEVariationalProblem
+
+    cache = {} if cache is None else cache
+    ms = cache.get(req.n)
+    if ms is None:
+        ms = cache[req.n] = _MeshState(req.n, device or "cuda")
+    prob = PDEVariationalProblem([ms.V, ms.V, ms.V], f=1.0, bc=ms.bc, solver_tolerance=rel_tolerance,
+                                 matrix_free_solves=True, check_finite=False)
+    m = ms.field(req.seed)
+    u = ms.V.vector()
+    if req.kind == "forward":
+        prob.solveFwd(u, [u, m, None])
+        return u
+    model = Model(prob, None, ms.misfit)
+    p = ms.V.vector()
+    x = [u, m, p]
+    model.solveFwd(u, x)
+    model.solveAdj(p, x)
+    prob.setLinearizationPoint(x, matrix_free=True)
+    H = ReducedHessian(model)
+    y = ms.V.vector()
+    H.mult(ms.direction(req.seed), y)
+    return y

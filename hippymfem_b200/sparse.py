@@ -199,3 +199,84 @@ class MixedPCGSolver:
             return x
         check(rc, "hm_pcg_mixed")
         return x
+
+
+class SolvePlan:
+    """A resident solve workspace for one lattice and its Dirichlet nodes
+    (``hm_pcg_plan_*``): the operator storage of a point (FP64, plus FP32 for the
+    mixed-precision solve), the Jacobi diagonal, fixed right-hand side and solution
+    buffers and the PCG workspace.  ``set_point`` loads a point's quadrature data;
+    ``solve`` copies the right-hand side in, solves from zero and copies the solution
+    out.  Solves in a stream other than the legacy default stream replay a CUDA graph of
+    each batch of ``check_every`` iterations, captured on first use.  One host thread at
+    a time; the reference keeps its solver objects per operator the same way."""
+
+    def __init__(self, mesh, ess_marker, precision="fp64", rel_tolerance=1e-8, max_iter=20000,
+                 check_every=16, reliable_delta=0.1, max_updates=200):
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.mesh, self.ess, self.precision = mesh, ess_marker, precision
+        self.parameters = {"rel_tolerance": float(rel_tolerance), "max_iter": int(max_iter),
+                           "check_every": int(check_every), "reliable_delta": float(reliable_delta),
+                           "max_updates": int(max_updates)}
+        dev, n, h = mesh.device, mesh.ndof, mesh.handle
+
+        def buf(nbytes):
+            return torch.empty((int(nbytes) + 7) // 8, dtype=torch.float64, device=dev)
+
+        self.jac64 = buf(lib.hm_lattice_jacobian_bytes(h, _lib.HM_FP64))
+        self.jac32 = (buf(lib.hm_lattice_jacobian_bytes(h, _lib.HM_FP32))
+                      if precision == "mixed" else None)
+        self.diag = torch.empty(n, dtype=torch.float64, device=dev)
+        self.b = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.x = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.work = buf(lib.hm_pcg_mixed_workspace_bytes(n) if precision == "mixed"
+                        else lib.hm_pcg_workspace_bytes(n))
+        self.nbytes = sum(t.numel() * 8 for t in (self.jac64, self.jac32, self.diag, self.b,
+                                                  self.x, self.work) if t is not None)
+        self._plan = ctypes.c_void_p()
+        check(lib.hm_pcg_plan_create(h, ptr(self.jac64), ptr(self.jac32), ptr(ess_marker),
+                                     ptr(self.diag), ptr(self.b), ptr(self.x), ptr(self.work),
+                                     int(check_every), ctypes.byref(self._plan)),
+              "hm_pcg_plan_create")
+        self.last = None
+        self.last_updates = 0
+
+    def set_point(self, quad, stream=None):
+        """Load the operator of a point from its FP64 quadrature data."""
+        h, sp = self.mesh.handle, stream_ptr(stream)
+        check(lib.hm_lattice_jacobian_prepare(h, ptr(quad), _lib.HM_FP64, ptr(self.jac64),
+                                              _lib.HM_FP64, sp), "hm_lattice_jacobian_prepare")
+        if self.jac32 is not None:
+            check(lib.hm_lattice_jacobian_prepare(h, ptr(quad), _lib.HM_FP64, ptr(self.jac32),
+                                                  _lib.HM_FP32, sp), "hm_lattice_jacobian_prepare")
+        check(lib.hm_lattice_diag_A(h, ptr(quad), _lib.HM_FP64, ptr(self.ess), ptr(self.diag), sp),
+              "hm_lattice_diag_A")
+        return self
+
+    def solve(self, out, rhs, stream=None):
+        """``out = A^{-1} rhs`` (rhs zero on the Dirichlet nodes)."""
+        prm = self.parameters
+        if rhs is not self.b:
+            self.b.copy_(rhs)
+        it, nup, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        rc = lib.hm_pcg_plan_solve(self._plan, prm["rel_tolerance"], prm["reliable_delta"],
+                                   prm["max_updates"], prm["max_iter"], ctypes.byref(it),
+                                   ctypes.byref(nup), ctypes.byref(rr), stream_ptr(stream))
+        self.last = PCGResult(it.value, rr.value, rc == _lib.HM_OK)
+        self.last_updates = nup.value
+        check(rc, "hm_pcg_plan_solve")
+        if out is not None and out is not self.x:
+            out.copy_(self.x)
+        return out
+
+    def close(self):
+        if self._plan:
+            lib.hm_pcg_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:                                   # noqa: BLE001
+            pass

@@ -112,6 +112,16 @@ int hm_lattice_quadrature(const hm_lattice* h, const double* d_u, const double* 
                           const double* d_p, int precision, void* d_quad,
                           uint32_t* d_status, void* stream);
 
+/* The same quadrature data with D = w|J| e^m mhat: the derivative of the pointwise
+ * data along a parameter direction mhat.  Assembled by hm_lattice_assemble with f = 0,
+ * its vectors are the second-order products of the point (u, m, p) applied to mhat --
+ * ADJOINT: C mhat, STATE: W_um mhat, PARAMETER: W_mm mhat -- without any block formed:
+ * the matrix-free element HVP of the reference (hvp_block, hippymfem/fem/kernel.py:
+ * 1756-1782, behind apply_ij_at, modeling/PDEVariationalProblem.py:1672). */
+int hm_lattice_quadrature_dir(const hm_lattice* h, const double* d_u, const double* d_m,
+                              const double* d_p, const double* d_mhat, int precision,
+                              void* d_quad, uint32_t* d_status, void* stream);
+
 /* Fused assembly from quadrature data: the CSR values of the blocks whose pointer is
  * not NULL -- A = d2R/dp du (ADJOINT, STATE), C = d2R/dp dm (ADJOINT, PARAMETER),
  * Wum = d2R/du dm (STATE, PARAMETER), Wmm = d2R/dm dm -- in the lattice pattern
@@ -216,6 +226,25 @@ int hm_pcg_mixed(const hm_lattice* lattice, void* d_jac64, void* d_jac32, const 
                  const double* d_diag, const double* d_b, double* d_x, double rtol,
                  double delta, int max_updates, int maxiter, int check_every, void* d_work,
                  int* iterations, int* updates, double* relres, void* stream);
+
+/* A solve plan: one lattice Jacobian solve on fixed device buffers, for callers that
+ * solve again and again with the same operator storage (a request loop keeping one
+ * workspace per mesh size).  d_jac32 == NULL: FP64 Jacobi-PCG (d_work of
+ * hm_pcg_workspace_bytes); otherwise the mixed-precision solve of hm_pcg_mixed (d_work
+ * of hm_pcg_mixed_workspace_bytes).  The caller writes the right-hand side into d_b; a
+ * solve starts from x = 0 and leaves the solution in d_x.  The operator data behind
+ * d_jac64 / d_jac32 and d_diag may change between solves, the pointers may not.  A full
+ * batch of check_every iterations is captured once as a CUDA graph (on the first solve
+ * in a stream other than the legacy default stream) and replayed from then on.  A plan
+ * is used by one host thread at a time.  The iterative solves of solveFwd/solveAdj/
+ * solveIncremental (modeling/PDEVariationalProblem.py:1046-1609) on a resident workspace. */
+typedef struct hm_pcg_plan hm_pcg_plan;
+int hm_pcg_plan_create(const hm_lattice* lattice, void* d_jac64, void* d_jac32,
+                       const uint8_t* d_ess, const double* d_diag, double* d_b, double* d_x,
+                       void* d_work, int check_every, hm_pcg_plan** plan);
+int hm_pcg_plan_solve(hm_pcg_plan* plan, double rtol, double delta, int max_updates,
+                      int maxiter, int* iterations, int* updates, double* relres, void* stream);
+int hm_pcg_plan_destroy(hm_pcg_plan* plan);
 
 /* deterministic FP64 dot product into *d_out (a fixed-order two-pass reduction) */
 int64_t hm_dot_workspace_bytes(int64_t n);
