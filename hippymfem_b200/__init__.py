@@ -7,7 +7,8 @@ of ``include/hippymfem_b200.h``); importing this package fails if it is not buil
 
 from ._lib import HM_FP32, HM_FP64, NotConvergedError  # noqa: F401  (loads the library)
 from .mesh import BoxMesh, DirichletBC, Q2Space  # noqa: F401
-from .modeling import (DiscreteStateObservation, Model, PointwiseStateObservation,  # noqa: F401
+from .modeling import (BiLaplacianPrior, DiscreteStateObservation, Model,  # noqa: F401
+                       PointwiseStateObservation,
                        ReducedHessian, observation_operator)
 from .pattern import LatticePattern, build_tables  # noqa: F401
 from .problem import ADJOINT, NVAR, PARAMETER, STATE, PDEVariationalProblem  # noqa: F401

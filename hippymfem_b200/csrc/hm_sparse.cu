@@ -354,9 +354,13 @@ extern "C" int hm_dot(int64_t n, const double* x, const double* y, double* out, 
   return ok_or_cuda();
 }
 
+// slots for the partial sums of p.q: one per block of the lattice operator's gather
+// (at most n), or the fixed reduction grid after a CSR product
+inline int64_t pq_slots(int64_t n) { return n > kReduceBlocks ? n : (int64_t)kReduceBlocks; }
+
 extern "C" int64_t hm_pcg_workspace_bytes(int64_t n) {
-  // r, z, p, q, the partial sums of p.q (at most one per node), scalars, partials
-  return (int64_t)sizeof(double) * (5 * n + SC_N + 3 * (int64_t)kReduceBlocks + 8);
+  // r, z, p, q, the partial sums of p.q, scalars, partials
+  return (int64_t)sizeof(double) * (4 * n + pq_slots(n) + SC_N + 3 * (int64_t)kReduceBlocks + 8);
 }
 
 int hm_launch_apply_A_dot(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
@@ -470,7 +474,7 @@ int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, i
   T* p = wt + 2 * n;
   T* q = wt + 3 * n;
   double* pq_part = wd;
-  double* sc = wd + n;
+  double* sc = wd + pq_slots(n);
   double* part = sc + SC_N;
   if (check_every <= 0) check_every = 1;
   int64_t nparts = 0;
@@ -514,7 +518,7 @@ extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indi
 extern "C" int64_t hm_pcg_mixed_workspace_bytes(int64_t n) {
   // FP64: r, t, the p.q partials (at most one per node), scalars, partials, b.b;
   // FP32: x, r, z, p, q of the single-precision recurrence
-  return (int64_t)sizeof(double) * (3 * n + SC_N + 3 * (int64_t)kReduceBlocks + 8) +
+  return (int64_t)sizeof(double) * (2 * n + pq_slots(n) + SC_N + 3 * (int64_t)kReduceBlocks + 8) +
          (int64_t)sizeof(float) * (5 * n + 16);
 }
 
@@ -541,7 +545,7 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
   double* r64 = w;
   double* t64 = w + n;
   double* pq_part = w + 2 * n;
-  double* sc = w + 3 * n;
+  double* sc = pq_part + pq_slots(n);
   double* part = sc + SC_N;
   double* bbp = part + 3 * kReduceBlocks;
   float* f32 = reinterpret_cast<float*>(bbp + 8);

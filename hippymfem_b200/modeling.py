@@ -6,8 +6,8 @@ Mirrors, with the same method names and signs:
   hippymfem/modeling/misfit.py:65-125 and the observation operator of
   hippymfem/modeling/pointwiseObservation.py:36-224 (rows of Q2 basis values at the
   points), held as device CSR matrices ``B`` and ``B^T``;
-* ``Model`` -- the block dispatch of hippymfem/modeling/model.py:100-261 (misfit only:
-  the prior is not part of this path, so ``applyR`` is zero);
+* ``BiLaplacianPrior`` -- hippymfem/modeling/prior.py:894-952 (isotropic, natural BCs);
+* ``Model`` -- the block dispatch of hippymfem/modeling/model.py:100-261;
 * ``ReducedHessian`` -- hippymfem/modeling/reducedHessian.py:30-131.
 """
 
@@ -15,6 +15,7 @@ import numpy as np
 import scipy.sparse as sp
 import torch
 
+from . import _lib
 from ._lib import check, lib, ptr, stream_ptr
 from .problem import ADJOINT, PARAMETER, STATE
 
@@ -116,13 +117,128 @@ def PointwiseStateObservation(Vh, obs_points, data=None, noise_variance=None):
                                     noise_variance, device=mesh.device)
 
 
+class _BlockSolver:
+    """``x = M^{-1} b`` for an assembled SPD block (Jacobi-PCG, from zero)."""
+
+    def __init__(self, block, rel_tolerance, max_iter):
+        from .sparse import PCGSolver
+        self.pcg = PCGSolver(block, rel_tolerance=rel_tolerance, max_iter=max_iter)
+
+    def solve(self, x, b):
+        x.zero_()
+        self.pcg.solve(x, b)
+        return x
+
+
+class _BilaplacianR:
+    """``R = A M^{-1} A`` applied matrix-free (prior.py:319-350)."""
+
+    def __init__(self, A, Msolver):
+        self.A, self.Msolver = A, Msolver
+        self._t1 = torch.empty(A.nrow, dtype=torch.float64, device=A.values.device)
+        self._t2 = torch.empty_like(self._t1)
+
+    def mult(self, x, y):
+        self.A.mult(x, self._t1)
+        self.Msolver.solve(self._t2, self._t1)
+        self.A.mult(self._t2, y)
+        return y
+
+    multTranspose = mult
+
+
+class _BilaplacianRsolver:
+    """``R^{-1} = A^{-1} M A^{-1}`` (prior.py:353-373)."""
+
+    def __init__(self, Asolver, M):
+        self.Asolver, self.M = Asolver, M
+        self._t1 = torch.empty(M.nrow, dtype=torch.float64, device=M.values.device)
+        self._t2 = torch.empty_like(self._t1)
+
+    def solve(self, x, b):
+        self.Asolver.solve(self._t1, b)
+        self.M.mult(self._t1, self._t2)
+        self.Asolver.solve(x, self._t2)
+        return x
+
+
+class BiLaplacianPrior:
+    """Matern-class Gaussian prior with precision ``R = A M^{-1} A``,
+    ``A = gamma K + delta M`` (isotropic, natural boundary conditions):
+    BiLaplacianPrior of modeling/prior.py:894-952 (no ``Theta``, no Robin term, no
+    lumped mass).
+
+    The operators come from the fused assembly kernel on the lattice's pattern: ``gamma
+    K`` is the Jacobian block ``A`` at the constant field ``m = log gamma``, and
+    ``delta M`` the block ``W_mm`` at ``u = p = x`` (so that ``grad u . grad p = 1``) and
+    ``m = log delta``; no Dirichlet elimination.  Solves with ``A`` and ``M`` are
+    Jacobi-PCG to ``rel_tol``."""
+
+    def __init__(self, Vh, gamma, delta, mean=None, rel_tol=1e-12, max_iter=1000,
+                 robin_bc=False):
+        from .pattern import LatticePattern
+        from .problem import PDEVariationalProblem
+        from .sparse import CSRBlock
+
+        if robin_bc:
+            raise NotImplementedError("the Robin boundary term is not part of this prior")
+        if not (gamma > 0 and delta > 0):
+            raise ValueError("gamma and delta must be positive")
+        self.Vh = Vh
+        mesh = Vh.mesh
+        self.gamma, self.delta, self.robin_bc = float(gamma), float(delta), False
+        pat = LatticePattern(mesh)
+        prob = PDEVariationalProblem([Vh, Vh, Vh], f=0.0, check_finite=True)
+        prob._pattern = pat
+        x = torch.as_tensor(mesh.node_coords()[:, 0], device=mesh.device).contiguous()
+        zero = Vh.vector()
+        const = Vh.vector()
+
+        def block(name, u, logc, p):
+            const.fill_(float(logc))
+            quad = prob._quadrature([u, const, p], "prior")
+            vals = pat.new_values()
+            check(lib.hm_lattice_assemble(
+                mesh.handle, ptr(quad), _lib.HM_FP64, ptr(pat.indptr), None, 0.0,
+                ptr(vals) if name == "A" else None, None, None,
+                ptr(vals) if name == "Wmm" else None, None, None, None, 0, stream_ptr()),
+                "hm_lattice_assemble")
+            prob._require_finite("the prior's operators")
+            return vals
+
+        import math
+        K = block("A", zero, math.log(self.gamma), zero)
+        Md = block("Wmm", x, math.log(self.delta), x)
+        M1 = block("Wmm", x, 0.0, x)
+        self.A = CSRBlock(pat, K.add_(Md))
+        self.M = CSRBlock(pat, M1)
+        self.Msolver = _BlockSolver(self.M, rel_tol, max_iter)
+        self.Asolver = _BlockSolver(self.A, rel_tol, max_iter)
+        self.R = _BilaplacianR(self.A, self.Msolver)
+        self.Rsolver = _BilaplacianRsolver(self.Asolver, self.M)
+        self.mean = mean.clone() if mean is not None else Vh.vector()
+
+    def init_vector(self, x=None, dim=0):
+        return self.Vh.vector()
+
+    def cost(self, m):
+        """``1/2 (m - mean)^T R (m - mean)`` (prior.py:575-580)."""
+        d = m - self.mean
+        Rd = torch.empty_like(d)
+        self.R.mult(d, Rd)
+        return 0.5 * float(torch.dot(Rd, d))
+
+    def grad(self, m, out):
+        """``R (m - mean)`` (prior.py:582-586)."""
+        self.R.mult(m - self.mean, out)
+        return out
+
+
 class Model:
-    """``Model(problem, prior, misfit)``: the block dispatch of model.py (prior: the
-    ``R`` term is not part of this path; pass ``None``)."""
+    """``Model(problem, prior, misfit)``: the block dispatch of model.py:201-261; the prior
+    may be ``None`` (a misfit-only model: no regularization cost, gradient or ``R``)."""
 
     def __init__(self, problem, prior, misfit):
-        if prior is not None:
-            raise NotImplementedError("priors are not part of this path (misfit-only Hessian)")
         self.problem = problem
         self.prior = prior
         self.misfit = misfit
@@ -137,8 +253,10 @@ class Model:
         return gen[component]()
 
     def cost(self, x):
+        """``[total, regularization, misfit]`` at ``x`` (model.py:213-217)."""
         misfit = self.misfit.cost(x)
-        return [misfit, 0.0, misfit]
+        reg = self.prior.cost(x[PARAMETER]) if self.prior is not None else 0.0
+        return [misfit + reg, reg, misfit]
 
     def solveFwd(self, out, x):
         self.n_fwd_solve += 1
@@ -151,9 +269,20 @@ class Model:
         rhs.neg_()
         return self.problem.solveAdj(out, x, rhs)
 
-    def evalGradientParameter(self, x, mg, misfit_only=True):
+    def evalGradientParameter(self, x, mg, misfit_only=False):
+        """The cost's gradient in ``mg`` (model.py:219-236); returns its norm, the
+        discrete L2 norm ``sqrt(g^T M^{-1} g)`` with a prior, the Euclidean one
+        without."""
         self.problem.evalGradientParameter(x, mg)
-        return float(torch.sqrt(torch.dot(mg, mg)))
+        if self.prior is None:
+            return float(torch.sqrt(torch.dot(mg, mg)))
+        if not misfit_only:
+            tmp = self.problem.generate_parameter()
+            self.prior.grad(x[PARAMETER], tmp)
+            mg.add_(tmp)
+        g = self.problem.generate_parameter()
+        self.prior.Msolver.solve(g, mg)
+        return max(float(torch.dot(g, mg)), 0.0) ** 0.5
 
     def setPointForHessianEvaluations(self, x, gauss_newton_approx=False):
         self.gauss_newton_approx = bool(gauss_newton_approx)
@@ -195,14 +324,22 @@ class Model:
         return self._second_order(PARAMETER, PARAMETER, dm, out)
 
     def applyR(self, dm, out):
-        out.zero_()
-        return out
+        if self.prior is None:
+            out.zero_()
+            return out
+        return self.prior.R.mult(dm, out)
+
+    def Rsolver(self):
+        """The solver of the prior's precision (the Newton-CG preconditioner)."""
+        if self.prior is None:
+            raise ValueError("a misfit-only model has no prior precision")
+        return self.prior.Rsolver
 
 
 class ReducedHessian:
     """Matrix-free reduced Hessian at the point set on the model (reducedHessian.py)."""
 
-    def __init__(self, model, misfit_only=True):
+    def __init__(self, model, misfit_only=False):
         self.model = model
         self.gauss_newton_approx = model.gauss_newton_approx
         self.misfit_only = bool(misfit_only)

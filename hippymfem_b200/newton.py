@@ -1,0 +1,251 @@
+"""Inexact Newton-CG in the reduced parameter space, on the device.
+
+Semantics of the reference's ``ReducedSpaceNewtonCG`` (algorithms/NewtonCG.py:262-375,
+line-search globalization), its Steihaug CG (algorithms/cgsolverSteihaug.py:71-344,
+with the explicit reorthogonalization it uses by default) and its Armijo step
+(algorithms/linesearch.py:12-62): at Newton step k the system ``H mhat = -g`` is solved
+by preconditioned CG (preconditioner ``R^{-1}`` of the prior, identity without one)
+truncated at the Eisenstat-Walker tolerance ``min(cg_coarse_tolerance,
+sqrt(|g| / |g_0|))``; the first ``GN_iter`` steps use the Gauss-Newton Hessian; the step
+is accepted by Armijo backtracking.  Same parameters, defaults and termination codes.
+Vectors are FP64 torch tensors; every Hessian action is ``ReducedHessian.mult`` (two
+incremental solves on the device).
+"""
+
+import math
+
+import torch
+
+from .modeling import ReducedHessian
+from .problem import ADJOINT, PARAMETER, STATE
+
+
+def ReducedSpaceNewtonCG_ParameterList():
+    return {"rel_tolerance": 1e-6, "abs_tolerance": 1e-12, "gdm_tolerance": 1e-18,
+            "max_iter": 20, "globalization": "LS", "print_level": 0, "GN_iter": 5,
+            "cg_coarse_tolerance": 0.5, "cg_max_iter": 100, "cg_reorthogonalize": True,
+            "LS": {"c_armijo": 1e-4, "max_backtracking_iter": 10}}
+
+
+def CGSolverSteihaug_ParameterList():
+    return {"rel_tolerance": 1e-9, "abs_tolerance": 1e-12, "max_iter": 1000,
+            "zero_initial_guess": True, "print_level": 0, "reorthogonalize": False}
+
+
+class _Identity:
+    def solve(self, x, b):
+        x.copy_(b)
+        return x
+
+
+class CGSolverSteihaug:
+    """Preconditioned CG with Steihaug truncation (no trust region): stops on a
+    direction of nonpositive curvature (taking it whole at the first iteration), on the
+    relative/absolute residual in the preconditioner's norm, or at ``max_iter``."""
+
+    reason = ["Maximum Number of Iterations Reached", "Relative/Absolute residual less than tol",
+              "Reached a negative direction", "Reached trust region boundary"]
+
+    def __init__(self, parameters=None):
+        self.parameters = parameters if parameters is not None else CGSolverSteihaug_ParameterList()
+        self.A = None
+        self.B_solver = _Identity()
+        self.converged = False
+        self.iter = 0
+        self.reasonid = 0
+        self.final_norm = 0.0
+
+    def set_operator(self, A):
+        self.A = A
+        return self
+
+    def set_preconditioner(self, B_solver):
+        self.B_solver = B_solver if B_solver is not None else _Identity()
+        return self
+
+    def solve(self, x, b):
+        prm = self.parameters
+        self.iter, self.converged, self.reasonid = 0, False, 0
+        if prm["zero_initial_guess"]:
+            r = b.clone()
+            x.zero_()
+        else:
+            r = torch.empty_like(b)
+            self.A.mult(x, r)
+            r.neg_().add_(b)
+        z = torch.empty_like(b)
+        self.B_solver.solve(z, r)
+        d = z.clone()
+        Ad = torch.empty_like(b)
+        nom0 = nom = float(torch.dot(d, r))
+        basis = [(r.clone(), z.clone(), nom)] if prm["reorthogonalize"] else None
+        r0 = max(nom * prm["rel_tolerance"] ** 2, prm["abs_tolerance"] ** 2)
+        if nom <= r0:
+            self.converged, self.reasonid = True, 1
+            self.final_norm = math.sqrt(max(nom, 0.0))
+            return self.iter
+        self.A.mult(d, Ad)
+        den = float(torch.dot(Ad, d))
+        if den <= 0.0:
+            return self._negative_curvature(x, r, z, d, Ad, first=True)
+        self.iter = 1
+        while True:
+            alpha = nom / den
+            x.add_(d, alpha=alpha)
+            r.add_(Ad, alpha=-alpha)
+            if basis is not None:
+                for rj, zj, rho in basis:
+                    r.add_(rj, alpha=-float(torch.dot(r, zj)) / rho)
+            self.B_solver.solve(z, r)
+            betanom = float(torch.dot(r, z))
+            if betanom < r0:
+                self.converged, self.reasonid = True, 1
+                self.final_norm = math.sqrt(max(betanom, 0.0))
+                break
+            self.iter += 1
+            if self.iter > prm["max_iter"]:
+                self.converged, self.reasonid = False, 0
+                self.final_norm = math.sqrt(max(betanom, 0.0))
+                break
+            if basis is not None:
+                basis.append((r.clone(), z.clone(), betanom))
+            d.mul_(betanom / nom).add_(z)
+            self.A.mult(d, Ad)
+            den = float(torch.dot(d, Ad))
+            if den <= 0.0:
+                return self._negative_curvature(x, r, z, d, Ad, first=False)
+            nom = betanom
+        return self.iter
+
+    def _negative_curvature(self, x, r, z, d, Ad, first):
+        self.converged, self.reasonid = True, 2
+        if first:
+            x.add_(d)
+            r.sub_(Ad)
+            self.B_solver.solve(z, r)
+        self.final_norm = math.sqrt(max(float(torch.dot(r, z)), 0.0))
+        return self.iter
+
+
+def armijo_backtrack(model, x, x_star, mhat, mg_mhat, cost_old, alpha=1.0, c_armijo=1e-4,
+                     max_backtracking=10, gdm_tolerance=None, failures=(RuntimeError,)):
+    """Try ``x + alpha mhat``, halving ``alpha`` until the cost decreases enough
+    (linesearch.py:12-62); returns ``(accepted, alpha, n_backtrack, cost, fwd_failed)``."""
+    n_back, fwd_failed, cost = 0, False, None
+    while n_back < max_backtracking:
+        x_star[PARAMETER].copy_(x[PARAMETER]).add_(mhat, alpha=alpha)
+        x_star[STATE].copy_(x[STATE])
+        try:
+            model.solveFwd(x_star[STATE], x_star)
+            cost = list(model.cost(x_star))
+            fwd_failed = False
+        except failures:
+            cost = [cost_old + 1.0, float("nan"), float("nan")]
+            fwd_failed = True
+        if (cost[0] < cost_old + alpha * c_armijo * mg_mhat
+                or (gdm_tolerance is not None and -mg_mhat <= gdm_tolerance)):
+            x[PARAMETER].copy_(x_star[PARAMETER])
+            x[STATE].copy_(x_star[STATE])
+            return True, alpha, n_back, cost, fwd_failed
+        n_back += 1
+        alpha *= 0.5
+    return False, alpha, n_back, cost, fwd_failed
+
+
+class ReducedSpaceNewtonCG:
+    """``ReducedSpaceNewtonCG(model, parameters=None, callback=None).solve(x)`` with
+    ``x = [u, m, p]``; ``m`` is the initial guess and the result."""
+
+    termination_reasons = ["Maximum number of Iteration reached",
+                           "Norm of the gradient less than tolerance",
+                           "Maximum number of backtracking reached",
+                           "Norm of (g, dm) less than tolerance",
+                           "Forward solve failed during backtracking"]
+
+    def __init__(self, model, parameters=None, callback=None):
+        self.model = model
+        self.parameters = parameters if parameters is not None else ReducedSpaceNewtonCG_ParameterList()
+        self.callback = callback
+        self.it = 0
+        self.converged = False
+        self.total_cg_iter = 0
+        self.ncalls = 0
+        self.reason = 0
+        self.final_grad_norm = float("nan")
+        self.final_cost = float("nan")
+        self.history = []
+
+    def solve(self, x):
+        if self.parameters["globalization"] != "LS":
+            raise NotImplementedError("only the line-search globalization is built")
+        return self._solve_ls(x)
+
+    def _solve_ls(self, x):
+        p = self.parameters
+        rel_tol, abs_tol = p["rel_tolerance"], p["abs_tolerance"]
+        model = self.model
+        model.solveFwd(x[STATE], x)
+        self.it, self.converged = 0, False
+        self.ncalls += 1
+        mhat = model.generate_vector(PARAMETER)
+        mg = model.generate_vector(PARAMETER)
+        x_star = [model.generate_vector(STATE), model.generate_vector(PARAMETER), None]
+        cost_old = model.cost(x)[0]
+        cost_new = cost_old
+        gradnorm = gradnorm_ini = float("nan")
+        tol = abs_tol
+        while self.it < p["max_iter"] and not self.converged:
+            model.solveAdj(x[ADJOINT], x)
+            model.setPointForHessianEvaluations(x, gauss_newton_approx=(self.it < p["GN_iter"]))
+            gradnorm = model.evalGradientParameter(x, mg)
+            if self.it == 0:
+                gradnorm_ini = gradnorm
+                tol = max(abs_tol, gradnorm_ini * rel_tol)
+                if gradnorm_ini == 0.0:
+                    self.converged, self.reason = True, 1
+                    break
+            if gradnorm < tol and self.it > 0:
+                self.converged, self.reason = True, 1
+                break
+            self.it += 1
+            tolcg = min(p["cg_coarse_tolerance"], math.sqrt(gradnorm / gradnorm_ini))
+            H = ReducedHessian(model)
+            solver = CGSolverSteihaug()
+            solver.set_operator(H)
+            solver.set_preconditioner(model.Rsolver() if model.prior is not None else None)
+            solver.parameters.update({"rel_tolerance": tolcg, "max_iter": p["cg_max_iter"],
+                                      "zero_initial_guess": True,
+                                      "reorthogonalize": bool(p["cg_reorthogonalize"])})
+            solver.solve(mhat, -mg)
+            self.total_cg_iter += H.ncalls
+            mg_mhat = float(torch.dot(mg, mhat))
+            accepted, alpha, n_back, cost, fwd_failed = armijo_backtrack(
+                model, x, x_star, mhat, mg_mhat, cost_old, c_armijo=p["LS"]["c_armijo"],
+                max_backtracking=p["LS"]["max_backtracking_iter"],
+                gdm_tolerance=p["gdm_tolerance"])
+            if accepted:
+                cost_old = cost_new = cost[0]
+            self.history.append({"it": self.it, "cg_it": H.ncalls, "cost": cost[0],
+                                 "misfit": cost[2], "reg": cost[1], "gdm": mg_mhat,
+                                 "gradnorm": gradnorm, "alpha": alpha, "tolcg": tolcg})
+            if p["print_level"] >= 0:
+                h = self.history[-1]
+                if self.it == 1:
+                    print("\n%3s %5s %15s %15s %15s %15s %14s %14s %14s"
+                          % ("It", "cg_it", "cost", "misfit", "reg", "(g,dm)", "||g||", "alpha",
+                             "tolcg"), flush=True)
+                print("%3d %5d %15e %15e %15e %15e %14e %14e %14e"
+                      % (h["it"], h["cg_it"], h["cost"], h["misfit"], h["reg"], h["gdm"],
+                         h["gradnorm"], h["alpha"], h["tolcg"]), flush=True)
+            if self.callback:
+                self.callback(self.it, x)
+            if n_back == p["LS"]["max_backtracking_iter"]:
+                self.converged = False
+                self.reason = 4 if fwd_failed else 2
+                break
+            if -mg_mhat <= p["gdm_tolerance"]:
+                self.converged, self.reason = True, 3
+                break
+        self.final_grad_norm = gradnorm
+        self.final_cost = cost_new
+        return x

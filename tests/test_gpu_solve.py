@@ -163,3 +163,22 @@ def test_gradient_matches_adjoint_identity(cuda):
     prob.apply_ij(PARAMETER, ADJOINT, p, ctp)
     # dR/dm_k = sum_i C_ik p_i only holds for the unconstrained C: compare on the values
     assert (g - ctp).abs().max().item() <= 1e-12 * g.abs().max().item()
+
+
+@pytest.mark.parametrize("n", [(2, 2, 2), (4, 3, 5)])
+def test_small_assembled_solves(cuda, n):
+    """Systems smaller than the fixed reduction grid (here 125 and 693 dofs): the CSR
+    PCG's partial sums must not reach its scalars."""
+    from hippymfem_b200.sparse import PCGSolver
+
+    mesh, V, prob, model, m = _setup(n)
+    A, _ = prob._jacobian([None, m, None])
+    b = torch.as_tensor(np.random.default_rng(1).standard_normal(mesh.ndof), device=cuda)
+    prob.bc0.zero(b)
+    x = V.vector()
+    s = PCGSolver(A, rel_tolerance=1e-12)
+    s.solve(x, b)
+    assert s.last.converged and s.last.iterations > 0
+    r = V.vector()
+    A.mult(x, r)
+    assert float((r - b).norm()) <= 1e-10 * float(b.norm())
