@@ -113,4 +113,56 @@ HM_HD int64_t stencil_prefix(int i, int N) {
   return (i & 1) ? even + stencil_n(2 * k, N) : even;
 }
 
+// ------------------------------------------------------------ PCG device scalars
+// (shared by the solver and the operator kernels that finish a CG step's reductions)
+enum { SC_RZ = 0, SC_PQ, SC_ALPHA, SC_BETA, SC_RR, SC_BB, SC_TOL2, SC_CONV, SC_TMP0, SC_TMP1,
+       SC_TMP2, SC_IT, SC_N };
+
+#ifdef __CUDACC__
+// sum over the block (valid in thread 0); every thread of the block must call it
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;
+}
+
+// After thread 0 of every block has written its partial: true in the block that
+// finishes last (block-uniform).  The partials it then reads are complete; the
+// counter is reset by that block.  Which block is last does not change any result:
+// it sums the partials in a fixed order.
+__device__ __forceinline__ bool last_block(unsigned* counter) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  return last;
+}
+
+// alpha = r.z / p.q from the p.q partials (the last block of the product)
+__device__ __forceinline__ void finish_alpha(const double* part, unsigned nparts, double* sc,
+                                             unsigned* counter, double* sh) {
+  double t = 0.0;
+  for (unsigned b = threadIdx.x; b < nparts; b += blockDim.x) t += __ldcg(part + b);
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) {
+    sc[SC_PQ] = t;
+    const double a = sc[SC_RZ] / t;
+    sc[SC_ALPHA] = (sc[SC_CONV] >= 0.0 || t == 0.0 || !isfinite(a)) ? 0.0 : a;
+    *counter = 0u;
+  }
+}
+#endif
+
 }  // namespace hm

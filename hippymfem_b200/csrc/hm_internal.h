@@ -29,7 +29,9 @@ int hm_launch_apply_A(const hm::Lattice& L, void* jac, int precision, const uint
 int hm_launch_diag_A(const hm::Lattice& L, const void* quad, int precision,
                      const uint8_t* ess, double* diag, void* stream);
 int hm_launch_apply_A_dot(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
-                          const double* x, double* y, double* part, void* stream);
+                          const double* x, double* y, double* part, void* stream,
+                          double* sc = nullptr, unsigned* counter = nullptr);
 int64_t hm_apply_dot_parts(const hm::Lattice& L);
 int hm_launch_apply_A32_dot(const hm::Lattice& L, void* jac32, const uint8_t* ess, const float* x,
-                            float* y, double* part, void* stream);
+                            float* y, double* part, void* stream, double* sc = nullptr,
+                            unsigned* counter = nullptr);

@@ -335,52 +335,66 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-// One thread per node; with part != nullptr each block also
-// writes its partial sum of dotw . y (the p.q of a CG step), in a fixed order.
+// One thread per pair of x-neighbours (2m, 2m+1) of a node row (the row's last node,
+// 2n, alone), so that every lane of a warp runs the same loop: node 2m takes element
+// m-1 (local a1 = 2) and m (a1 = 0), node 2m+1 element m (a1 = 1); consecutive lanes
+// read consecutive elements of each Ye plane.  Per node the contributions are summed
+// over (z, y, x) element pairs with the lower element first, a fixed order.  With part
+// != nullptr each block also writes its partial sum of dotw . y (the p.q of a CG step).
+__device__ __forceinline__ void axis_elems(int i, int nel, int& e0, int& a0, int& cnt) {
+  if (i & 1) { e0 = i >> 1; a0 = 1; cnt = 1; }
+  else if (i == 0) { e0 = 0; a0 = 0; cnt = 1; }
+  else if ((i >> 1) >= nel) { e0 = (i >> 1) - 1; a0 = 2; cnt = 1; }
+  else { e0 = (i >> 1) - 1; a0 = 2; cnt = 2; }   // elements i/2-1 (a=2), i/2 (a=0)
+}
+
 template <typename real, typename vec>
 __global__ void __launch_bounds__(256)
     k_node_gather(Lattice L, const real* __restrict__ Ye, const uint8_t* __restrict__ ess,
                   const vec* __restrict__ xin, vec* __restrict__ yout,
-                  const vec* __restrict__ dotw, double* __restrict__ part) {
-  const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = n < (unsigned)L.ndof;
-  const unsigned nxy = n / (unsigned)L.Nx;
-  const int ix = (int)(n - nxy * (unsigned)L.Nx);
-  const int iz = (int)(nxy / (unsigned)L.Ny), iy = (int)(nxy - (unsigned)iz * (unsigned)L.Ny);
-  double yv = 0.0;
+                  const vec* __restrict__ dotw, double* __restrict__ part,
+                  double* __restrict__ sc, unsigned* __restrict__ counter) {
+  const unsigned per_row = (unsigned)L.nx + 1u;                  // pairs + the last node
+  const unsigned rows = (unsigned)L.Ny * (unsigned)L.Nz;
+  const unsigned task = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = task < rows * per_row;
+  const unsigned row = live ? task / per_row : 0u;
+  const unsigned m = live ? task - row * per_row : 0u;
+  const unsigned iz = row / (unsigned)L.Ny, iy = row - iz * (unsigned)L.Ny;
+  const bool last = m == (unsigned)L.nx;                          // node 2n alone
+  const unsigned n0 = row * (unsigned)L.Nx + 2u * m;              // node 2m
+  double dot = 0.0;
   if (live) {
-    if (ess != nullptr && ess[n]) {
-      yv = xin[n];
-    } else {
-      const int gi[3] = {ix, iy, iz};
-      const int nel[3] = {L.nx, L.ny, L.nz};
-      // per axis: up to two (element, local index) pairs
-      int e0[3], a0[3], cnt[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const int i = gi[d];
-        if (i & 1) { e0[d] = i >> 1; a0[d] = 1; cnt[d] = 1; }
-        else if (i == 0) { e0[d] = 0; a0[d] = 0; cnt[d] = 1; }
-        else if ((i >> 1) >= nel[d]) { e0[d] = (i >> 1) - 1; a0[d] = 2; cnt[d] = 1; }
-        else { e0[d] = (i >> 1) - 1; a0[d] = 2; cnt[d] = 2; }   // elements i/2-1 (a=2), i/2 (a=0)
+    int ey0, ay0, cy, ez0, az0, cz;
+    axis_elems((int)iy, L.ny, ey0, ay0, cy);
+    axis_elems((int)iz, L.nz, ez0, az0, cz);
+    const unsigned ne = (unsigned)L.ne, nx = (unsigned)L.nx;
+    const bool f0 = ess != nullptr && ess[n0];
+    const bool f1 = !last && ess != nullptr && ess[n0 + 1];
+    real acc0 = 0, acc1 = 0;
+    for (int c3 = 0; c3 < cz; ++c3)
+      for (int c2 = 0; c2 < cy; ++c2) {
+        const unsigned a23 = 3u * (unsigned)(c2 ? 0 : ay0) + 9u * (unsigned)(c3 ? 0 : az0);
+        const unsigned erow = nx * ((unsigned)(ey0 + c2) + (unsigned)L.ny * (unsigned)(ez0 + c3));
+        // node 2m: element m-1 (a1 = 2) then element m (a1 = 0); node 2m+1: element m
+        if (m > 0) acc0 += Ye[(size_t)(2u + a23) * ne + erow + m - 1u];
+        if (!last) {
+          acc0 += Ye[(size_t)a23 * ne + erow + m];
+          acc1 += Ye[(size_t)(1u + a23) * ne + erow + m];
+        }
       }
-      const unsigned ne = (unsigned)L.ne;
-      real acc = 0;
-      for (int c3 = 0; c3 < cnt[2]; ++c3)
-        for (int c2 = 0; c2 < cnt[1]; ++c2)
-          for (int c1 = 0; c1 < cnt[0]; ++c1) {
-            const unsigned ex = e0[0] + c1, ey = e0[1] + c2, ez = e0[2] + c3;
-            const unsigned a1 = c1 ? 0 : a0[0], a2 = c2 ? 0 : a0[1], a3 = c3 ? 0 : a0[2];
-            const unsigned e = ex + (unsigned)L.nx * (ey + (unsigned)L.ny * ez);
-            acc += Ye[(size_t)(a1 + 3 * a2 + 9 * a3) * ne + e];
-          }
-      yv = (double)acc;
+    const double y0 = f0 ? (double)xin[n0] : (double)acc0;
+    yout[n0] = (vec)y0;
+    if (dotw) dot = (double)dotw[n0] * y0;
+    if (!last) {
+      const double y1 = f1 ? (double)xin[n0 + 1] : (double)acc1;
+      yout[n0 + 1] = (vec)y1;
+      if (dotw) dot = fma((double)dotw[n0 + 1], y1, dot);
     }
-    yout[n] = (vec)yv;
   }
   if (part != nullptr) {
     __shared__ double sh[32];
-    double v = live ? (double)dotw[n] * yv : 0.0;
+    double v = dot;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
@@ -391,6 +405,8 @@ __global__ void __launch_bounds__(256)
       for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
       if (threadIdx.x == 0) part[blockIdx.x] = t;
     }
+    // a CG step: the last block takes alpha from the partials
+    if (sc != nullptr && last_block(counter)) finish_alpha(part, gridDim.x, sc, counter, sh);
   }
 }
 
@@ -442,6 +458,10 @@ using namespace hm;
 namespace {
 inline int grid1(int64_t n, int block) { return (int)((n + block - 1) / block); }
 inline cudaStream_t S_(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+// blocks of the gather: one thread per x-pair of every node row
+inline int gather_blocks(const Lattice& L) {
+  return grid1((int64_t)L.Ny * L.Nz * (L.nx + 1), 256);
+}
 }
 
 int hm_launch_pattern(const Lattice& L, int32_t* indptr, int32_t* indices, int32_t* slot, void* stream) {
@@ -483,17 +503,19 @@ int hm_launch_jacobian_prepare(const Lattice& L, const void* quad, int quad_prec
 
 template <typename real, typename vec>
 static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const vec* x,
-                          vec* y, const vec* dotw, double* part, void* stream) {
+                          vec* y, const vec* dotw, double* part, void* stream,
+                          double* sc = nullptr, unsigned* counter = nullptr) {
   real* Dq = static_cast<real*>(jac);
   real* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
   k_elem_apply<real, vec><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
-  k_node_gather<real, vec><<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L, Ye, ess, x, y, dotw, part);
+  k_node_gather<real, vec><<<gather_blocks(L), 256, 0, S_(stream)>>>(
+      L, Ye, ess, x, y, dotw, part, part != nullptr ? sc : nullptr, counter);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 
 // number of partial sums k_node_gather writes when asked for the fused dot product
-int64_t hm_apply_dot_parts(const Lattice& L) { return grid1(L.ndof, 256); }
+int64_t hm_apply_dot_parts(const Lattice& L) { return gather_blocks(L); }
 
 int hm_launch_apply_A(const Lattice& L, void* jac, int precision, const uint8_t* ess,
                       const double* x, double* y, void* stream) {
@@ -502,16 +524,20 @@ int hm_launch_apply_A(const Lattice& L, void* jac, int precision, const uint8_t*
   return launch_apply_t<double, double>(L, jac, ess, x, y, nullptr, nullptr, stream);
 }
 
+// with sc and counter the gather's last block also takes the CG step's alpha
 int hm_launch_apply_A_dot(const Lattice& L, void* jac, int precision, const uint8_t* ess,
-                          const double* x, double* y, double* part, void* stream) {
-  if (precision == HM_FP32) return launch_apply_t<float, double>(L, jac, ess, x, y, x, part, stream);
-  return launch_apply_t<double, double>(L, jac, ess, x, y, x, part, stream);
+                          const double* x, double* y, double* part, void* stream, double* sc,
+                          unsigned* counter) {
+  if (precision == HM_FP32)
+    return launch_apply_t<float, double>(L, jac, ess, x, y, x, part, stream, sc, counter);
+  return launch_apply_t<double, double>(L, jac, ess, x, y, x, part, stream, sc, counter);
 }
 
 // the FP32 operator on FP32 vectors (the inner solves of the mixed-precision PCG)
 int hm_launch_apply_A32_dot(const Lattice& L, void* jac32, const uint8_t* ess, const float* x,
-                            float* y, double* part, void* stream) {
-  return launch_apply_t<float, float>(L, jac32, ess, x, y, part ? x : nullptr, part, stream);
+                            float* y, double* part, void* stream, double* sc, unsigned* counter) {
+  return launch_apply_t<float, float>(L, jac32, ess, x, y, part ? x : nullptr, part, stream, sc,
+                                      counter);
 }
 
 int hm_launch_diag_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,

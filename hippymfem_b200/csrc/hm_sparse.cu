@@ -47,22 +47,6 @@ __global__ void k_csr_diag(int64_t nrow, const int32_t* __restrict__ indptr,
 }
 
 // ---------------------------------------------------------------- reductions
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  double t = 0.0;
-  if (threadIdx.x < 32) {
-    t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-  }
-  __syncthreads();
-  return t;  // valid in thread 0
-}
-
 __global__ void __launch_bounds__(kReduceThreads)
     k_dot_partial(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                   double* __restrict__ part) {
@@ -87,7 +71,6 @@ __global__ void k_reduce_final(const double* __restrict__ part, int nq, double* 
 
 // ----------------------------------------------------------------------- PCG
 // device scalars
-enum { SC_RZ = 0, SC_PQ, SC_ALPHA, SC_BETA, SC_RR, SC_BB, SC_TOL2, SC_CONV, SC_TMP0, SC_TMP1, SC_TMP2, SC_IT, SC_N };
 
 // Vector kernels, templated on the vector type T (double, or float for the inner solves
 // of the mixed-precision PCG); sums are accumulated in double.
@@ -148,12 +131,28 @@ __global__ void k_pcg_alpha(const double* __restrict__ part, int64_t nparts, dou
   }
 }
 
-// x += alpha p, r -= alpha q, z = r / diag; partials of r.z and r.r
+// beta = (r.z)_new / (r.z)_old, the convergence test and the iteration count (thread 0)
+__device__ __forceinline__ void beta_step(double rz, double rr, double* sc) {
+  const bool was = sc[SC_CONV] >= 0.0;
+  if (!was) {
+    const double it = sc[SC_IT] + 1.0;
+    sc[SC_IT] = it;
+    sc[SC_RR] = rr;
+    if (rr <= sc[SC_TOL2] * sc[SC_BB]) sc[SC_CONV] = it;
+    const double beta = sc[SC_RZ] == 0.0 ? 0.0 : rz / sc[SC_RZ];
+    sc[SC_BETA] = isfinite(beta) ? beta : 0.0;
+    sc[SC_RZ] = rz;
+  }
+}
+
+// x += alpha p, r -= alpha q, z = r / diag; partials of r.z and r.r; with counter, the
+// last block to finish takes the step's beta (else k_pcg_beta does)
 template <typename T>
 __global__ void __launch_bounds__(kReduceThreads)
-    k_pcg_update(int64_t n, const double* __restrict__ sc, T* __restrict__ x, T* __restrict__ r,
+    k_pcg_update(int64_t n, double* __restrict__ sc, T* __restrict__ x, T* __restrict__ r,
                  T* __restrict__ z, const T* __restrict__ p, const T* __restrict__ q,
-                 const double* __restrict__ diag, double* __restrict__ part) {
+                 const double* __restrict__ diag, double* __restrict__ part,
+                 unsigned* __restrict__ counter) {
   __shared__ double sh[32];
   const T alpha = (T)sc[SC_ALPHA];
   double rz = 0.0, rr = 0.0;
@@ -171,6 +170,19 @@ __global__ void __launch_bounds__(kReduceThreads)
     part[blockIdx.x] = rz;
     part[kReduceBlocks + blockIdx.x] = rr;
   }
+  if (counter != nullptr && last_block(counter)) {
+    double v0 = 0.0, v1 = 0.0;
+    for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) {
+      v0 += __ldcg(part + b);
+      v1 += __ldcg(part + kReduceBlocks + b);
+    }
+    v0 = block_sum(v0, sh);
+    v1 = block_sum(v1, sh);
+    if (threadIdx.x == 0) {
+      beta_step(v0, v1, sc);
+      *counter = 0u;
+    }
+  }
 }
 
 // the iteration count lives on the device (sc[SC_IT]), so that every batch of
@@ -183,18 +195,7 @@ __global__ void k_pcg_beta(const double* __restrict__ part, double* __restrict__
     for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) t += part[q * kReduceBlocks + b];
     v[q] = block_sum(t, sh);
   }
-  if (threadIdx.x == 0) {
-    const bool was = sc[SC_CONV] >= 0.0;
-    if (!was) {
-      const double it = sc[SC_IT] + 1.0;
-      sc[SC_IT] = it;
-      sc[SC_RR] = v[1];
-      if (v[1] <= sc[SC_TOL2] * sc[SC_BB]) sc[SC_CONV] = it;
-      const double beta = sc[SC_RZ] == 0.0 ? 0.0 : v[0] / sc[SC_RZ];
-      sc[SC_BETA] = isfinite(beta) ? beta : 0.0;
-      sc[SC_RZ] = v[0];
-    }
-  }
+  if (threadIdx.x == 0) beta_step(v[0], v[1], sc);
 }
 
 template <typename T>
@@ -363,11 +364,7 @@ extern "C" int64_t hm_pcg_workspace_bytes(int64_t n) {
   return (int64_t)sizeof(double) * (4 * n + pq_slots(n) + SC_N + 3 * (int64_t)kReduceBlocks + 8);
 }
 
-int hm_launch_apply_A_dot(const hm::Lattice& L, void* jac, int precision, const uint8_t* ess,
-                          const double* x, double* y, double* part, void* stream);
 int64_t hm_apply_dot_parts(const hm::Lattice& L);
-int hm_launch_apply_A32_dot(const hm::Lattice& L, void* jac32, const uint8_t* ess, const float* x,
-                            float* y, double* part, void* stream);
 int hm_pcg_operator(int64_t n, const int32_t* indptr, const int32_t* indices, const double* vals,
                     const hm::Lattice* L, const void* quad, int precision, const uint8_t* ess,
                     const double* x, double* y, void* stream);
@@ -387,11 +384,16 @@ struct PcgOp {
   const uint8_t* ess;
 };
 
-int op_apply(const PcgOp& o, const double* x, double* y, double* part, int64_t* nparts, void* stream) {
+// With sc and counter, the lattice operator's last block also takes the step's alpha
+// (*fused = true); the CSR product leaves it to k_pcg_alpha.
+int op_apply(const PcgOp& o, const double* x, double* y, double* part, int64_t* nparts, void* stream,
+             double* sc = nullptr, unsigned* counter = nullptr, bool* fused = nullptr) {
+  if (fused) *fused = false;
   if (o.L != nullptr) {
     if (part) {
       *nparts = hm_apply_dot_parts(*o.L);
-      return hm_launch_apply_A_dot(*o.L, o.jac, o.precision, o.ess, x, y, part, stream);
+      if (fused) *fused = sc != nullptr;
+      return hm_launch_apply_A_dot(*o.L, o.jac, o.precision, o.ess, x, y, part, stream, sc, counter);
     }
     return hm_pcg_operator(o.n, nullptr, nullptr, nullptr, o.L, o.jac, o.precision, o.ess, x, y, stream);
   }
@@ -402,23 +404,27 @@ int op_apply(const PcgOp& o, const double* x, double* y, double* part, int64_t* 
   return ok_or_cuda();
 }
 
-int op_apply(const PcgOp& o, const float* x, float* y, double* part, int64_t* nparts, void* stream) {
+int op_apply(const PcgOp& o, const float* x, float* y, double* part, int64_t* nparts, void* stream,
+             double* sc = nullptr, unsigned* counter = nullptr, bool* fused = nullptr) {
   if (part) *nparts = hm_apply_dot_parts(*o.L);
-  return hm_launch_apply_A32_dot(*o.L, o.jac, o.ess, x, y, part, stream);
+  if (fused) *fused = part != nullptr && sc != nullptr;
+  return hm_launch_apply_A32_dot(*o.L, o.jac, o.ess, x, y, part, stream, sc, counter);
 }
 
 // `count` PCG iterations (operator + fused p.q, alpha, update with r.z and r.r, beta,
 // direction); nothing in it synchronises with the host
+// cnt: two counters (zero between uses) for the reductions the producing kernels finish
 template <typename T>
 int pcg_batch(const PcgOp& o, const double* diag, T* x, T* r, T* z, T* p, T* q, double* pq_part,
-              double* sc, double* part, int count, cudaStream_t s) {
+              double* sc, double* part, unsigned* cnt, int count, cudaStream_t s) {
   int64_t np = 0;
   for (int j = 0; j < count; ++j) {
-    const int rc = op_apply(o, p, q, pq_part, &np, (void*)s);
+    bool fused = false;
+    const int rc = op_apply(o, p, q, pq_part, &np, (void*)s, sc, cnt, &fused);
     if (rc) return rc;
-    k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
-    k_pcg_update<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(o.n, sc, x, r, z, p, q, diag, part);
-    k_pcg_beta<<<1, 1024, 0, s>>>(part, sc);
+    if (!fused) k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
+    k_pcg_update<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(o.n, sc, x, r, z, p, q, diag, part,
+                                                               cnt + 1);
     k_pcg_pupdate<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(o.n, sc, z, p);
   }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
@@ -476,7 +482,9 @@ int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, i
   double* pq_part = wd;
   double* sc = wd + pq_slots(n);
   double* part = sc + SC_N;
+  unsigned* cnt = reinterpret_cast<unsigned*>(part + 3 * kReduceBlocks);
   if (check_every <= 0) check_every = 1;
+  if (cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), S_(stream)) != cudaSuccess) return HM_ERR_CUDA;
   int64_t nparts = 0;
   int rc = op_apply(o, x, q, nullptr, &nparts, stream);
   if (rc) return rc;
@@ -490,7 +498,7 @@ int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, i
     if (host[SC_CONV] >= 0.0 || it >= maxiter) break;
     const int count = it + check_every < maxiter ? check_every : maxiter - it;
     rc = run_batch(graph, count == check_every, s, [&] {
-      return pcg_batch<T>(o, diag, x, r, z, p, q, pq_part, sc, part, count, s);
+      return pcg_batch<T>(o, diag, x, r, z, p, q, pq_part, sc, part, cnt, count, s);
     });
     if (rc) return rc;
     it += count;
@@ -548,6 +556,7 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
   double* sc = pq_part + pq_slots(n);
   double* part = sc + SC_N;
   double* bbp = part + 3 * kReduceBlocks;
+  unsigned* cnt = reinterpret_cast<unsigned*>(bbp + 1);
   float* f32 = reinterpret_cast<float*>(bbp + 8);
   float* x32 = f32;
   float* r32 = f32 + n;
@@ -580,6 +589,7 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
     return read();
   };
   if (cudaMemsetAsync(sc, 0, sizeof(double) * SC_N, s) != cudaSuccess ||
+      cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), s) != cudaSuccess ||
       cudaMemsetAsync(x, 0, sizeof(double) * n, s) != cudaSuccess ||
       cudaMemsetAsync(x32, 0, sizeof(float) * n, s) != cudaSuccess)
     return HM_ERR_CUDA;
@@ -593,7 +603,7 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
   while (!conv) {
     const int count = it + check_every < maxiter ? check_every : maxiter - it;
     rc = run_batch(graph, count == check_every, s, [&] {
-      return pcg_batch<float>(o32, diag, x32, r32, z32, p32, q32, pq_part, sc, part, count, s);
+      return pcg_batch<float>(o32, diag, x32, r32, z32, p32, q32, pq_part, sc, part, cnt, count, s);
     });
     if (rc) return rc;
     it += count;
