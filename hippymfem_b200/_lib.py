@@ -69,6 +69,14 @@ SIGNATURES = {
     "hm_pcg_plan_solve": (_i32, [_p, _d, _d, _i32, _i32, _p, _p, _p, _p]),
     "hm_pcg_plan_destroy": (_i32, [_p]),
     "hm_lattice_quadrature_dir": (_i32, [_p, _p, _p, _p, _p, _i32, _p, _p, _p]),
+    "hm_mg_workspace_bytes": (_i64, [_p]),
+    "hm_mg_create": (_i32, [_p, _p, _i32, _i32, _p]),
+    "hm_mg_setup": (_i32, [_p, _p, _p, _p, _p]),
+    "hm_mg_apply": (_i32, [_p, _p, _p, _p]),
+    "hm_mg_levels": (_i32, [_p]),
+    "hm_mg_destroy": (_i32, [_p]),
+    "hm_pcg_mg": (_i32, [_p, _p, _p, _d, _i32, _i32, _p, _p, _p, _p]),
+    "hm_pcg_plan_set_mg": (_i32, [_p, _p]),
     "hm_dot_workspace_bytes": (_i64, [_i64]),
     "hm_dot": (_i32, [_i64, _p, _p, _p, _p, _p]),
 }

@@ -1,0 +1,499 @@
+// Geometric multigrid preconditioner for the lattice Jacobian (sm_100a).
+//
+// The structured-lattice counterpart of the BoomerAMG preconditioner the reference puts
+// in its Jacobian solves (algorithms/linSolvers.py:243-828): a symmetric V-cycle over
+//   level 0   the Q2 lattice itself (the matrix-free operator and its Jacobi diagonal),
+//   level 1   Q1 on the same elements (the Q2 lattice's vertices),
+//   level l   Q1 on elements coarsened 2:1 while every axis stays even and >= 4,
+// with Chebyshev-Jacobi smoothing (degree s before and after, the same polynomial, so the
+// cycle is symmetric and positive: a fixed linear preconditioner for CG) and a
+// Chebyshev solve of higher degree on the coarsest level.  Between any two levels the
+// node lattices are 2:1 (F = 2C - 1 nodes per axis: the Q1 space is nested in Q2 and in
+// the next finer Q1), so one trilinear prolongation P and its transpose R = P^T (full
+// weighting) serve every pair.  Coarse operators are rediscretised: Q1 stiffness with
+// one coefficient per element, the Gauss-weighted mean of e^m over the Q2 element
+// (level 1), the mean of the 8 children above.  The Dirichlet nodes must be the whole
+// boundary: eliminated rows are the identity on every level and restricted residuals
+// are zero there.  Everything is FP64, deterministic, and free of host
+// synchronisation after set-up, so a CG iteration with its V-cycle can be captured as a
+// CUDA graph.
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "hm_common.cuh"
+#include "hm_internal.h"
+
+namespace hm {
+
+struct MGLevel {
+  int nx, ny, nz;        // elements
+  int Nx, Ny, Nz;        // nodes per axis
+  double hx, hy, hz;     // element sizes
+  int64_t nodes, elems;
+  double* coef;          // per element (levels >= 1)
+  double* diag;          // Jacobi diagonal (level 0: the caller's)
+  double *x, *b, *r, *d, *t;
+  double theta;                  // Chebyshev: d0 = r / (theta diag)
+  double c1[40], c2[40];         // and the recurrence's coefficients
+  int degree;
+};
+
+}  // namespace hm
+
+struct hm_mg {
+  hm::Lattice L;
+  int nlev;
+  hm::MGLevel lv[16];
+  void* jac;             // level-0 operator data (FP64, from hm_lattice_jacobian_prepare)
+  const uint8_t* ess;
+  int degree, coarse_degree;
+  double* scratch;       // partial sums of the set-up's inner products
+};
+
+namespace hm {
+
+constexpr int kMGBlocks = 296;
+
+__device__ __forceinline__ bool on_boundary(int i, int j, int k, int Nx, int Ny, int Nz) {
+  return i == 0 || j == 0 || k == 0 || i == Nx - 1 || j == Ny - 1 || k == Nz - 1;
+}
+
+// y = A_l x for a Q1 level: node-centric, identity on the boundary, boundary values of
+// x taken as zero in the interior rows
+__global__ void __launch_bounds__(256) k_q1_apply(MGLevel lv, const double* __restrict__ x,
+                                                  double* __restrict__ y) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= lv.nodes) return;
+  const int i = (int)(n % lv.Nx);
+  const int64_t t = n / lv.Nx;
+  const int j = (int)(t % lv.Ny), k = (int)(t / lv.Ny);
+  if (on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz)) { y[n] = x[n]; return; }
+  // 1D element matrices: k = [1 -1; -1 1] / h, m = [2 1; 1 2] h / 6
+  const double kx[2] = {1.0 / lv.hx, -1.0 / lv.hx}, ky[2] = {1.0 / lv.hy, -1.0 / lv.hy},
+               kz[2] = {1.0 / lv.hz, -1.0 / lv.hz};
+  const double mx[2] = {lv.hx / 3.0, lv.hx / 6.0}, my[2] = {lv.hy / 3.0, lv.hy / 6.0},
+               mz[2] = {lv.hz / 3.0, lv.hz / 6.0};
+  double xs[3][3][3];
+#pragma unroll
+  for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+      for (int di = 0; di < 3; ++di) {
+        const int ii = i + di - 1, jj = j + dj - 1, kk = k + dk - 1;
+        xs[dk][dj][di] = on_boundary(ii, jj, kk, lv.Nx, lv.Ny, lv.Nz)
+                             ? 0.0 : x[ii + (int64_t)lv.Nx * (jj + (int64_t)lv.Ny * kk)];
+      }
+  double acc = 0.0;
+#pragma unroll
+  for (int e3 = 0; e3 < 2; ++e3)
+#pragma unroll
+    for (int e2 = 0; e2 < 2; ++e2)
+#pragma unroll
+      for (int e1 = 0; e1 < 2; ++e1) {
+        // element (i-1+e1, j-1+e2, k-1+e3); the node's local index is 1 - e
+        const double c = lv.coef[(i - 1 + e1) + (int64_t)lv.nx * ((j - 1 + e2) + (int64_t)lv.ny * (k - 1 + e3))];
+        double s = 0.0;
+#pragma unroll
+        for (int b3 = 0; b3 < 2; ++b3)
+#pragma unroll
+          for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+            for (int b1 = 0; b1 < 2; ++b1) {
+              // K[a][b] with a = 1 - e, so |a - b| = |1 - e - b|: entry 0 on the diagonal
+              const int o1 = (1 - e1) != b1, o2 = (1 - e2) != b2, o3 = (1 - e3) != b3;
+              const double kab = kx[o1] * my[o2] * mz[o3] + mx[o1] * ky[o2] * mz[o3] +
+                                 mx[o1] * my[o2] * kz[o3];
+              s = fma(kab, xs[e3 + b3][e2 + b2][e1 + b1], s);
+            }
+        acc = fma(c, s, acc);
+      }
+  y[n] = acc;
+}
+
+__global__ void k_q1_diag(MGLevel lv, double* __restrict__ diag) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= lv.nodes) return;
+  const int i = (int)(n % lv.Nx);
+  const int64_t t = n / lv.Nx;
+  const int j = (int)(t % lv.Ny), k = (int)(t / lv.Ny);
+  if (on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz)) { diag[n] = 1.0; return; }
+  const double kaa = (1.0 / lv.hx) * (lv.hy / 3.0) * (lv.hz / 3.0) +
+                     (lv.hx / 3.0) * (1.0 / lv.hy) * (lv.hz / 3.0) +
+                     (lv.hx / 3.0) * (lv.hy / 3.0) * (1.0 / lv.hz);
+  double c = 0.0;
+  for (int e3 = 0; e3 < 2; ++e3)
+    for (int e2 = 0; e2 < 2; ++e2)
+      for (int e1 = 0; e1 < 2; ++e1)
+        c += lv.coef[(i - 1 + e1) + (int64_t)lv.nx * ((j - 1 + e2) + (int64_t)lv.ny * (k - 1 + e3))];
+  diag[n] = c * kaa;
+}
+
+// level-1 coefficients: sum_q D(q) / |e| (D = w|J| e^m in the operator's SoA layout)
+__global__ void k_coef_from_q2(int64_t ne, const double* __restrict__ Dq, double inv_vol,
+                               double* __restrict__ coef) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) s += Dq[(int64_t)q * ne + e];
+  coef[e] = s * inv_vol;
+}
+
+// a coarse element's coefficient: the mean of its 8 children
+__global__ void k_coef_coarsen(MGLevel f, MGLevel c, const double* __restrict__ cf,
+                               double* __restrict__ cc) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= c.elems) return;
+  const int ex = (int)(e % c.nx);
+  const int64_t t = e / c.nx;
+  const int ey = (int)(t % c.ny), ez = (int)(t / c.ny);
+  double s = 0.0;
+  for (int z = 0; z < 2; ++z)
+    for (int y = 0; y < 2; ++y)
+      for (int x = 0; x < 2; ++x)
+        s += cf[(2 * ex + x) + (int64_t)f.nx * ((2 * ey + y) + (int64_t)f.ny * (2 * ez + z))];
+  cc[e] = 0.125 * s;
+}
+
+// b_c = R r_f (full weighting, the transpose of trilinear interpolation); 0 on the
+// coarse boundary
+__global__ void k_restrict(MGLevel f, MGLevel c, const double* __restrict__ rf,
+                           double* __restrict__ bc) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= c.nodes) return;
+  const int i = (int)(n % c.Nx);
+  const int64_t t = n / c.Nx;
+  const int j = (int)(t % c.Ny), k = (int)(t / c.Ny);
+  if (on_boundary(i, j, k, c.Nx, c.Ny, c.Nz)) { bc[n] = 0.0; return; }
+  const double w[3] = {0.5, 1.0, 0.5};
+  double s = 0.0;
+#pragma unroll
+  for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 3; ++dj) {
+      const double wjk = w[dj] * w[dk];
+      const int64_t row = (int64_t)f.Nx * ((2 * j + dj - 1) + (int64_t)f.Ny * (2 * k + dk - 1));
+#pragma unroll
+      for (int di = 0; di < 3; ++di) s = fma(wjk * w[di], rf[row + 2 * i + di - 1], s);
+    }
+  bc[n] = s;
+}
+
+// x_f += P x_c (trilinear); fine boundary nodes untouched
+__global__ void k_prolong_add(MGLevel f, MGLevel c, const double* __restrict__ xc,
+                              double* __restrict__ xf) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= f.nodes) return;
+  const int i = (int)(n % f.Nx);
+  const int64_t t = n / f.Nx;
+  const int j = (int)(t % f.Ny), k = (int)(t / f.Ny);
+  if (on_boundary(i, j, k, f.Nx, f.Ny, f.Nz)) return;
+  const int ci0 = i >> 1, cj0 = j >> 1, ck0 = k >> 1;
+  const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
+  const double wi = (i & 1) ? 0.5 : 1.0, wj = (j & 1) ? 0.5 : 1.0, wk = (k & 1) ? 0.5 : 1.0;
+  double s = 0.0;
+  for (int dk = 0; dk < nk; ++dk)
+    for (int dj = 0; dj < nj; ++dj)
+      for (int di = 0; di < ni; ++di)
+        s += xc[(ci0 + di) + (int64_t)c.Nx * ((cj0 + dj) + (int64_t)c.Ny * (ck0 + dk))];
+  xf[n] += wi * wj * wk * s;
+}
+
+// Chebyshev-Jacobi: start (r = b - t, or r = b with t == nullptr; d = r / (theta diag);
+// x = 0 when zero_x), step (x += d; r -= t; d = c1 d + c2 r / diag unless last), finish
+// (x += d)
+__global__ void k_cheb_start(int64_t n, const double* __restrict__ b, const double* __restrict__ t,
+                             const double* __restrict__ diag, double inv_theta, int zero_x,
+                             double* __restrict__ x, double* __restrict__ r, double* __restrict__ d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ri = t ? b[i] - t[i] : b[i];
+    r[i] = ri;
+    d[i] = inv_theta * ri / diag[i];
+    if (zero_x) x[i] = 0.0;
+  }
+}
+__global__ void k_cheb_step(int64_t n, double* __restrict__ x, double* __restrict__ d,
+                            double* __restrict__ r, const double* __restrict__ t,
+                            const double* __restrict__ diag, double c1, double c2, int last) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double di = d[i];
+    x[i] += di;
+    const double ri = r[i] - t[i];
+    r[i] = ri;
+    if (!last) d[i] = fma(c1, di, c2 * ri / diag[i]);
+  }
+}
+__global__ void k_cheb_finish(int64_t n, double* __restrict__ x, const double* __restrict__ d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += d[i];
+}
+
+// set-up: a deterministic pseudo-random start vector (0 on the boundary), partial sums of
+// a.b, and v = w / (s * diag)
+__global__ void k_mg_seed(MGLevel lv, double* __restrict__ v) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= lv.nodes) return;
+  const int i = (int)(n % lv.Nx);
+  const int64_t t = n / lv.Nx;
+  const int j = (int)(t % lv.Ny), k = (int)(t / lv.Ny);
+  uint64_t h = (uint64_t)n * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  h ^= h >> 31; h *= 0xBF58476D1CE4E5B9ull; h ^= h >> 29;
+  v[n] = on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz) ? 0.0 : (double)(h >> 11) * 0x1.0p-53 - 0.5;
+}
+__global__ void __launch_bounds__(256) k_mg_dot(int64_t n, const double* __restrict__ a,
+                                                const double* __restrict__ b,
+                                                const double* __restrict__ w,
+                                                double* __restrict__ part) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s = fma(a[i] * (w ? w[i] : 1.0), b[i], s);
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+__global__ void k_mg_scale_div(int64_t n, const double* __restrict__ w, const double* __restrict__ diag,
+                               double s, double* __restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = s * w[i] / diag[i];
+}
+
+}  // namespace hm
+
+using namespace hm;
+
+namespace {
+inline cudaStream_t S_(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+inline int blocks_for(int64_t n) { return (int)((n + 255) / 256); }
+
+int apply_level(hm_mg* mg, int l, const double* x, double* y, cudaStream_t s) {
+  if (l == 0) return hm_launch_apply_A(mg->L, mg->jac, HM_FP64, mg->ess, x, y, (void*)s);
+  const MGLevel& lv = mg->lv[l];
+  k_q1_apply<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, x, y);
+  return HM_OK;
+}
+
+// Chebyshev smoothing of A_l x = b: from x = 0 (zero_x) or from the given x; with
+// want_r the residual b - A x of the result is left in lv.r
+int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_r, int degree,
+           cudaStream_t s) {
+  MGLevel& lv = mg->lv[l];
+  int rc;
+  const int g = kMGBlocks;
+  if (zero_x) {
+    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, nullptr, lv.diag, 1.0 / lv.theta, 1, x, lv.r, lv.d);
+  } else {
+    if ((rc = apply_level(mg, l, x, lv.t, s))) return rc;
+    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, lv.t, lv.diag, 1.0 / lv.theta, 0, x, lv.r, lv.d);
+  }
+  for (int k = 1; k <= degree; ++k) {
+    const bool last = k == degree;
+    if (last && !want_r) {
+      k_cheb_finish<<<g, 256, 0, s>>>(lv.nodes, x, lv.d);
+      break;
+    }
+    if ((rc = apply_level(mg, l, lv.d, lv.t, s))) return rc;
+    k_cheb_step<<<g, 256, 0, s>>>(lv.nodes, x, lv.d, lv.r, lv.t, lv.diag, lv.c1[k], lv.c2[k], last ? 1 : 0);
+  }
+  return HM_OK;
+}
+
+int vcycle(hm_mg* mg, int l, const double* b, double* x, cudaStream_t s) {
+  int rc;
+  if (l == mg->nlev - 1) return smooth(mg, l, b, x, true, false, mg->coarse_degree, s);
+  MGLevel& lv = mg->lv[l];
+  MGLevel& cv = mg->lv[l + 1];
+  if ((rc = smooth(mg, l, b, x, true, true, mg->degree, s))) return rc;
+  k_restrict<<<blocks_for(cv.nodes), 256, 0, s>>>(lv, cv, lv.r, cv.b);
+  if ((rc = vcycle(mg, l + 1, cv.b, cv.x, s))) return rc;
+  k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, cv.x, x);
+  return smooth(mg, l, b, x, false, false, mg->degree, s);
+}
+
+// Chebyshev coefficients of a level for the interval [lo, hi] of D^{-1} A
+void set_interval(MGLevel& lv, double lo, double hi, int degree) {
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  lv.theta = theta;
+  lv.degree = degree;
+  for (int k = 1; k <= degree && k < 40; ++k) {
+    const double rho = 1.0 / (2.0 * sigma - rho_old);
+    lv.c1[k] = rho * rho_old;
+    lv.c2[k] = 2.0 * rho / delta;
+    rho_old = rho;
+  }
+}
+
+double host_dot(hm_mg* mg, int64_t n, const double* a, const double* b, const double* w,
+                cudaStream_t s, int* rc) {
+  k_mg_dot<<<kMGBlocks, 256, 0, s>>>(n, a, b, w, mg->scratch);
+  double h[kMGBlocks];
+  if (cudaMemcpyAsync(h, mg->scratch, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    *rc = HM_ERR_CUDA;
+    return 0.0;
+  }
+  double t = 0.0;
+  for (int i = 0; i < kMGBlocks; ++i) t += h[i];   // fixed order
+  return t;
+}
+
+// the level hierarchy of a lattice (no memory touched)
+int plan_levels(const Lattice& L, MGLevel* lv, int max_levels) {
+  int nl = 0;
+  MGLevel z{};
+  z.nx = L.nx; z.ny = L.ny; z.nz = L.nz;
+  z.Nx = L.Nx; z.Ny = L.Ny; z.Nz = L.Nz;
+  z.hx = L.hx; z.hy = L.hy; z.hz = L.hz;
+  z.nodes = L.ndof; z.elems = L.ne;
+  lv[nl++] = z;
+  MGLevel q = z;                       // Q1 on the same elements
+  q.Nx = L.nx + 1; q.Ny = L.ny + 1; q.Nz = L.nz + 1;
+  q.nodes = (int64_t)q.Nx * q.Ny * q.Nz;
+  if (L.nx < 2 || L.ny < 2 || L.nz < 2) return nl;
+  lv[nl++] = q;
+  while (nl < max_levels) {
+    const MGLevel& f = lv[nl - 1];
+    if ((f.nx & 1) || (f.ny & 1) || (f.nz & 1) || f.nx < 4 || f.ny < 4 || f.nz < 4) break;
+    MGLevel c{};
+    c.nx = f.nx / 2; c.ny = f.ny / 2; c.nz = f.nz / 2;
+    c.Nx = c.nx + 1; c.Ny = c.ny + 1; c.Nz = c.nz + 1;
+    c.hx = 2 * f.hx; c.hy = 2 * f.hy; c.hz = 2 * f.hz;
+    c.nodes = (int64_t)c.Nx * c.Ny * c.Nz;
+    c.elems = (int64_t)c.nx * c.ny * c.nz;
+    lv[nl++] = c;
+  }
+  return nl;
+}
+
+__global__ void k_count_mismatch(Lattice L, const uint8_t* __restrict__ ess, unsigned* __restrict__ bad) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= L.ndof) return;
+  const int i = (int)(n % L.Nx);
+  const int64_t t = n / L.Nx;
+  const int j = (int)(t % L.Ny), k = (int)(t / L.Ny);
+  const bool b = on_boundary(i, j, k, L.Nx, L.Ny, L.Nz);
+  if ((ess != nullptr && ess[n] != 0) != b) atomicAdd(bad, 1u);
+}
+}  // namespace
+
+int hm_mg_vcycle(hm_mg* mg, const double* r, double* z, void* stream) {
+  return vcycle(mg, 0, r, z, S_(stream));
+}
+const double* hm_mg_level0_diag(const hm_mg* mg) { return mg->lv[0].diag; }
+void* hm_mg_jac(const hm_mg* mg) { return mg->jac; }
+const uint8_t* hm_mg_ess(const hm_mg* mg) { return mg->ess; }
+const hm::Lattice* hm_mg_lattice(const hm_mg* mg) { return &mg->L; }
+
+extern "C" int64_t hm_mg_workspace_bytes(const hm_lattice* h) {
+  const Lattice* L = hm_lattice_geometry(h);
+  if (!L) return 0;
+  MGLevel lv[16];
+  const int nl = plan_levels(*L, lv, 16);
+  int64_t doubles = 3 * L->ndof + kMGBlocks + 32;
+  for (int l = 1; l < nl; ++l) doubles += lv[l].elems + 6 * lv[l].nodes + 8;
+  return doubles * (int64_t)sizeof(double);
+}
+
+extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coarse_degree,
+                            hm_mg** out) {
+  const Lattice* L = hm_lattice_geometry(h);
+  if (!L || !work || !out || degree < 1 || degree > 30 || coarse_degree < 1 || coarse_degree > 39)
+    return HM_ERR_ARG;
+  hm_mg* mg = new (std::nothrow) hm_mg();
+  if (!mg) return HM_ERR_NOMEM;
+  mg->L = *L;
+  mg->degree = degree;
+  mg->coarse_degree = coarse_degree;
+  mg->nlev = plan_levels(*L, mg->lv, 16);
+  double* w = static_cast<double*>(work);
+  auto take = [&](int64_t n) { double* p = w; w += n; return p; };
+  mg->scratch = take(kMGBlocks + 32);
+  MGLevel& z = mg->lv[0];
+  z.r = take(L->ndof); z.d = take(L->ndof); z.t = take(L->ndof);
+  z.x = z.b = nullptr; z.coef = nullptr; z.diag = nullptr;
+  for (int l = 1; l < mg->nlev; ++l) {
+    MGLevel& lv = mg->lv[l];
+    lv.coef = take(lv.elems);
+    lv.diag = take(lv.nodes);
+    lv.x = take(lv.nodes); lv.b = take(lv.nodes); lv.r = take(lv.nodes);
+    lv.d = take(lv.nodes); lv.t = take(lv.nodes);
+    w += 8;
+  }
+  *out = mg;
+  return HM_OK;
+}
+
+// the point's operator: coefficients, diagonals and eigenvalue bounds (synchronises)
+extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const double* diag,
+                           void* stream) {
+  if (!mg || !jac || !ess || !diag) return HM_ERR_ARG;
+  cudaStream_t s = S_(stream);
+  const Lattice& L = mg->L;
+  // the Dirichlet nodes must be exactly the boundary
+  unsigned* bad = reinterpret_cast<unsigned*>(mg->scratch + kMGBlocks);
+  if (cudaMemsetAsync(bad, 0, sizeof(unsigned), s) != cudaSuccess) return HM_ERR_CUDA;
+  k_count_mismatch<<<blocks_for(L.ndof), 256, 0, s>>>(L, ess, bad);
+  unsigned hbad = 0;
+  if (cudaMemcpyAsync(&hbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return HM_ERR_CUDA;
+  if (hbad != 0) return HM_ERR_UNSUPPORTED;
+  mg->jac = jac;
+  mg->ess = ess;
+  mg->lv[0].diag = const_cast<double*>(diag);
+  // coefficients and diagonals of the Q1 levels
+  if (mg->nlev > 1) {
+    MGLevel& q = mg->lv[1];
+    k_coef_from_q2<<<blocks_for(L.ne), 256, 0, s>>>(L.ne, static_cast<const double*>(jac),
+                                                    1.0 / (L.hx * L.hy * L.hz), q.coef);
+    for (int l = 2; l < mg->nlev; ++l)
+      k_coef_coarsen<<<blocks_for(mg->lv[l].elems), 256, 0, s>>>(mg->lv[l - 1], mg->lv[l],
+                                                                  mg->lv[l - 1].coef, mg->lv[l].coef);
+    for (int l = 1; l < mg->nlev; ++l)
+      k_q1_diag<<<blocks_for(mg->lv[l].nodes), 256, 0, s>>>(mg->lv[l], mg->lv[l].diag);
+  }
+  if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
+  // largest eigenvalue of D^{-1} A per level: power iteration with the Rayleigh quotient
+  // v.Av / v.Dv (12 steps from a fixed start); smoothing interval [hi/4, hi], the coarsest
+  // level's solve on [hi/64, hi]
+  int rc = HM_OK;
+  for (int l = 0; l < mg->nlev; ++l) {
+    MGLevel& lv = mg->lv[l];
+    double* v = lv.d;
+    double* w = lv.t;
+    k_mg_seed<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, v);
+    double lam = 1.0;
+    for (int it = 0; it < 12; ++it) {
+      if ((rc = apply_level(mg, l, v, w, s))) return rc;
+      const double vav = host_dot(mg, lv.nodes, v, w, nullptr, s, &rc);
+      const double vdv = host_dot(mg, lv.nodes, v, v, lv.diag, s, &rc);
+      if (rc) return rc;
+      if (!(vdv > 0.0)) break;
+      lam = vav / vdv;
+      const double ww = host_dot(mg, lv.nodes, w, w, nullptr, s, &rc);
+      if (rc) return rc;
+      if (!(ww > 0.0)) break;
+      k_mg_scale_div<<<kMGBlocks, 256, 0, s>>>(lv.nodes, w, lv.diag, 1.0 / std::sqrt(ww), v);
+    }
+    const double hi = 1.1 * lam;
+    const bool coarsest = l == mg->nlev - 1;
+    set_interval(lv, coarsest ? hi / 64.0 : hi / 4.0, hi, coarsest ? mg->coarse_degree : mg->degree);
+  }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+extern "C" int hm_mg_apply(hm_mg* mg, const double* r, double* z, void* stream) {
+  if (!mg || !r || !z || !mg->jac) return HM_ERR_ARG;
+  const int rc = vcycle(mg, 0, r, z, S_(stream));
+  if (rc) return rc;
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+extern "C" int hm_mg_levels(const hm_mg* mg) { return mg ? mg->nlev : 0; }
+
+extern "C" int hm_mg_destroy(hm_mg* mg) {
+  delete mg;
+  return HM_OK;
+}

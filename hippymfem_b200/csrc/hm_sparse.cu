@@ -207,6 +207,70 @@ __global__ void k_pcg_pupdate(int64_t n, const double* __restrict__ sc, const T*
     p[i] = fma(beta, p[i], z[i]);
 }
 
+// x += alpha p, r -= alpha q; partials of r.r (for a preconditioner applied after it)
+__global__ void __launch_bounds__(kReduceThreads)
+    k_pcg_update_rr(int64_t n, const double* __restrict__ sc, double* __restrict__ x,
+                    double* __restrict__ r, const double* __restrict__ p,
+                    const double* __restrict__ q, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const double alpha = sc[SC_ALPHA];
+  double rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] = fma(alpha, p[i], x[i]);
+    const double ri = fma(-alpha, q[i], r[i]);
+    r[i] = ri;
+    rr = fma(ri, ri, rr);
+  }
+  rr = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[kReduceBlocks + blockIdx.x] = rr;
+}
+
+// partials of r.z; the last block takes beta from them and the r.r partials
+__global__ void __launch_bounds__(kReduceThreads)
+    k_pcg_rz_beta(int64_t n, const double* __restrict__ r, const double* __restrict__ z,
+                  double* __restrict__ part, unsigned* __restrict__ counter,
+                  double* __restrict__ sc) {
+  __shared__ double sh[32];
+  double rz = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    rz = fma(r[i], z[i], rz);
+  rz = block_sum(rz, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = rz;
+  if (last_block(counter)) {
+    double v0 = 0.0, v1 = 0.0;
+    for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) {
+      v0 += __ldcg(part + b);
+      v1 += __ldcg(part + kReduceBlocks + b);
+    }
+    v0 = block_sum(v0, sh);
+    v1 = block_sum(v1, sh);
+    if (threadIdx.x == 0) {
+      beta_step(v0, v1, sc);
+      *counter = 0u;
+    }
+  }
+}
+
+// r = b - q; partials of r.r and b.b (slots 1 and 2)
+__global__ void __launch_bounds__(kReduceThreads)
+    k_pcg_mg_init(int64_t n, const double* __restrict__ b, const double* __restrict__ q,
+                  double* __restrict__ r, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double rr = 0.0, bb = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ri = b[i] - q[i];
+    r[i] = ri;
+    rr = fma(ri, ri, rr);
+    bb = fma(b[i], b[i], bb);
+  }
+  rr = block_sum(rr, sh);
+  bb = block_sum(bb, sh);
+  if (threadIdx.x == 0) {
+    part[kReduceBlocks + blockIdx.x] = rr;
+    part[2 * kReduceBlocks + blockIdx.x] = bb;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kReduceThreads)
     k_dot_partial_t(int64_t n, const T* __restrict__ a, const T* __restrict__ b, double* __restrict__ part) {
@@ -523,6 +587,80 @@ extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indi
                          relres, stream);
 }
 
+int hm_mg_vcycle(hm_mg* mg, const double* r, double* z, void* stream);
+const double* hm_mg_level0_diag(const hm_mg* mg);
+void* hm_mg_jac(const hm_mg* mg);
+const uint8_t* hm_mg_ess(const hm_mg* mg);
+const hm::Lattice* hm_mg_lattice(const hm_mg* mg);
+
+namespace {
+// PCG preconditioned by a multigrid V-cycle (the operator and diagonal are the MG's
+// level 0); work as for hm_pcg.  x is the initial guess.
+int pcg_mg_run(hm_mg* mg, const double* b, double* x, double rtol, int maxiter, int check_every,
+               void* work, int* iterations, double* relres, void* stream, HmBatchGraph* graph) {
+  const hm::Lattice* L = hm_mg_lattice(mg);
+  if (!L || !hm_mg_jac(mg)) return HM_ERR_ARG;
+  const int64_t n = L->ndof;
+  cudaStream_t s = S_(stream);
+  PcgOp o{n, nullptr, nullptr, nullptr, L, hm_mg_jac(mg), HM_FP64, hm_mg_ess(mg)};
+  double* w = static_cast<double*>(work);
+  double* r = w;
+  double* z = w + n;
+  double* p = w + 2 * n;
+  double* q = w + 3 * n;
+  double* pq_part = w + 4 * n;
+  double* sc = pq_part + pq_slots(n);
+  double* part = sc + SC_N;
+  unsigned* cnt = reinterpret_cast<unsigned*>(part + 3 * kReduceBlocks);
+  if (check_every <= 0) check_every = 1;
+  if (cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), s) != cudaSuccess) return HM_ERR_CUDA;
+  int64_t np = 0;
+  int rc = op_apply(o, x, q, nullptr, &np, stream);
+  if (rc) return rc;
+  k_pcg_mg_init<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, q, r, part);
+  if ((rc = hm_mg_vcycle(mg, r, z, stream))) return rc;
+  k_dot_partial_t<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, part);
+  k_pcg_init_final<<<1, 1024, 0, s>>>(part, sc, rtol);
+  if (cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return HM_ERR_CUDA;
+  double host[SC_N];
+  int it = 0;
+  for (;;) {
+    if (cudaMemcpyAsync(host, sc, sizeof(host), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HM_ERR_CUDA;
+    if (host[SC_CONV] >= 0.0 || it >= maxiter) break;
+    const int count = it + check_every < maxiter ? check_every : maxiter - it;
+    rc = run_batch(graph, count == check_every, s, [&]() -> int {
+      for (int j = 0; j < count; ++j) {
+        bool fused = false;
+        int e = op_apply(o, p, q, pq_part, &np, (void*)s, sc, cnt, &fused);
+        if (e) return e;
+        if (!fused) k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
+        k_pcg_update_rr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, p, q, part);
+        if ((e = hm_mg_vcycle(mg, r, z, (void*)s))) return e;
+        k_pcg_rz_beta<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, part, cnt + 1, sc);
+        k_pcg_pupdate<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z, p);
+      }
+      return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+    });
+    if (rc) return rc;
+    it += count;
+  }
+  const bool conv = host[SC_CONV] >= 0.0;
+  if (iterations) *iterations = conv ? (int)host[SC_CONV] : it;
+  if (relres) *relres = host[SC_BB] > 0.0 ? std::sqrt(host[SC_RR] / host[SC_BB]) : 0.0;
+  return conv ? HM_OK : HM_ERR_NOCONV;
+}
+}  // namespace
+
+extern "C" int hm_pcg_mg(hm_mg* mg, const double* b, double* x, double rtol, int maxiter,
+                         int check_every, void* work, int* iterations, double* relres,
+                         void* stream) {
+  if (!mg || !b || !x || !work || maxiter < 0) return HM_ERR_ARG;
+  return pcg_mg_run(mg, b, x, rtol, maxiter, check_every, work, iterations, relres, stream,
+                    nullptr);
+}
+
 extern "C" int64_t hm_pcg_mixed_workspace_bytes(int64_t n) {
   // FP64: r, t, the p.q partials (at most one per node), scalars, partials, b.b;
   // FP32: x, r, z, p, q of the single-precision recurrence
@@ -649,6 +787,7 @@ struct hm_pcg_plan {
   double* x;
   void* work;
   int check_every;
+  hm_mg* mg;            // non-NULL: MG-preconditioned FP64 solves
   HmBatchGraph graph;
 };
 
@@ -668,7 +807,18 @@ extern "C" int hm_pcg_plan_create(const hm_lattice* h, void* jac64, void* jac32,
   p->x = x;
   p->work = work;
   p->check_every = check_every;
+  p->mg = nullptr;
   *plan = p;
+  return HM_OK;
+}
+
+extern "C" int hm_pcg_plan_set_mg(hm_pcg_plan* p, hm_mg* mg) {
+  if (!p || (mg && p->jac32 != nullptr)) return HM_ERR_ARG;
+  if (p->graph.exec) {
+    cudaGraphExecDestroy(p->graph.exec);
+    p->graph.exec = nullptr;
+  }
+  p->mg = mg;
   return HM_OK;
 }
 
@@ -676,6 +826,13 @@ extern "C" int hm_pcg_plan_solve(hm_pcg_plan* p, double rtol, double delta, int 
                                  int maxiter, int* iterations, int* updates, double* relres,
                                  void* stream) {
   if (!p || maxiter < 0) return HM_ERR_ARG;
+  if (p->mg != nullptr) {
+    if (updates) *updates = 0;
+    if (cudaMemsetAsync(p->x, 0, sizeof(double) * p->L.ndof, S_(stream)) != cudaSuccess)
+      return HM_ERR_CUDA;
+    return pcg_mg_run(p->mg, p->b, p->x, rtol, maxiter, p->check_every, p->work, iterations,
+                      relres, stream, &p->graph);
+  }
   if (p->jac32 != nullptr)
     return pcg_mixed_run(&p->L, p->jac64, p->jac32, p->ess, p->diag, p->b, p->x, rtol, delta,
                          max_updates, maxiter, p->check_every, p->work, iterations, updates,

@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import check, lib, ptr, stream_ptr
 from .mesh import DirichletBC
 from .pattern import LatticePattern
-from .sparse import CSRBlock, MatrixFreeJacobian, MixedPCGSolver, PCGSolver
+from .sparse import CSRBlock, MatrixFreeJacobian, MGPCGSolver, MixedPCGSolver, PCGSolver
 
 STATE, PARAMETER, ADJOINT = 0, 1, 2
 NVAR = 3
@@ -67,6 +67,9 @@ class PDEVariationalProblem:
     check_finite : read the device status word after each assembly and raise
         ``RuntimeError`` on non-finite values (``require_finite_arrays``,
         modeling/PDEVariationalProblem.py:1844-1892); one synchronisation each.
+    preconditioner : ``"jacobi"`` or ``"mg"`` (the lattice's geometric multigrid V-cycle,
+        in place of the reference's BoomerAMG; FP64 matrix-free solves, Dirichlet nodes
+        on the whole boundary).
     solver_precision : ``"fp64"``, or ``"mixed"``: Jacobi-PCG whose recurrence runs in
         FP32 with the FP32 matrix-free operator, re-anchored to the FP64 true residual
         each time it falls by ``reliable_delta``, to the same tolerance (in place of the
@@ -75,7 +78,7 @@ class PDEVariationalProblem:
 
     def __init__(self, Vh, f=1.0, bc=None, bc0=None, is_fwd_linear=True, solver_tolerance=1e-12,
                  matrix_free_solves=False, check_finite=True, max_iter=50000,
-                 solver_precision="fp64", reliable_delta=0.1):
+                 solver_precision="fp64", reliable_delta=0.1, preconditioner="jacobi"):
         if len(Vh) != NVAR:
             raise ValueError("Vh must have %d entries" % NVAR)
         self.Vh = list(Vh)
@@ -93,7 +96,13 @@ class PDEVariationalProblem:
             raise ValueError("solver_precision must be 'fp64' or 'mixed'")
         self.solver_precision = solver_precision
         self.reliable_delta = float(reliable_delta)
-        self.matrix_free_solves = bool(matrix_free_solves) or solver_precision == "mixed"
+        if preconditioner not in ("jacobi", "mg"):
+            raise ValueError("preconditioner must be 'jacobi' or 'mg'")
+        if preconditioner == "mg" and solver_precision != "fp64":
+            raise ValueError("the multigrid preconditioner is for FP64 solves")
+        self.preconditioner = preconditioner
+        self.matrix_free_solves = (bool(matrix_free_solves) or solver_precision == "mixed"
+                                   or preconditioner == "mg")
         self.check_finite = bool(check_finite)
         self.max_iter = int(max_iter)
         self.precision = _lib.HM_FP64
@@ -222,6 +231,8 @@ class PDEVariationalProblem:
         return blocks["A"]
 
     def _get_solver(self, A):
+        if self.preconditioner == "mg":
+            return MGPCGSolver(A, rel_tolerance=self.solver_tolerance, max_iter=self.max_iter)
         if self.solver_precision == "mixed":
             return MixedPCGSolver(A, self._jac_cache[2], rel_tolerance=self.solver_tolerance,
                                   reliable_delta=self.reliable_delta, max_iter=self.max_iter)

@@ -212,7 +212,7 @@ class SolvePlan:
     a time; the reference keeps its solver objects per operator the same way."""
 
     def __init__(self, mesh, ess_marker, precision="fp64", rel_tolerance=1e-8, max_iter=20000,
-                 check_every=16, reliable_delta=0.1, max_updates=200):
+                 check_every=16, reliable_delta=0.1, max_updates=200, multigrid=False):
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.mesh, self.ess, self.precision = mesh, ess_marker, precision
@@ -241,6 +241,13 @@ class SolvePlan:
               "hm_pcg_plan_create")
         self.last = None
         self.last_updates = 0
+        self.mg = None
+        if multigrid:
+            if precision != "fp64":
+                raise ValueError("the multigrid plan is FP64")
+            self.mg = Multigrid(mesh)
+            self.nbytes += self.mg.work.numel() * 8
+            check(lib.hm_pcg_plan_set_mg(self._plan, self.mg._mg), "hm_pcg_plan_set_mg")
 
     def set_point(self, quad, stream=None):
         """Load the operator of a point from its FP64 quadrature data."""
@@ -252,6 +259,8 @@ class SolvePlan:
                                                   _lib.HM_FP32, sp), "hm_lattice_jacobian_prepare")
         check(lib.hm_lattice_diag_A(h, ptr(quad), _lib.HM_FP64, ptr(self.ess), ptr(self.diag), sp),
               "hm_lattice_diag_A")
+        if self.mg is not None:
+            self.mg.setup(self.jac64, self.ess, self.diag, stream)
         return self
 
     def solve(self, out, rhs, stream=None):
@@ -274,9 +283,78 @@ class SolvePlan:
         if self._plan:
             lib.hm_pcg_plan_destroy(self._plan)
             self._plan = ctypes.c_void_p()
+        if getattr(self, "mg", None) is not None:
+            self.mg.close()
 
     def __del__(self):
         try:
             self.close()
         except Exception:                                   # noqa: BLE001
             pass
+
+
+class Multigrid:
+    """The lattice Jacobian's geometric multigrid V-cycle (``hm_mg_*``): hierarchy and
+    level storage on one workspace; ``setup`` loads a point's FP64 operator data (again
+    whenever the point changes); ``apply(r, z)`` is ``z = V(r)``."""
+
+    def __init__(self, mesh, degree=2, coarse_degree=24):
+        self.mesh = mesh
+        nbytes = lib.hm_mg_workspace_bytes(mesh.handle)
+        self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=mesh.device)
+        self._mg = ctypes.c_void_p()
+        check(lib.hm_mg_create(mesh.handle, ptr(self.work), int(degree), int(coarse_degree),
+                               ctypes.byref(self._mg)), "hm_mg_create")
+        self.levels = lib.hm_mg_levels(self._mg)
+
+    def setup(self, jac64, ess, diag, stream=None):
+        check(lib.hm_mg_setup(self._mg, ptr(jac64), ptr(ess), ptr(diag), stream_ptr(stream)),
+              "hm_mg_setup")
+        return self
+
+    def apply(self, r, z, stream=None):
+        check(lib.hm_mg_apply(self._mg, ptr(r), ptr(z), stream_ptr(stream)), "hm_mg_apply")
+        return z
+
+    def close(self):
+        if self._mg:
+            lib.hm_mg_destroy(self._mg)
+            self._mg = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:                                   # noqa: BLE001
+            pass
+
+
+class MGPCGSolver:
+    """PCG for ``A x = b`` with the matrix-free FP64 Jacobian, preconditioned by the
+    geometric multigrid V-cycle (``hm_pcg_mg``) -- in place of the reference's
+    BoomerAMG-preconditioned hypre PCG (algorithms/linSolvers.py:243-828, 709)."""
+
+    def __init__(self, operator, rel_tolerance=1e-12, max_iter=2000, check_every=4,
+                 degree=2, coarse_degree=24, raise_on_fail=True):
+        if not isinstance(operator, MatrixFreeJacobian) or operator.precision != _lib.HM_FP64:
+            raise TypeError("the multigrid solve needs the FP64 matrix-free Jacobian")
+        self.op = operator
+        self.parameters = {"rel_tolerance": float(rel_tolerance), "max_iter": int(max_iter),
+                           "check_every": int(check_every)}
+        self.raise_on_fail = raise_on_fail
+        self.mg = Multigrid(operator.mesh, degree, coarse_degree)
+        self.mg.setup(operator.jac, operator.ess, operator._diag)
+        nbytes = lib.hm_pcg_workspace_bytes(operator.nrow)
+        self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=operator.mesh.device)
+        self.last = None
+
+    def solve(self, x, b, stream=None):
+        prm = self.parameters
+        it, rr = ctypes.c_int(), ctypes.c_double()
+        rc = lib.hm_pcg_mg(self.mg._mg, ptr(b), ptr(x), prm["rel_tolerance"], prm["max_iter"],
+                           prm["check_every"], ptr(self.work), ctypes.byref(it), ctypes.byref(rr),
+                           stream_ptr(stream))
+        self.last = PCGResult(it.value, rr.value, rc == _lib.HM_OK)
+        if rc == _lib.HM_ERR_NOCONV and not self.raise_on_fail:
+            return x
+        check(rc, "hm_pcg_mg")
+        return x

@@ -246,6 +246,34 @@ int hm_pcg_plan_solve(hm_pcg_plan* plan, double rtol, double delta, int max_upda
                       int maxiter, int* iterations, int* updates, double* relres, void* stream);
 int hm_pcg_plan_destroy(hm_pcg_plan* plan);
 
+/* Geometric multigrid preconditioner for the lattice Jacobian, the structured-lattice
+ * counterpart of the BoomerAMG preconditioner of the reference's solves
+ * (algorithms/linSolvers.py:243-828): a symmetric V-cycle Q2 -> Q1 on the same elements
+ * -> Q1 coarsened 2:1 while every axis stays even and >= 4, Chebyshev-Jacobi smoothing
+ * of `degree` before and after, a Chebyshev solve of `coarse_degree` on the coarsest
+ * level, trilinear transfers, coarse operators rediscretised with element-mean
+ * coefficients.  FP64.  The Dirichlet nodes must be the whole boundary
+ * (HM_ERR_UNSUPPORTED otherwise).
+ *   hm_mg_create: the hierarchy on d_work (hm_mg_workspace_bytes);
+ *   hm_mg_setup: a point's operator -- d_jac64 of hm_lattice_jacobian_prepare (FP64),
+ *     its markers and Jacobi diagonal (hm_lattice_diag_A); estimates the smoothers'
+ *     eigenvalue bounds (synchronises the stream); again whenever the point changes;
+ *   hm_mg_apply: z = V-cycle(r);
+ *   hm_pcg_mg: PCG with the V-cycle (x: initial guess; d_work of hm_pcg_workspace_bytes);
+ *   hm_pcg_plan_set_mg: a plan's FP64 solves use it (graph-captured with the V-cycle). */
+typedef struct hm_mg hm_mg;
+int64_t hm_mg_workspace_bytes(const hm_lattice* lattice);
+int hm_mg_create(const hm_lattice* lattice, void* d_work, int degree, int coarse_degree,
+                 hm_mg** mg);
+int hm_mg_setup(hm_mg* mg, void* d_jac64, const uint8_t* d_ess, const double* d_diag,
+                void* stream);
+int hm_mg_apply(hm_mg* mg, const double* d_r, double* d_z, void* stream);
+int hm_mg_levels(const hm_mg* mg);
+int hm_mg_destroy(hm_mg* mg);
+int hm_pcg_mg(hm_mg* mg, const double* d_b, double* d_x, double rtol, int maxiter,
+              int check_every, void* d_work, int* iterations, double* relres, void* stream);
+int hm_pcg_plan_set_mg(hm_pcg_plan* plan, hm_mg* mg);
+
 /* deterministic FP64 dot product into *d_out (a fixed-order two-pass reduction) */
 int64_t hm_dot_workspace_bytes(int64_t n);
 int hm_dot(int64_t n, const double* d_x, const double* d_y, double* d_out, void* d_work,
