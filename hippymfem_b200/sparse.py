@@ -330,8 +330,11 @@ class Multigrid:
 
 class MGPCGSolver:
     """PCG for ``A x = b`` with the matrix-free FP64 Jacobian, preconditioned by the
-    geometric multigrid V-cycle (``hm_pcg_mg``) -- in place of the reference's
-    BoomerAMG-preconditioned hypre PCG (algorithms/linSolvers.py:243-828, 709)."""
+    geometric multigrid V-cycle -- in place of the reference's BoomerAMG-preconditioned
+    hypre PCG (algorithms/linSolvers.py:243-828, 709).  It runs as a solve plan on the
+    operator's own storage (``hm_pcg_plan_*`` with ``hm_pcg_plan_set_mg``): in a stream
+    other than the legacy default stream every batch of iterations, V-cycles included,
+    replays a captured CUDA graph.  ``x`` is overwritten (the solve starts from zero)."""
 
     def __init__(self, operator, rel_tolerance=1e-12, max_iter=2000, check_every=4,
                  degree=2, coarse_degree=24, raise_on_fail=True):
@@ -341,20 +344,40 @@ class MGPCGSolver:
         self.parameters = {"rel_tolerance": float(rel_tolerance), "max_iter": int(max_iter),
                            "check_every": int(check_every)}
         self.raise_on_fail = raise_on_fail
-        self.mg = Multigrid(operator.mesh, degree, coarse_degree)
+        mesh = operator.mesh
+        self.mg = Multigrid(mesh, degree, coarse_degree)
         self.mg.setup(operator.jac, operator.ess, operator._diag)
-        nbytes = lib.hm_pcg_workspace_bytes(operator.nrow)
-        self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=operator.mesh.device)
+        n = operator.nrow
+        self.b = torch.zeros(n, dtype=torch.float64, device=mesh.device)
+        self.x = torch.zeros(n, dtype=torch.float64, device=mesh.device)
+        nbytes = lib.hm_pcg_workspace_bytes(n)
+        self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=mesh.device)
+        self._plan = ctypes.c_void_p()
+        check(lib.hm_pcg_plan_create(mesh.handle, ptr(operator.jac), None, ptr(operator.ess),
+                                     ptr(operator._diag), ptr(self.b), ptr(self.x), ptr(self.work),
+                                     int(check_every), ctypes.byref(self._plan)), "hm_pcg_plan_create")
+        check(lib.hm_pcg_plan_set_mg(self._plan, self.mg._mg), "hm_pcg_plan_set_mg")
         self.last = None
 
     def solve(self, x, b, stream=None):
         prm = self.parameters
-        it, rr = ctypes.c_int(), ctypes.c_double()
-        rc = lib.hm_pcg_mg(self.mg._mg, ptr(b), ptr(x), prm["rel_tolerance"], prm["max_iter"],
-                           prm["check_every"], ptr(self.work), ctypes.byref(it), ctypes.byref(rr),
-                           stream_ptr(stream))
+        self.b.copy_(b)
+        it, nup, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        rc = lib.hm_pcg_plan_solve(self._plan, prm["rel_tolerance"], 0.1, 1, prm["max_iter"],
+                                   ctypes.byref(it), ctypes.byref(nup), ctypes.byref(rr),
+                                   stream_ptr(stream))
         self.last = PCGResult(it.value, rr.value, rc == _lib.HM_OK)
         if rc == _lib.HM_ERR_NOCONV and not self.raise_on_fail:
+            x.copy_(self.x)
             return x
-        check(rc, "hm_pcg_mg")
+        check(rc, "hm_pcg_plan_solve")
+        x.copy_(self.x)
         return x
+
+    def __del__(self):
+        try:
+            if self._plan:
+                lib.hm_pcg_plan_destroy(self._plan)
+                self._plan = ctypes.c_void_p()
+        except Exception:                                   # noqa: BLE001
+            pass

@@ -112,3 +112,25 @@ def test_plan_with_multigrid_replays_the_same_solve(cuda):
         assert torch.equal(x, outs[0])
     assert float((outs[0] - ref).norm()) <= 1e-12 * float(ref.norm())
     plan.close()
+
+
+def test_c_abi_mg_pcg_matches_the_plan(cuda):
+    """hm_pcg_mg (initial guess zero) against the plan-based solver."""
+    import ctypes
+
+    from hippymfem_b200._lib import check, lib, ptr, stream_ptr
+    from hippymfem_b200.sparse import MGPCGSolver
+
+    mesh, V, prob, m, A = _jacobian((8, 10, 12), seed=5)
+    b = _interior(mesh, V, prob.bc0.mask, 7)
+    s = MGPCGSolver(A, rel_tolerance=1e-12)
+    ref = V.vector()
+    s.solve(ref, b)
+    work = torch.empty(lib.hm_pcg_workspace_bytes(mesh.ndof) // 8 + 1, dtype=torch.float64,
+                       device=cuda)
+    x = V.vector()
+    it, rr = ctypes.c_int(), ctypes.c_double()
+    check(lib.hm_pcg_mg(s.mg._mg, ptr(b), ptr(x), 1e-12, 200, 4, ptr(work), ctypes.byref(it),
+                        ctypes.byref(rr), stream_ptr()))
+    assert it.value == s.last.iterations
+    assert torch.equal(x, ref)
