@@ -213,6 +213,19 @@ def run_reference(a):
 
 
 # ------------------------------------------------------------------------- ours
+def _capacity(srv, sizes, poisson_trace, n=240):
+    """Requests/s of a burst from the serving mix, all arriving at once, after a first
+    burst has created every slot's workspaces and captured its graphs."""
+    from hippymfem_b200.serving import latency_stats
+
+    for seed in (10, 11):
+        burst = poisson_trace(n, 1e9, sizes, seed=seed)
+        for r in burst:
+            r.arrival = 0.0
+        srv.run(burst)
+    return latency_stats(burst)["requests_per_s"]
+
+
 def run_serving(nreq, dev, sizes=(8, 12, 16, 24, 32, 48), slots=4, plain_sample=200):
     """The serving configuration: requests on n^3 meshes, n uniform over ``sizes``, 70%
     forward solves (Jacobi-PCG to rtol 1e-8) / 30% Hessian actions, Poisson arrivals at
@@ -226,12 +239,7 @@ def run_serving(nreq, dev, sizes=(8, 12, 16, 24, 32, 48), slots=4, plain_sample=
     srv = Server(slots=slots, precision="mixed", rel_tolerance=1e-8, device=dev,
                  keep_results=False)
     tuned = srv.autotune(sizes, candidates=(8, 16, 32), reps=2)
-    # capacity: a burst of requests from the same mix, all arriving at once
-    burst = poisson_trace(120, 1e9, sizes, seed=11)
-    for r in burst:
-        r.arrival = 0.0
-    srv.run(burst)
-    capacity = latency_stats(burst)["requests_per_s"]
+    capacity = _capacity(srv, sizes, poisson_trace)
     trace = poisson_trace(nreq, 0.8 * capacity, sizes, seed=12)
     srv.run(trace)
     st = latency_stats(trace)
@@ -240,6 +248,20 @@ def run_serving(nreq, dev, sizes=(8, 12, 16, 24, 32, 48), slots=4, plain_sample=
                "graph_batch_by_n": {str(k): v for k, v in tuned.items()},
                "solves_per_s": sum(len(r.iterations) for r in trace) / (
                    max(r.t_done for r in trace) - min(r.arrival for r in trace))})
+    srv.close()
+    # the same mix served with FP64 multigrid-preconditioned solves
+    srv = Server(slots=slots, precision="fp64", multigrid=True, rel_tolerance=1e-8, device=dev,
+                 keep_results=False)
+    tuned_mg = srv.autotune(sizes, candidates=(4, 8, 16), reps=2)
+    cap_mg = _capacity(srv, sizes, poisson_trace)
+    trace_mg = poisson_trace(nreq, 0.8 * cap_mg, sizes, seed=12)
+    srv.run(trace_mg)
+    st_mg = latency_stats(trace_mg)
+    st_mg.update({"capacity_requests_per_s": cap_mg, "arrival_rate": 0.8 * cap_mg,
+                  "graph_batch_by_n": {str(k): v for k, v in tuned_mg.items()},
+                  "what": "the same request mix (same sizes, seeds) at 80% of this server's "
+                          "capacity, FP64 solves with the lattice multigrid V-cycle"})
+    st["multigrid_fp64"] = st_mg
     srv.close()
     # the plain FP64 path, request by request (no overlap, no resident workspace)
     cache = {}

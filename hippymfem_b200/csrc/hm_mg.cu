@@ -34,10 +34,11 @@ struct MGLevel {
   double* coef;          // per element (levels >= 1)
   double* diag;          // Jacobi diagonal (level 0: the caller's)
   double *x, *b, *r, *d, *t;
-  double theta;                  // Chebyshev: d0 = r / (theta diag)
-  double c1[40], c2[40];         // and the recurrence's coefficients
+  double* cheb;          // Chebyshev on the device: [0] theta (d0 = r / (theta diag)),
+                         // [1 + k] c1_k, [1 + kChebMax + k] c2_k (d = c1 d + c2 r / diag)
   int degree;
 };
+constexpr int kChebMax = 40;
 
 }  // namespace hm
 
@@ -48,7 +49,8 @@ struct hm_mg {
   void* jac;             // level-0 operator data (FP64, from hm_lattice_jacobian_prepare)
   const uint8_t* ess;
   int degree, coarse_degree;
-  double* scratch;       // partial sums of the set-up's inner products
+  double* scratch;       // partial sums of the set-up's inner products, eigenvalue state
+  const uint8_t* checked_ess;   // the markers last found to be the whole boundary
 };
 
 namespace hm {
@@ -205,8 +207,10 @@ __global__ void k_prolong_add(MGLevel f, MGLevel c, const double* __restrict__ x
 // x = 0 when zero_x), step (x += d; r -= t; d = c1 d + c2 r / diag unless last), finish
 // (x += d)
 __global__ void k_cheb_start(int64_t n, const double* __restrict__ b, const double* __restrict__ t,
-                             const double* __restrict__ diag, double inv_theta, int zero_x,
-                             double* __restrict__ x, double* __restrict__ r, double* __restrict__ d) {
+                             const double* __restrict__ diag, const double* __restrict__ cheb,
+                             int zero_x, double* __restrict__ x, double* __restrict__ r,
+                             double* __restrict__ d) {
+  const double inv_theta = 1.0 / cheb[0];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double ri = t ? b[i] - t[i] : b[i];
     r[i] = ri;
@@ -216,7 +220,9 @@ __global__ void k_cheb_start(int64_t n, const double* __restrict__ b, const doub
 }
 __global__ void k_cheb_step(int64_t n, double* __restrict__ x, double* __restrict__ d,
                             double* __restrict__ r, const double* __restrict__ t,
-                            const double* __restrict__ diag, double c1, double c2, int last) {
+                            const double* __restrict__ diag, const double* __restrict__ cheb,
+                            int k, int last) {
+  const double c1 = cheb[1 + k], c2 = cheb[1 + kChebMax + k];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double di = d[i];
     x[i] += di;
@@ -253,10 +259,67 @@ __global__ void __launch_bounds__(256) k_mg_dot(int64_t n, const double* __restr
   s = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
+// partials of v.w, v.diag.v and w.w (slots 0, 1, 2)
+__global__ void __launch_bounds__(256) k_mg_dot3(int64_t n, const double* __restrict__ v,
+                                                 const double* __restrict__ w,
+                                                 const double* __restrict__ diag,
+                                                 double* __restrict__ part) {
+  __shared__ double sh[32];
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double vi = v[i], wi = w[i];
+    a = fma(vi, wi, a);
+    b = fma(vi * diag[i], vi, b);
+    c = fma(wi, wi, c);
+  }
+  a = block_sum(a, sh);
+  b = block_sum(b, sh);
+  c = block_sum(c, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = a;
+    part[kMGBlocks + blockIdx.x] = b;
+    part[2 * kMGBlocks + blockIdx.x] = c;
+  }
+}
+// eig[0] = v.Av / v.Dv (kept while the iteration is defined), eig[1] = 1 / |w|
+__global__ void k_mg_eig_step(const double* __restrict__ part, double* __restrict__ eig) {
+  __shared__ double sh[32];
+  double v[3];
+  for (int q = 0; q < 3; ++q) {
+    double t = 0.0;
+    for (int b = threadIdx.x; b < kMGBlocks; b += blockDim.x) t += part[q * kMGBlocks + b];
+    v[q] = block_sum(t, sh);
+  }
+  if (threadIdx.x == 0) {
+    if (v[1] > 0.0 && v[2] > 0.0 && isfinite(v[0] / v[1])) {
+      eig[0] = v[0] / v[1];
+      eig[1] = 1.0 / sqrt(v[2]);
+    } else {
+      eig[1] = 0.0;
+    }
+  }
+}
 __global__ void k_mg_scale_div(int64_t n, const double* __restrict__ w, const double* __restrict__ diag,
-                               double s, double* __restrict__ v) {
+                               const double* __restrict__ eig, double* __restrict__ v) {
+  const double s = eig[1];
+  if (s == 0.0) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     v[i] = s * w[i] / diag[i];
+}
+// the Chebyshev coefficients of the interval [hi / lo_div, hi], hi = 1.1 lambda
+__global__ void k_mg_cheb_coeffs(const double* __restrict__ eig, double lo_div, int degree,
+                                 double* __restrict__ cheb) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double hi = 1.1 * eig[0], lo = hi / lo_div;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  cheb[0] = theta;
+  for (int k = 1; k <= degree && k < kChebMax; ++k) {
+    const double rho = 1.0 / (2.0 * sigma - rho_old);
+    cheb[1 + k] = rho * rho_old;
+    cheb[1 + kChebMax + k] = 2.0 * rho / delta;
+    rho_old = rho;
+  }
 }
 
 }  // namespace hm
@@ -282,10 +345,10 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
   int rc;
   const int g = kMGBlocks;
   if (zero_x) {
-    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, nullptr, lv.diag, 1.0 / lv.theta, 1, x, lv.r, lv.d);
+    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, nullptr, lv.diag, lv.cheb, 1, x, lv.r, lv.d);
   } else {
     if ((rc = apply_level(mg, l, x, lv.t, s))) return rc;
-    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, lv.t, lv.diag, 1.0 / lv.theta, 0, x, lv.r, lv.d);
+    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, lv.t, lv.diag, lv.cheb, 0, x, lv.r, lv.d);
   }
   for (int k = 1; k <= degree; ++k) {
     const bool last = k == degree;
@@ -294,7 +357,7 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
       break;
     }
     if ((rc = apply_level(mg, l, lv.d, lv.t, s))) return rc;
-    k_cheb_step<<<g, 256, 0, s>>>(lv.nodes, x, lv.d, lv.r, lv.t, lv.diag, lv.c1[k], lv.c2[k], last ? 1 : 0);
+    k_cheb_step<<<g, 256, 0, s>>>(lv.nodes, x, lv.d, lv.r, lv.t, lv.diag, lv.cheb, k, last ? 1 : 0);
   }
   return HM_OK;
 }
@@ -309,34 +372,6 @@ int vcycle(hm_mg* mg, int l, const double* b, double* x, cudaStream_t s) {
   if ((rc = vcycle(mg, l + 1, cv.b, cv.x, s))) return rc;
   k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, cv.x, x);
   return smooth(mg, l, b, x, false, false, mg->degree, s);
-}
-
-// Chebyshev coefficients of a level for the interval [lo, hi] of D^{-1} A
-void set_interval(MGLevel& lv, double lo, double hi, int degree) {
-  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
-  double rho_old = 1.0 / sigma;
-  lv.theta = theta;
-  lv.degree = degree;
-  for (int k = 1; k <= degree && k < 40; ++k) {
-    const double rho = 1.0 / (2.0 * sigma - rho_old);
-    lv.c1[k] = rho * rho_old;
-    lv.c2[k] = 2.0 * rho / delta;
-    rho_old = rho;
-  }
-}
-
-double host_dot(hm_mg* mg, int64_t n, const double* a, const double* b, const double* w,
-                cudaStream_t s, int* rc) {
-  k_mg_dot<<<kMGBlocks, 256, 0, s>>>(n, a, b, w, mg->scratch);
-  double h[kMGBlocks];
-  if (cudaMemcpyAsync(h, mg->scratch, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
-    *rc = HM_ERR_CUDA;
-    return 0.0;
-  }
-  double t = 0.0;
-  for (int i = 0; i < kMGBlocks; ++i) t += h[i];   // fixed order
-  return t;
 }
 
 // the level hierarchy of a lattice (no memory touched)
@@ -391,7 +426,7 @@ extern "C" int64_t hm_mg_workspace_bytes(const hm_lattice* h) {
   if (!L) return 0;
   MGLevel lv[16];
   const int nl = plan_levels(*L, lv, 16);
-  int64_t doubles = 3 * L->ndof + kMGBlocks + 32;
+  int64_t doubles = 3 * L->ndof + 3 * kMGBlocks + 64 + nl * (2 * kChebMax + 8);
   for (int l = 1; l < nl; ++l) doubles += lv[l].elems + 6 * lv[l].nodes + 8;
   return doubles * (int64_t)sizeof(double);
 }
@@ -399,7 +434,8 @@ extern "C" int64_t hm_mg_workspace_bytes(const hm_lattice* h) {
 extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coarse_degree,
                             hm_mg** out) {
   const Lattice* L = hm_lattice_geometry(h);
-  if (!L || !work || !out || degree < 1 || degree > 30 || coarse_degree < 1 || coarse_degree > 39)
+  if (!L || !work || !out || degree < 1 || degree >= kChebMax || coarse_degree < 1 ||
+      coarse_degree >= kChebMax)
     return HM_ERR_ARG;
   hm_mg* mg = new (std::nothrow) hm_mg();
   if (!mg) return HM_ERR_NOMEM;
@@ -409,7 +445,9 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
   mg->nlev = plan_levels(*L, mg->lv, 16);
   double* w = static_cast<double*>(work);
   auto take = [&](int64_t n) { double* p = w; w += n; return p; };
-  mg->scratch = take(kMGBlocks + 32);
+  mg->scratch = take(3 * kMGBlocks + 64);
+  mg->checked_ess = nullptr;
+  for (int l = 0; l < mg->nlev; ++l) mg->lv[l].cheb = take(2 * kChebMax + 8);
   MGLevel& z = mg->lv[0];
   z.r = take(L->ndof); z.d = take(L->ndof); z.t = take(L->ndof);
   z.x = z.b = nullptr; z.coef = nullptr; z.diag = nullptr;
@@ -425,21 +463,25 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
   return HM_OK;
 }
 
-// the point's operator: coefficients, diagonals and eigenvalue bounds (synchronises)
+// the point's operator: coefficients, diagonals and eigenvalue bounds, all on the device
+// (the first set-up with a marker array checks it: one synchronisation)
 extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const double* diag,
                            void* stream) {
   if (!mg || !jac || !ess || !diag) return HM_ERR_ARG;
   cudaStream_t s = S_(stream);
   const Lattice& L = mg->L;
-  // the Dirichlet nodes must be exactly the boundary
-  unsigned* bad = reinterpret_cast<unsigned*>(mg->scratch + kMGBlocks);
-  if (cudaMemsetAsync(bad, 0, sizeof(unsigned), s) != cudaSuccess) return HM_ERR_CUDA;
-  k_count_mismatch<<<blocks_for(L.ndof), 256, 0, s>>>(L, ess, bad);
-  unsigned hbad = 0;
-  if (cudaMemcpyAsync(&hbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return HM_ERR_CUDA;
-  if (hbad != 0) return HM_ERR_UNSUPPORTED;
+  // the Dirichlet nodes must be exactly the boundary (checked once per marker array)
+  if (ess != mg->checked_ess) {
+    unsigned* bad = reinterpret_cast<unsigned*>(mg->scratch + 3 * kMGBlocks + 8);
+    if (cudaMemsetAsync(bad, 0, sizeof(unsigned), s) != cudaSuccess) return HM_ERR_CUDA;
+    k_count_mismatch<<<blocks_for(L.ndof), 256, 0, s>>>(L, ess, bad);
+    unsigned hbad = 0;
+    if (cudaMemcpyAsync(&hbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return HM_ERR_CUDA;
+    if (hbad != 0) return HM_ERR_UNSUPPORTED;
+    mg->checked_ess = ess;
+  }
   mg->jac = jac;
   mg->ess = ess;
   mg->lv[0].diag = const_cast<double*>(diag);
@@ -454,32 +496,27 @@ extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const doubl
     for (int l = 1; l < mg->nlev; ++l)
       k_q1_diag<<<blocks_for(mg->lv[l].nodes), 256, 0, s>>>(mg->lv[l], mg->lv[l].diag);
   }
-  if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
-  // largest eigenvalue of D^{-1} A per level: power iteration with the Rayleigh quotient
-  // v.Av / v.Dv (12 steps from a fixed start); smoothing interval [hi/4, hi], the coarsest
-  // level's solve on [hi/64, hi]
-  int rc = HM_OK;
+  // largest eigenvalue of D^{-1} A per level, on the device: power iteration with the
+  // Rayleigh quotient v.Av / v.Dv (10 steps from a fixed start); smoothing interval
+  // [hi/4, hi], the coarsest level's solve on [hi/64, hi]
+  double* part = mg->scratch;
+  double* eig = mg->scratch + 3 * kMGBlocks;
   for (int l = 0; l < mg->nlev; ++l) {
     MGLevel& lv = mg->lv[l];
     double* v = lv.d;
     double* w = lv.t;
     k_mg_seed<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, v);
-    double lam = 1.0;
-    for (int it = 0; it < 12; ++it) {
-      if ((rc = apply_level(mg, l, v, w, s))) return rc;
-      const double vav = host_dot(mg, lv.nodes, v, w, nullptr, s, &rc);
-      const double vdv = host_dot(mg, lv.nodes, v, v, lv.diag, s, &rc);
+    if (cudaMemsetAsync(eig, 0, 2 * sizeof(double), s) != cudaSuccess) return HM_ERR_CUDA;
+    for (int it = 0; it < 10; ++it) {
+      const int rc = apply_level(mg, l, v, w, s);
       if (rc) return rc;
-      if (!(vdv > 0.0)) break;
-      lam = vav / vdv;
-      const double ww = host_dot(mg, lv.nodes, w, w, nullptr, s, &rc);
-      if (rc) return rc;
-      if (!(ww > 0.0)) break;
-      k_mg_scale_div<<<kMGBlocks, 256, 0, s>>>(lv.nodes, w, lv.diag, 1.0 / std::sqrt(ww), v);
+      k_mg_dot3<<<kMGBlocks, 256, 0, s>>>(lv.nodes, v, w, lv.diag, part);
+      k_mg_eig_step<<<1, 256, 0, s>>>(part, eig);
+      k_mg_scale_div<<<kMGBlocks, 256, 0, s>>>(lv.nodes, w, lv.diag, eig, v);
     }
-    const double hi = 1.1 * lam;
     const bool coarsest = l == mg->nlev - 1;
-    set_interval(lv, coarsest ? hi / 64.0 : hi / 4.0, hi, coarsest ? mg->coarse_degree : mg->degree);
+    lv.degree = coarsest ? mg->coarse_degree : mg->degree;
+    k_mg_cheb_coeffs<<<1, 32, 0, s>>>(eig, coarsest ? 64.0 : 4.0, lv.degree, lv.cheb);
   }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }

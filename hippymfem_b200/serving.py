@@ -19,7 +19,8 @@ picked per mesh size by ``autotune`` (timed solves over a few candidates; the re
 a solve does not depend on it).
 
 Work of a request (FP64 outer loops; FP32 operator and recurrence with FP64 reliable
-updates when ``precision="mixed"``):
+updates when ``precision="mixed"``; with ``multigrid=True``, FP64 solves preconditioned
+by the lattice multigrid V-cycle):
 
 * ``forward``: ``m`` from the request's seed (the benchmark's cosine field, computed on
   the device), its quadrature data, the residual at ``u = 0`` (Dirichlet data 0), one
@@ -94,22 +95,23 @@ class _MeshState:
         g = torch.Generator(device="cpu").manual_seed(int(seed) + 7919)
         return torch.randn(self.mesh.ndof, dtype=torch.float64, generator=g).to(self.coords.device)
 
-    def footprint(self, precision):
+    def footprint(self, precision, multigrid=False):
         """Bytes of one slot's workspace for this size."""
         nd, q = self.mesh.ndof, self.mesh.quad_bytes(_lib.HM_FP64)
+        mg = lib.hm_mg_workspace_bytes(self.mesh.handle) if multigrid else 0
         jac = lib.hm_lattice_jacobian_bytes(self.mesh.handle, _lib.HM_FP64)
         if precision == "mixed":
             jac += lib.hm_lattice_jacobian_bytes(self.mesh.handle, _lib.HM_FP32)
             work = lib.hm_pcg_mixed_workspace_bytes(nd)
         else:
             work = lib.hm_pcg_workspace_bytes(nd)
-        return int(2 * q + jac + work + 14 * 8 * nd)
+        return int(2 * q + jac + work + mg + 14 * 8 * nd)
 
 
 class _Workspace:
     """One slot's resident buffers for one mesh size."""
 
-    def __init__(self, ms, precision, rtol, check_every):
+    def __init__(self, ms, precision, rtol, check_every, multigrid=False):
         self.ms = ms
         mesh, dev = ms.mesh, ms.mesh.device
         nq = (mesh.quad_bytes(_lib.HM_FP64) + 7) // 8
@@ -117,7 +119,7 @@ class _Workspace:
         self.quad2 = torch.empty(nq, dtype=torch.float64, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.plan = SolvePlan(mesh, ms.bc.marker, precision, rel_tolerance=rtol,
-                              check_every=check_every)
+                              check_every=check_every, multigrid=multigrid)
         nd = mesh.ndof
         self.vec = {k: torch.zeros(nd, dtype=torch.float64, device=dev)
                     for k in ("u", "p", "uh", "ph", "zero", "r1", "r2", "r3", "y")}
@@ -125,7 +127,7 @@ class _Workspace:
         mis = ms.misfit
         self.misfit = DiscreteStateObservation(mis.Bh, mis.d.cpu().numpy(), mis.noise_variance,
                                                device=dev)
-        self.nbytes = ms.footprint(precision)
+        self.nbytes = ms.footprint(precision, multigrid)
         self.in_use = False
         self.last_used = 0.0
 
@@ -200,7 +202,10 @@ class Server:
     device memory)."""
 
     def __init__(self, slots=4, precision="mixed", rel_tolerance=1e-8, memory_budget=None,
-                 device=None, check_every=None, keep_results=True):
+                 device=None, check_every=None, keep_results=True, multigrid=False):
+        if multigrid and precision != "fp64":
+            raise ValueError("the multigrid solves are FP64")
+        self.multigrid = bool(multigrid)
         self.device = torch.device(device if device is not None else "cuda")
         self.slots = int(slots)
         self.precision = precision
@@ -242,7 +247,7 @@ class Server:
             ms = self.mesh_state(n)
             best = None
             for ce in candidates:
-                ws = _Workspace(ms, self.precision, self.rtol, ce)
+                ws = _Workspace(ms, self.precision, self.rtol, ce, self.multigrid)
                 req = Request("forward", n, 0)
                 with torch.cuda.stream(stream):
                     m = ms.field(0)
@@ -269,7 +274,7 @@ class Server:
         if ws is not None:
             ws.in_use = True
             return ws, None
-        need = self.mesh_state_locked(n).footprint(self.precision)
+        need = self.mesh_state_locked(n).footprint(self.precision, self.multigrid)
         while self._resident + need > self.budget:
             idle = [(w.last_used, k) for k, w in self._ws.items() if not w.in_use]
             if idle:
@@ -309,7 +314,8 @@ class Server:
             if ws is None:
                 ms = self.mesh_state(req.n)
                 with torch.cuda.stream(stream):
-                    ws = _Workspace(ms, self.precision, self.rtol, self.check_every(req.n))
+                    ws = _Workspace(ms, self.precision, self.rtol, self.check_every(req.n),
+                                    self.multigrid)
                 ws.nbytes = reserved
                 ws.in_use = True
                 with self._lock:

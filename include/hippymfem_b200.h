@@ -256,8 +256,10 @@ int hm_pcg_plan_destroy(hm_pcg_plan* plan);
  * (HM_ERR_UNSUPPORTED otherwise).
  *   hm_mg_create: the hierarchy on d_work (hm_mg_workspace_bytes);
  *   hm_mg_setup: a point's operator -- d_jac64 of hm_lattice_jacobian_prepare (FP64),
- *     its markers and Jacobi diagonal (hm_lattice_diag_A); estimates the smoothers'
- *     eigenvalue bounds (synchronises the stream); again whenever the point changes;
+ *     its markers and Jacobi diagonal (hm_lattice_diag_A); coarse coefficients,
+ *     diagonals and the smoothers' eigenvalue bounds are computed on the device (the
+ *     first set-up with a marker array checks it against the boundary: one
+ *     synchronisation); again whenever the point changes;
  *   hm_mg_apply: z = V-cycle(r);
  *   hm_pcg_mg: PCG with the V-cycle (x: initial guess; d_work of hm_pcg_workspace_bytes);
  *   hm_pcg_plan_set_mg: a plan's FP64 solves use it (graph-captured with the V-cycle). */
