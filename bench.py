@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", type=int, default=2000,
                     help="requests of the serving trace (0: skip)")
+    ap.add_argument("--config", choices=("main", "precision", "differentiation"), default="main",
+                    help="precision: 128^3, FP32 contractions and mixed-precision Hessian "
+                         "actions against FP64; differentiation: 32^3 finite-difference "
+                         "checks of the autograd wrappers")
     return ap.parse_args()
 
 
@@ -568,10 +572,176 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def _problem_at(n, sigma, dev, precision="fp64", preconditioner="jacobi", lines=False):
+    """Mesh, space, problem, misfit (data from m_true, 1 % noise) and m of a config."""
+    import torch
+
+    import hippymfem_b200 as hm
+    from hippymfem_b200.synthetic import interior_points, log_conductivity, vertical_lines
+
+    mesh = hm.BoxMesh(n, device=dev)
+    V = hm.Q2Space(mesh)
+    bc = hm.DirichletBC(V)
+    prob = hm.PDEVariationalProblem([V, V, V], f=1.0, bc=bc, check_finite=False,
+                                    solver_tolerance=1e-12, matrix_free_solves=True,
+                                    solver_precision=precision, preconditioner=preconditioner)
+    coords = mesh.node_coords()
+    m = torch.as_tensor(log_conductivity(coords, seed=0, sigma=sigma), device=dev)
+    mt = torch.as_tensor(log_conductivity(coords, seed=1, sigma=sigma), device=dev)
+    pts = vertical_lines(60, 64, seed=3) if lines else interior_points(4096, seed=2)
+    ut = V.vector()
+    prob.solveFwd(ut, [ut, mt, None])
+    d = hm.observation_operator(mesh, pts) @ ut.cpu().numpy()
+    noise = 0.01 * float(np.abs(d).max())
+    d = d + noise * np.random.default_rng(5).standard_normal(d.shape)
+    misfit = hm.PointwiseStateObservation(V, pts, data=d, noise_variance=noise ** 2)
+    return mesh, V, bc, prob, misfit, m
+
+
+def run_precision(a, n=128, nactions=20):
+    """The precision configuration: 128^3, m of amplitude sigma = 1.  Every block and
+    vector assembled with FP32 element contractions (FP64 CSR values) against the FP64
+    kernels, and nactions Hessian actions whose solves run the FP32 recurrence with FP64
+    reliable updates against FP64 solves; relative errors per block and per action."""
+    import torch
+
+    import hippymfem_b200 as hm
+    from hippymfem_b200 import _lib
+    from hippymfem_b200._lib import check, lib, ptr, stream_ptr
+
+    dev = torch.device("cuda", 0)
+    mesh, V, bc, prob, misfit, m = _problem_at(n, 1.0, dev, preconditioner="mg")
+    model = hm.Model(prob, None, misfit)
+    u, p = V.vector(), V.vector()
+    x = [u, m, p]
+    model.solveFwd(u, x)
+    model.solveAdj(p, x)
+    pat = hm.LatticePattern(mesh)
+    prob._pattern = pat
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    sp = stream_ptr()
+    blocks = {}
+    for name in ("A", "C", "Wum", "Wmm"):
+        vals, ms = {}, {}
+        for prec in (_lib.HM_FP64, _lib.HM_FP32):
+            quad = torch.empty(mesh.quad_bytes(prec) // 8 + 1, dtype=torch.float64, device=dev)
+            v = pat.new_values()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            check(lib.hm_lattice_quadrature(mesh.handle, ptr(u), ptr(m), ptr(p), prec, ptr(quad),
+                                            ptr(status), sp))
+            check(lib.hm_lattice_assemble(
+                mesh.handle, ptr(quad), prec, ptr(pat.indptr), ptr(bc.marker), 1.0,
+                *(ptr(v) if name == b else None for b in ("A", "C", "Wum", "Wmm")),
+                None, None, None, 0, sp))
+            e1.record()
+            torch.cuda.synchronize()
+            vals[prec], ms[prec] = v, e0.elapsed_time(e1)
+            del quad
+        d = vals[_lib.HM_FP32] - vals[_lib.HM_FP64]
+        ref = vals[_lib.HM_FP64]
+        blocks[name] = {"rel_err_max": float(d.abs().max() / ref.abs().max()),
+                        "rel_err_fro": float(d.norm() / ref.norm()),
+                        "ms_fp64": ms[_lib.HM_FP64], "ms_fp32": ms[_lib.HM_FP32]}
+        del vals, d, ref
+        torch.cuda.empty_cache()
+    # Hessian actions: FP64 (multigrid) against mixed-precision solves
+    model.setPointForHessianEvaluations(x)
+    H64 = hm.ReducedHessian(model)
+    prob32 = hm.PDEVariationalProblem([V, V, V], f=1.0, bc=bc, check_finite=False,
+                                      solver_tolerance=1e-12, solver_precision="mixed")
+    prob32._pattern = pat
+    model32 = hm.Model(prob32, None, misfit)
+    model32.setPointForHessianEvaluations(x)
+    H32 = hm.ReducedHessian(model32)
+    rng = np.random.default_rng(21)
+    errs, t64, t32 = [], [], []
+    y64, y32 = V.vector(), V.vector()
+    for i in range(nactions):
+        v = torch.as_tensor(rng.standard_normal(mesh.ndof), device=dev)
+        for H, y, t in ((H64, y64, t64), (H32, y32, t32)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            H.mult(v, y)
+            e1.record()
+            torch.cuda.synchronize()
+            t.append(e0.elapsed_time(e1))
+        errs.append(float((y32 - y64).norm() / y64.norm()))
+    line = {"config": {"workload": "precision: Q2 hex %d^3, sigma = 1" % n, "dofs": mesh.ndof,
+                       "nnz_per_block": mesh.nnz},
+            "blocks_fp32_vs_fp64": blocks,
+            "hessian_actions": {"n": nactions, "rel_err_mixed_vs_fp64": errs,
+                                "rel_err_max": max(errs),
+                                "ms_fp64_multigrid": float(np.mean(t64)),
+                                "ms_mixed_jacobi": float(np.mean(t32)),
+                                "pcg_iterations_mixed": H32.iterations[:4],
+                                "pcg_iterations_fp64": H64.iterations[:4]},
+            "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
+def run_differentiation(a, n=32, ndir=16, h=1e-6):
+    """The differentiation configuration: 32^3, 60 vertical lines x 64 depths, 1 % noise;
+    the gradient of the misfit by the autograd wrappers against central differences
+    along ndir seeded directions, and the Hessian action (the gradient's
+    vector-Jacobian product) against differences of the gradient."""
+    import torch
+
+    import hippymfem_b200 as hm
+    from hippymfem_b200.autograd import ReducedGradient, reduced_misfit
+
+    dev = torch.device("cuda", 0)
+    mesh, V, bc, prob, misfit, m = _problem_at(n, 0.1, dev, preconditioner="mg", lines=True)
+    model = hm.Model(prob, None, misfit)
+    mm = m.clone().requires_grad_(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    J = reduced_misfit(mm, prob, misfit)
+    (g,) = torch.autograd.grad(J, mm)
+    e1.record()
+    torch.cuda.synchronize()
+    t_grad = e0.elapsed_time(e1)
+    rng = np.random.default_rng(6)
+    rel = []
+    for _ in range(ndir):
+        d = torch.as_tensor(rng.standard_normal(mesh.ndof), device=dev)
+        with torch.no_grad():
+            fd = float((reduced_misfit(m + h * d, prob, misfit) - reduced_misfit(m - h * d, prob, misfit))
+                       / (2 * h))
+        an = float(torch.dot(g, d))
+        rel.append(abs(fd - an) / abs(an))
+    mh = m.clone().requires_grad_(True)
+    gg = ReducedGradient.apply(mh, model)
+    hrel = []
+    t_hv = []
+    for _ in range(4):
+        v = torch.as_tensor(rng.standard_normal(mesh.ndof), device=dev)
+        e0.record()
+        (hv,) = torch.autograd.grad(gg, mh, v, retain_graph=True)
+        e1.record()
+        torch.cuda.synchronize()
+        t_hv.append(e0.elapsed_time(e1))
+        with torch.no_grad():
+            fd = (ReducedGradient.apply(m + h * v, model) - ReducedGradient.apply(m - h * v, model)) / (2 * h)
+        hrel.append(float((fd - hv).norm() / hv.norm()))
+    line = {"config": {"workload": "differentiation: Q2 hex %d^3, 60 lines x 64 depths" % n,
+                       "dofs": mesh.ndof},
+            "gradient_fd": {"directions": ndir, "h": h, "rel_err_max": max(rel),
+                            "rel_err": rel, "ms_gradient": t_grad},
+            "hessian_fd": {"directions": 4, "rel_err_max": max(hrel), "rel_err": hrel,
+                           "ms_hessian_vector": float(np.mean(t_hv))},
+            "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "precision":
+        run_precision(a)
+    elif a.config == "differentiation":
+        run_differentiation(a)
     else:
         run_ours(a)
 

@@ -664,7 +664,7 @@ extern "C" int hm_pcg_mg(hm_mg* mg, const double* b, double* x, double rtol, int
 extern "C" int64_t hm_pcg_mixed_workspace_bytes(int64_t n) {
   // FP64: r, t, the p.q partials (at most one per node), scalars, partials, b.b;
   // FP32: x, r, z, p, q of the single-precision recurrence
-  return (int64_t)sizeof(double) * (2 * n + pq_slots(n) + SC_N + 3 * (int64_t)kReduceBlocks + 8) +
+  return (int64_t)sizeof(double) * (4 * n + pq_slots(n) + SC_N + 3 * (int64_t)kReduceBlocks + 8) +
          (int64_t)sizeof(float) * (5 * n + 16);
 }
 
@@ -690,7 +690,7 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
   double* w = static_cast<double*>(work);
   double* r64 = w;
   double* t64 = w + n;
-  double* pq_part = w + 2 * n;
+  double* pq_part = w + 4 * n;     // (w + 2n .. 4n: the FP64 finish's z and p)
   double* sc = pq_part + pq_slots(n);
   double* part = sc + SC_N;
   double* bbp = part + 3 * kReduceBlocks;
@@ -709,8 +709,9 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
     if (cudaMemcpyAsync(h, sc, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HM_ERR_CUDA;
     return cudaStreamSynchronize(s) == cudaSuccess ? HM_OK : HM_ERR_CUDA;
   };
-  // the anchor: [x += s x32; t = A64 x]; r = b - t; new scale; FP32 r, z, p from r
-  auto anchor = [&](bool first) -> int {
+  // the anchor: [x += s x32; t = A64 x]; r = b - t; new scale; FP32 r, z, p from r (p
+  // restarted as z on the first anchor and on a restart)
+  auto anchor = [&](bool first, bool restart) -> int {
     int64_t np = 0;
     if (!first) {
       k_mx_accum<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x32, x);
@@ -721,7 +722,8 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
     k_mx_scale<<<1, 1024, 0, s>>>(part, sc);
     if (first && cudaMemcpyAsync(bbp, sc + SC_TRUE, sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
       return HM_ERR_CUDA;
-    k_mx_anchor<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r64, diag, sc, first ? 1 : 0, r32, z32, p32, part);
+    k_mx_anchor<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r64, diag, sc, (first || restart) ? 1 : 0,
+                                                         r32, z32, p32, part);
     k_mx_anchor_final<<<1, 1024, 0, s>>>(part, sc, bbp, rtol);
     if (cudaGetLastError() != cudaSuccess) return HM_ERR_CUDA;
     return read();
@@ -731,12 +733,12 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
       cudaMemsetAsync(x, 0, sizeof(double) * n, s) != cudaSuccess ||
       cudaMemsetAsync(x32, 0, sizeof(float) * n, s) != cudaSuccess)
     return HM_ERR_CUDA;
-  int rc = anchor(true);
+  int rc = anchor(true, true);
   if (rc) return rc;
   const double bb = h[SC_TRUE];
   const double tol2 = rtol * rtol * bb, goal2 = 100.0 * tol2;
   double tr = bb, prev = bb;
-  int it = 0, nup = 0, stalls = 0;
+  int it = 0, nup = 0, stalls = 0, last_anchor = 0;
   bool conv = tr <= tol2;
   while (!conv) {
     const int count = it + check_every < maxiter ? check_every : maxiter - it;
@@ -747,8 +749,12 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
     it += count;
     if ((rc = read())) return rc;
     const bool claim = h[SC_CONV] >= 0.0;
-    if (!claim && h[SC_RR] > delta * delta && it < maxiter) continue;
-    if ((rc = anchor(false))) return rc;
+    // a recurrence that has grown above its anchor's residual, or has not fallen by
+    // delta in 2000 iterations, has lost its way in single precision: restart it
+    const bool lost = !(h[SC_RR] <= 1.0) || it - last_anchor > 2000;
+    if (!claim && !lost && h[SC_RR] > delta * delta && it < maxiter) continue;
+    if ((rc = anchor(false, lost))) return rc;
+    last_anchor = it;
     ++nup;
     tr = h[SC_TRUE];
     if (tr <= tol2) { conv = true; break; }
@@ -759,6 +765,20 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
       conv = tr <= goal2;
       break;
     }
+  }
+  if (!conv && it < maxiter) {
+    // single precision cannot carry this solve (its residual stalls above the goal, or
+    // the anchors run out): finish it in FP64 from the current x, as the reference's
+    // refined solves do (_solve_in_double, modeling/PDEVariationalProblem.py:1329-1360)
+    int its64 = 0;
+    double rr64 = 0.0;
+    const int rc64 = pcg_run<double>(o64, diag, b, x, rtol, maxiter - it, check_every, pq_part,
+                                     w, &its64, &rr64, stream);
+    if (rc64 != HM_OK && rc64 != HM_ERR_NOCONV) return rc64;
+    if (iterations) *iterations = it + its64;
+    if (updates) *updates = nup;
+    if (relres) *relres = rr64;
+    return rc64;
   }
   if (iterations) *iterations = it;
   if (updates) *updates = nup;

@@ -214,7 +214,10 @@ int hm_pcg(int64_t n, const int32_t* d_indptr, const int32_t* d_indices,
  * convergence, the correction is added to the FP64 x and the true residual b - A x of
  * the FP64 operator d_jac64 replaces the recurrence's, the search direction kept.
  * Converged when ||b - A x||_2 <= rtol ||b||_2; a true residual that stops halving
- * between anchors (its rounding floor) ends the solve, converged if within 10 rtol.
+ * between anchors (its rounding floor) ends the refinement, converged if within 10 rtol;
+ * a refinement that ends short of that (or runs out of anchors) is finished by FP64
+ * Jacobi-PCG from the current x, as the reference finishes its refined solves in
+ * double (_solve_in_double).
  * x starts from zero.  The mixed-precision route of the reference's solves
  * (_refined_solve, modeling/PDEVariationalProblem.py:1220-1329, a single-precision
  * hypre inside FP64 refinement), here without restarting the Krylov space.
