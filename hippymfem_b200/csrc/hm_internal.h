@@ -35,3 +35,9 @@ int64_t hm_apply_dot_parts(const hm::Lattice& L);
 int hm_launch_apply_A32_dot(const hm::Lattice& L, void* jac32, const uint8_t* ess, const float* x,
                             float* y, double* part, void* stream, double* sc = nullptr,
                             unsigned* counter = nullptr);
+// y = A x for an x that is zero on the Dirichlet nodes (FP64 operator)
+int hm_launch_apply_A_clean(const hm::Lattice& L, void* jac, const uint8_t* ess, const double* x,
+                            double* y, void* stream);
+// x = b on the Dirichlet nodes
+int hm_launch_ess_take_b(const hm::Lattice& L, const uint8_t* ess, const double* b, double* x,
+                         void* stream);

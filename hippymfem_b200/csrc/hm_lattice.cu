@@ -234,7 +234,9 @@ __device__ __forceinline__ real dbq_rt(int q, int a) {
   return q == 0 ? (real)dbq(0, a) : q == 1 ? (real)dbq(1, a) : (real)dbq(2, a);
 }
 
-template <typename real, typename vec>
+// ESS: zero x on the Dirichlet nodes on the fly (callers whose x is already zero there
+// -- every vector inside the lattice solves -- skip the markers)
+template <typename real, typename vec, bool ESS = true>
 __global__ void __launch_bounds__(256, 2)
     k_elem_apply(Lattice L, const real* __restrict__ Dq, const uint8_t* __restrict__ ess,
                  const vec* __restrict__ xin, real* __restrict__ Ye) {
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(256, 2)
     for (int i = 0; i < 9; ++i) {
       const unsigned n = n0 + (unsigned)(i % 3) + nsy * (unsigned)(i / 3) + nsz * (unsigned)a3;
       const real xv = live ? (real)__ldg(xin + n) : (real)0;
-      const bool fixed = ess != nullptr && live && __ldg(ess + n) != 0;
+      const bool fixed = ESS && ess != nullptr && live && __ldg(ess + n) != 0;
       const real x = fixed ? (real)0 : xv;
       Xb[i] = a3 == 0 ? b3 * x : fma(b3, x, Xb[i]);
       Xd[i] = a3 == 0 ? d3 * x : fma(d3, x, Xd[i]);
@@ -504,11 +506,15 @@ int hm_launch_jacobian_prepare(const Lattice& L, const void* quad, int quad_prec
 template <typename real, typename vec>
 static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const vec* x,
                           vec* y, const vec* dotw, double* part, void* stream,
-                          double* sc = nullptr, unsigned* counter = nullptr) {
+                          double* sc = nullptr, unsigned* counter = nullptr,
+                          bool x_zero_on_ess = false) {
   real* Dq = static_cast<real*>(jac);
   real* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
-  k_elem_apply<real, vec><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
+  if (x_zero_on_ess)
+    k_elem_apply<real, vec, false><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
+  else
+    k_elem_apply<real, vec, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
   k_node_gather<real, vec><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, x, y, dotw, part, part != nullptr ? sc : nullptr, counter);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
@@ -524,20 +530,43 @@ int hm_launch_apply_A(const Lattice& L, void* jac, int precision, const uint8_t*
   return launch_apply_t<double, double>(L, jac, ess, x, y, nullptr, nullptr, stream);
 }
 
-// with sc and counter the gather's last block also takes the CG step's alpha
+// with sc and counter the gather's last block also takes the CG step's alpha; x must be
+// zero on the Dirichlet nodes (the solves keep every search direction so)
 int hm_launch_apply_A_dot(const Lattice& L, void* jac, int precision, const uint8_t* ess,
                           const double* x, double* y, double* part, void* stream, double* sc,
                           unsigned* counter) {
   if (precision == HM_FP32)
-    return launch_apply_t<float, double>(L, jac, ess, x, y, x, part, stream, sc, counter);
-  return launch_apply_t<double, double>(L, jac, ess, x, y, x, part, stream, sc, counter);
+    return launch_apply_t<float, double>(L, jac, ess, x, y, x, part, stream, sc, counter, true);
+  return launch_apply_t<double, double>(L, jac, ess, x, y, x, part, stream, sc, counter, true);
 }
 
-// the FP32 operator on FP32 vectors (the inner solves of the mixed-precision PCG)
+// y = A x for an x that is zero on the Dirichlet nodes (FP64 operator)
+int hm_launch_apply_A_clean(const Lattice& L, void* jac, const uint8_t* ess, const double* x,
+                            double* y, void* stream) {
+  return launch_apply_t<double, double>(L, jac, ess, x, y, nullptr, nullptr, stream, nullptr,
+                                        nullptr, true);
+}
+
+// the FP32 operator on FP32 vectors (the inner solves of the mixed-precision PCG), x zero
+// on the Dirichlet nodes
 int hm_launch_apply_A32_dot(const Lattice& L, void* jac32, const uint8_t* ess, const float* x,
                             float* y, double* part, void* stream, double* sc, unsigned* counter) {
   return launch_apply_t<float, float>(L, jac32, ess, x, y, part ? x : nullptr, part, stream, sc,
-                                      counter);
+                                      counter, true);
+}
+
+// x = b on the Dirichlet nodes (the identity rows of the eliminated operator): after it
+// every residual of a solve, and so every search direction, is zero there
+__global__ void k_ess_take_b(int64_t n, const uint8_t* __restrict__ ess, const double* __restrict__ b,
+                             double* __restrict__ x) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n && ess[i]) x[i] = b[i];
+}
+int hm_launch_ess_take_b(const Lattice& L, const uint8_t* ess, const double* b, double* x,
+                         void* stream) {
+  if (ess == nullptr) return HM_OK;
+  k_ess_take_b<<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L.ndof, ess, b, x);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 
 int hm_launch_diag_A(const Lattice& L, const void* quad, int precision, const uint8_t* ess,

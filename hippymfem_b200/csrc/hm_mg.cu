@@ -330,8 +330,13 @@ namespace {
 inline cudaStream_t S_(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 inline int blocks_for(int64_t n) { return (int)((n + 255) / 256); }
 
-int apply_level(hm_mg* mg, int l, const double* x, double* y, cudaStream_t s) {
-  if (l == 0) return hm_launch_apply_A(mg->L, mg->jac, HM_FP64, mg->ess, x, y, (void*)s);
+// clean: x is zero on the Dirichlet nodes (the level-0 element pass then skips the
+// markers); every vector of a cycle is when its right-hand side is
+int apply_level(hm_mg* mg, int l, const double* x, double* y, bool clean, cudaStream_t s) {
+  if (l == 0) {
+    if (clean) return hm_launch_apply_A_clean(mg->L, mg->jac, mg->ess, x, y, (void*)s);
+    return hm_launch_apply_A(mg->L, mg->jac, HM_FP64, mg->ess, x, y, (void*)s);
+  }
   const MGLevel& lv = mg->lv[l];
   k_q1_apply<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, x, y);
   return HM_OK;
@@ -340,14 +345,14 @@ int apply_level(hm_mg* mg, int l, const double* x, double* y, cudaStream_t s) {
 // Chebyshev smoothing of A_l x = b: from x = 0 (zero_x) or from the given x; with
 // want_r the residual b - A x of the result is left in lv.r
 int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_r, int degree,
-           cudaStream_t s) {
+           bool clean, cudaStream_t s) {
   MGLevel& lv = mg->lv[l];
   int rc;
   const int g = kMGBlocks;
   if (zero_x) {
     k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, nullptr, lv.diag, lv.cheb, 1, x, lv.r, lv.d);
   } else {
-    if ((rc = apply_level(mg, l, x, lv.t, s))) return rc;
+    if ((rc = apply_level(mg, l, x, lv.t, clean, s))) return rc;
     k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, lv.t, lv.diag, lv.cheb, 0, x, lv.r, lv.d);
   }
   for (int k = 1; k <= degree; ++k) {
@@ -356,22 +361,22 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
       k_cheb_finish<<<g, 256, 0, s>>>(lv.nodes, x, lv.d);
       break;
     }
-    if ((rc = apply_level(mg, l, lv.d, lv.t, s))) return rc;
+    if ((rc = apply_level(mg, l, lv.d, lv.t, clean, s))) return rc;
     k_cheb_step<<<g, 256, 0, s>>>(lv.nodes, x, lv.d, lv.r, lv.t, lv.diag, lv.cheb, k, last ? 1 : 0);
   }
   return HM_OK;
 }
 
-int vcycle(hm_mg* mg, int l, const double* b, double* x, cudaStream_t s) {
+int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_t s) {
   int rc;
-  if (l == mg->nlev - 1) return smooth(mg, l, b, x, true, false, mg->coarse_degree, s);
+  if (l == mg->nlev - 1) return smooth(mg, l, b, x, true, false, mg->coarse_degree, clean, s);
   MGLevel& lv = mg->lv[l];
   MGLevel& cv = mg->lv[l + 1];
-  if ((rc = smooth(mg, l, b, x, true, true, mg->degree, s))) return rc;
+  if ((rc = smooth(mg, l, b, x, true, true, mg->degree, clean, s))) return rc;
   k_restrict<<<blocks_for(cv.nodes), 256, 0, s>>>(lv, cv, lv.r, cv.b);
-  if ((rc = vcycle(mg, l + 1, cv.b, cv.x, s))) return rc;
+  if ((rc = vcycle(mg, l + 1, cv.b, cv.x, clean, s))) return rc;
   k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, cv.x, x);
-  return smooth(mg, l, b, x, false, false, mg->degree, s);
+  return smooth(mg, l, b, x, false, false, mg->degree, clean, s);
 }
 
 // the level hierarchy of a lattice (no memory touched)
@@ -413,8 +418,9 @@ __global__ void k_count_mismatch(Lattice L, const uint8_t* __restrict__ ess, uns
 }
 }  // namespace
 
+// inside the MG-PCG, whose residuals are zero on the Dirichlet nodes
 int hm_mg_vcycle(hm_mg* mg, const double* r, double* z, void* stream) {
-  return vcycle(mg, 0, r, z, S_(stream));
+  return vcycle(mg, 0, r, z, true, S_(stream));
 }
 const double* hm_mg_level0_diag(const hm_mg* mg) { return mg->lv[0].diag; }
 void* hm_mg_jac(const hm_mg* mg) { return mg->jac; }
@@ -508,7 +514,7 @@ extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const doubl
     k_mg_seed<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, v);
     if (cudaMemsetAsync(eig, 0, 2 * sizeof(double), s) != cudaSuccess) return HM_ERR_CUDA;
     for (int it = 0; it < 10; ++it) {
-      const int rc = apply_level(mg, l, v, w, s);
+      const int rc = apply_level(mg, l, v, w, true, s);   // v is zero on the boundary
       if (rc) return rc;
       k_mg_dot3<<<kMGBlocks, 256, 0, s>>>(lv.nodes, v, w, lv.diag, part);
       k_mg_eig_step<<<1, 256, 0, s>>>(part, eig);
@@ -523,7 +529,7 @@ extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const doubl
 
 extern "C" int hm_mg_apply(hm_mg* mg, const double* r, double* z, void* stream) {
   if (!mg || !r || !z || !mg->jac) return HM_ERR_ARG;
-  const int rc = vcycle(mg, 0, r, z, S_(stream));
+  const int rc = vcycle(mg, 0, r, z, false, S_(stream));
   if (rc) return rc;
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }

@@ -8,6 +8,7 @@
 // whatever check_every is.
 #include <new>
 #include <cmath>
+#include <type_traits>
 
 #include "hm_common.cuh"
 #include "hm_internal.h"
@@ -299,11 +300,11 @@ __global__ void k_mx_accum(int64_t n, const double* __restrict__ sc, float* __re
 // r64 = b - t64; partials of r64.r64
 __global__ void __launch_bounds__(kReduceThreads)
     k_residual64(int64_t n, const double* __restrict__ b, const double* __restrict__ t,
-                 double* __restrict__ r, double* __restrict__ part) {
+                 const uint8_t* __restrict__ ess, double* __restrict__ r, double* __restrict__ part) {
   __shared__ double sh[32];
   double v = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double ri = b[i] - (t ? t[i] : 0.0);
+    const double ri = (ess && ess[i]) ? 0.0 : b[i] - (t ? t[i] : 0.0);
     r[i] = ri;
     v = fma(ri, ri, v);
   }
@@ -549,8 +550,13 @@ int pcg_run(const PcgOp& o, const double* diag, const T* b, T* x, double rtol, i
   unsigned* cnt = reinterpret_cast<unsigned*>(part + 3 * kReduceBlocks);
   if (check_every <= 0) check_every = 1;
   if (cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), S_(stream)) != cudaSuccess) return HM_ERR_CUDA;
+  int rc;
+  // x = b on the Dirichlet nodes: every residual and direction is then zero there, which
+  // the lattice operator's direction products rely on
+  if constexpr (std::is_same<T, double>::value)
+    if (o.L && (rc = hm_launch_ess_take_b(*o.L, o.ess, b, x, stream))) return rc;
   int64_t nparts = 0;
-  int rc = op_apply(o, x, q, nullptr, &nparts, stream);
+  rc = op_apply(o, x, q, nullptr, &nparts, stream);
   if (rc) return rc;
   k_pcg_init<T><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, q, diag, r, z, p, part);
   k_pcg_init_final<<<1, 1024, 0, s>>>(part, sc, rtol);
@@ -614,8 +620,10 @@ int pcg_mg_run(hm_mg* mg, const double* b, double* x, double rtol, int maxiter, 
   unsigned* cnt = reinterpret_cast<unsigned*>(part + 3 * kReduceBlocks);
   if (check_every <= 0) check_every = 1;
   if (cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), s) != cudaSuccess) return HM_ERR_CUDA;
+  int rc = hm_launch_ess_take_b(*L, o.ess, b, x, stream);   // as in pcg_run
+  if (rc) return rc;
   int64_t np = 0;
-  int rc = op_apply(o, x, q, nullptr, &np, stream);
+  rc = op_apply(o, x, q, nullptr, &np, stream);
   if (rc) return rc;
   k_pcg_mg_init<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, q, r, part);
   if ((rc = hm_mg_vcycle(mg, r, z, stream))) return rc;
@@ -718,7 +726,9 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
       const int rc = op_apply(o64, x, t64, nullptr, &np, stream);
       if (rc) return rc;
     }
-    k_residual64<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, first ? nullptr : t64, r64, part);
+    // first: x is b on the Dirichlet nodes and 0 elsewhere, so r = b off them, 0 on them
+    k_residual64<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, b, first ? nullptr : t64,
+                                                          first ? ess : nullptr, r64, part);
     k_mx_scale<<<1, 1024, 0, s>>>(part, sc);
     if (first && cudaMemcpyAsync(bbp, sc + SC_TRUE, sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
       return HM_ERR_CUDA;
@@ -733,7 +743,9 @@ int pcg_mixed_run(const hm::Lattice* L, void* jac64, void* jac32, const uint8_t*
       cudaMemsetAsync(x, 0, sizeof(double) * n, s) != cudaSuccess ||
       cudaMemsetAsync(x32, 0, sizeof(float) * n, s) != cudaSuccess)
     return HM_ERR_CUDA;
-  int rc = anchor(true, true);
+  int rc = hm_launch_ess_take_b(*L, ess, b, x, stream);
+  if (rc) return rc;
+  rc = anchor(true, true);
   if (rc) return rc;
   const double bb = h[SC_TRUE];
   const double tol2 = rtol * rtol * bb, goal2 = 100.0 * tol2;
