@@ -112,6 +112,13 @@ HM_HD int64_t stencil_prefix(int i, int N) {
   const int64_t even = k >= 1 ? 8 * (int64_t)k - 2 : 0;
   return (i & 1) ? even + stencil_n(2 * k, N) : even;
 }
+// CSR offset of row (i, j, k) of the lattice pattern (rows in node order)
+HM_HD int64_t row_start(const Lattice& L, int i, int j, int k) {
+  const int64_t T1 = stencil_prefix(L.Nx, L.Nx), T2 = stencil_prefix(L.Ny, L.Ny);
+  return stencil_prefix(k, L.Nz) * T1 * T2 +
+         (int64_t)stencil_n(k, L.Nz) *
+             (stencil_prefix(j, L.Ny) * T1 + (int64_t)stencil_n(j, L.Ny) * stencil_prefix(i, L.Nx));
+}
 
 // ------------------------------------------------------------ PCG device scalars
 // (shared by the solver and the operator kernels that finish a CG step's reductions)

@@ -21,13 +21,6 @@ __device__ __forceinline__ void node_of(int64_t n, const Lattice& L, int& i, int
   k = (int)(t / L.Ny);
 }
 
-__device__ __forceinline__ int64_t row_start(const Lattice& L, int i, int j, int k) {
-  const int64_t T1 = stencil_prefix(L.Nx, L.Nx), T2 = stencil_prefix(L.Ny, L.Ny);
-  return stencil_prefix(k, L.Nz) * T1 * T2 +
-         (int64_t)stencil_n(k, L.Nz) *
-             (stencil_prefix(j, L.Ny) * T1 + (int64_t)stencil_n(j, L.Ny) * stencil_prefix(i, L.Nx));
-}
-
 // CSR position of column (ci, cj, ck) within row (i, j, k): diagonal first, the rest
 // ascending (ascending lexicographic node number = z, then y, then x rank)
 __device__ __forceinline__ int pos_in_row(const Lattice& L, int i, int j, int k, int ci,

@@ -70,6 +70,40 @@ HM_HD constexpr TileTabs make_tile_tabs() {
   return t;
 }
 __device__ const TileTabs kTileTabs = make_tile_tabs();
+// the run starts and lengths (as kTileTabs.runoff / runlen) folded into immediates, so
+// that the tile set-up reads them without a load
+struct RunTabs { int off[16]; int len[16]; };
+HM_HD constexpr RunTabs make_run_tabs() {
+  RunTabs t{};
+  int off = 0;
+  for (int run = 0; run < 16; ++run) {
+    const int n2 = row_stencil(run & 3), n3 = row_stencil(run >> 2);
+    off += kRunPad[run];
+    t.off[run] = off;
+    int len = 0;
+    for (int r1 = 0; r1 < 4; ++r1) len += row_stencil(r1) * n2 * n3;
+    t.len[run] = len;
+    off += len;
+  }
+  return t;
+}
+HM_HD constexpr bool run_tabs_agree() {
+  for (int i = 0; i < 16; ++i)
+    if (make_run_tabs().off[i] != make_tile_tabs().runoff[i] ||
+        make_run_tabs().len[i] != make_tile_tabs().runlen[i])
+      return false;
+  return true;
+}
+static_assert(run_tabs_agree(), "run tables");
+template <int Q = 0>
+__device__ __forceinline__ int run_sel(int run, bool len) {
+  if constexpr (Q < 16) {
+    constexpr int o = make_run_tabs().off[Q], n = make_run_tabs().len[Q];
+    return run == Q ? (len ? n : o) : run_sel<Q + 1>(run, len);
+  } else {
+    return 0;
+  }
+}
 HM_HD constexpr int run_pad_total() {
   int s = 0;
   for (int i = 0; i < 16; ++i) s += kRunPad[i];
@@ -255,34 +289,40 @@ __device__ __forceinline__ void y2_task(const real* __restrict__ col1, const rea
 }
 
 // x: a (p2, p3) row of T2 (one or two terms) -> 16 values of the image at the byte
-// offsets pk (two 16-bit offsets per word); with ESS the elimination masks apply.
-template <int TX1, int TX2, bool TWO, bool ESS, typename real, int P = 0>
+// offsets pk (two 16-bit offsets per word); with ESS the elimination masks apply.  With
+// ROWS the values before elimination are also summed per row r1 into rs (the block's
+// row sums: its assembled vector, by the partition of unity of the parameter basis).
+template <int TX1, int TX2, bool TWO, bool ESS, bool ROWS, typename real, int P = 0>
 __device__ __forceinline__ void x_outputs(const real (&w1)[9], const real (&w2)[9],
                                           unsigned char* __restrict__ img, const uint32_t (&pk)[8],
-                                          uint32_t zmask, uint32_t omask) {
+                                          uint32_t zmask, uint32_t omask, real (&rs)[4]) {
   if constexpr (P < 16) {
     real v = pchain<TX1, P>(w1);
     if constexpr (TWO) v = pchain_acc<TX2, P>(w2, v);
+    if constexpr (ROWS) {
+      if constexpr (P == row_pair_base(pair_row_of(P))) rs[pair_row_of(P)] = v;
+      else rs[pair_row_of(P)] += v;
+    }
     if constexpr (ESS) {
       if ((zmask >> P) & 1u) v = ((omask >> P) & 1u) ? (real)1 : (real)0;
     }
     const uint32_t off = (P & 1) ? (pk[P >> 1] >> 16) : (pk[P >> 1] & 0xffffu);
     *reinterpret_cast<real*>(img + off) = v;
-    x_outputs<TX1, TX2, TWO, ESS, real, P + 1>(w1, w2, img, pk, zmask, omask);
+    x_outputs<TX1, TX2, TWO, ESS, ROWS, real, P + 1>(w1, w2, img, pk, zmask, omask, rs);
   }
 }
-template <int TX1, int TX2, bool TWO, typename real>
+template <int TX1, int TX2, bool TWO, bool ROWS, typename real>
 __device__ __forceinline__ void x_task(const real* __restrict__ row1, const real* __restrict__ row2,
                                        unsigned char* __restrict__ img, const uint32_t (&pk)[8],
-                                       bool ess, uint32_t zmask, uint32_t omask) {
+                                       bool ess, uint32_t zmask, uint32_t omask, real (&rs)[4]) {
   real w1[9], w2[9];
 #pragma unroll
   for (int l = 0; l < 9; ++l) {
     w1[l] = row1[l];
     w2[l] = TWO ? row2[l] : (real)0;
   }
-  if (ess) x_outputs<TX1, TX2, TWO, true>(w1, w2, img, pk, zmask, omask);
-  else x_outputs<TX1, TX2, TWO, false>(w1, w2, img, pk, zmask, omask);
+  if (ess) x_outputs<TX1, TX2, TWO, true, ROWS>(w1, w2, img, pk, zmask, omask, rs);
+  else x_outputs<TX1, TX2, TWO, false, ROWS>(w1, w2, img, pk, zmask, omask, rs);
 }
 
 // ------------------------------------------------------------ vector stages
@@ -413,6 +453,11 @@ __global__ void __launch_bounds__(256, 2)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t1 = blockIdx.x, t2 = blockIdx.y, t3 = blockIdx.z;
   const int e1 = 2 * t1 - 1, e2 = 2 * t2 - 1, e3 = 2 * t3 - 1;   // first halo'd element
+  const int xp2 = tid & 15, xp3 = tid >> 4;    // this thread's x task (p2, p3)
+  // its image offsets in an interior tile, loaded before the set-up's other global reads
+  // are waited for (one round trip to memory instead of two)
+  const uint4* const tab = reinterpret_cast<const uint4*>(&kTileTabs.inv[xp3][xp2][0]);
+  const uint4 tab_a = __ldg(tab), tab_b = __ldg(tab + 1);
 
   // the phases with work: a block, or a vector that its fields carry
   const uint32_t pm = (o.vals[0] != nullptr ? 1u : 0u) |
@@ -450,20 +495,25 @@ __global__ void __launch_bounds__(256, 2)
     // and may hold rows outside the mesh
     clipped |= tt[d] == 0 || 4 * tt[d] + 4 > Nn[d] - 1;
   }
-  int any = 0;
-  for (int i = tid; i < 343; i += 256) {
+  // the Dirichlet markers of the halo'd nodes [s3][s2][s1] (343, two per thread at most):
+  // loaded now, stored to shared memory once the first phase's fields have landed, so
+  // that the two latencies overlap
+  uint8_t em[2] = {0, 0};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int i = tid + 256 * h;
     const int s1 = i % 7, s2 = (i / 7) % 7, s3 = i / 49;
     const int gx = 4 * t1 - 2 + s1, gy = 4 * t2 - 2 + s2, gz = 4 * t3 - 2 + s3;
-    uint8_t m = 0;
-    if (ess != nullptr && gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 && gz < L.Nz)
-      m = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
-    S.ess[s3][s2][s1] = m;
-    any |= m;
+    if (i < 343 && ess != nullptr && gx >= 0 && gx < L.Nx && gy >= 0 && gy < L.Ny && gz >= 0 &&
+        gz < L.Nz)
+      em[h] = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
   }
-  if (indptr != nullptr && tid < 16) {
+  // CSR offsets of the rows (0, r2, r3): the lattice pattern's (the indptr the caller
+  // passes), computed rather than loaded
+  if (tid < 16) {
     const int r2 = tid & 3, r3 = tid >> 2;
     const int gy = 4 * t2 + r2, gz = 4 * t3 + r3;
-    S.rowptr[tid] = (gy < L.Ny && gz < L.Nz) ? indptr[4 * t1 + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] : 0;
+    S.rowptr[tid] = (gy < L.Ny && gz < L.Nz) ? (int32_t)row_start(L, 4 * t1, gy, gz) : 0;
   }
   if (clipped && tid < 12) {
     const int d = tid / 4, r = tid % 4;
@@ -479,7 +529,7 @@ __global__ void __launch_bounds__(256, 2)
       S.nst[d][r] = 0; S.clip[d][r] = 0; S.dk[d][r] = 0;
     }
   }
-  const bool has_ess = __syncthreads_or(any) != 0;
+  __syncthreads();
   // image layout: run starts (with the parity of the run's CSR offset when the copy-out
   // is a bulk copy) and lengths; a clipped tile packs its clipped rows
   constexpr bool kBulk = sizeof(real) == 8;
@@ -487,9 +537,9 @@ __global__ void __launch_bounds__(256, 2)
     const int run = tid;
     const int want = kBulk ? (S.rowptr[run] & 1) : 0;
     if (!clipped) {
-      const int a0 = kTileTabs.runoff[run];
+      const int a0 = run_sel(run, false);
       S.runstart[run] = a0 + ((want - a0) & 1);
-      S.runlen[run] = kTileTabs.runlen[run];
+      S.runlen[run] = run_sel(run, true);
     } else {
       int off = 0;
       for (int q = 0; q <= run; ++q) {
@@ -508,15 +558,12 @@ __global__ void __launch_bounds__(256, 2)
   __syncthreads();
 
   // ---- this thread's x task (p2, p3): image byte offsets and elimination masks
-  const int xp2 = tid & 15, xp3 = tid >> 4;
   uint32_t pk[8];
   {
     if (!clipped) {
       const int run = pair_row_of(xp2) + 4 * pair_row_of(xp3);
-      const uint32_t shift = (uint32_t)(S.runstart[run] - kTileTabs.runoff[run]);   // 0 or 1
-      const uint4* src = reinterpret_cast<const uint4*>(&kTileTabs.inv[xp3][xp2][0]);
-      const uint4 a = __ldg(src), b = __ldg(src + 1);
-      const uint32_t v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      const uint32_t shift = (uint32_t)(S.runstart[run] - run_sel(run, false));   // 0 or 1
+      const uint32_t v[8] = {tab_a.x, tab_a.y, tab_a.z, tab_a.w, tab_b.x, tab_b.y, tab_b.z, tab_b.w};
 #pragma unroll
       for (int i = 0; i < 8; ++i)   // both halves stay below 2^16
         pk[i] = (v[i] + shift * 0x10001u) * (uint32_t)sizeof(real);
@@ -544,7 +591,9 @@ __global__ void __launch_bounds__(256, 2)
     }
   }
   uint32_t zA = 0, oA = 0, zC = 0;
-  if (has_ess) {
+  bool has_ess = false;
+  // the elimination masks of this thread's x task, from the markers (at the first phase)
+  auto ess_masks = [&]() {
     const int r2 = pair_row_of(xp2), r3 = pair_row_of(xp3);
     const int c2 = pair_c(xp2), c3 = pair_c(xp3);
     const bool diag23 = c2 == r2 + 2 && c3 == r3 + 2;
@@ -560,7 +609,7 @@ __global__ void __launch_bounds__(256, 2)
       if (re && diag23 && pair_c(p) == pair_s(p)) oA |= 1u << p;
       if (re) zC |= 1u << p;
     }
-  }
+  };
 
   // ---- per-thread addresses of the z tasks
   const int zi = tid % 81;                     // (g1, g2) of the z task
@@ -575,12 +624,36 @@ __global__ void __launch_bounds__(256, 2)
   real* const U2 = U1 + 3 * 324;              // [term][r3][r2][g1]
   const real ihx = (real)(1.0 / L.hx), ihy = (real)(1.0 / L.hy), ihz = (real)(1.0 / L.hz);
 
+  // a vector entry: the source term (dR/dp), elimination, the store
+  auto write_vec = [&](int ph, real y) {
+    double* const vec = ph == 1 ? o.vec_adj : ph == 2 ? o.vec_state : o.vec_param;
+    if (ph == PH_C) {
+      const real src = (real)(L.hx * L.hy * L.hz) * src_1d_rt<real>(vr1, vl[0]) *
+                       src_1d_rt<real>(vr2, vl[1]) * src_1d_rt<real>(vr3, vl[2]);
+      y = fma((real)(-o.f), src, y);
+    }
+    const int gx = 4 * t1 + vr1, gy = 4 * t2 + vr2, gz = 4 * t3 + vr3;
+    if (gx < L.Nx && gy < L.Ny && gz < L.Nz) {
+      double v = (double)y;
+      if (o.zero_ess && ph != PH_WMM && S.ess[vr3 + 2][vr2 + 2][vr1 + 2]) v = 0.0;
+      vec[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] = v;
+    }
+  };
+
   int k = 0;
 #pragma unroll 1
   for (int ph = 0; ph < 4; ++ph) {
     if (!((pm >> ph) & 1u)) continue;
     const int buf = k & 1;
     const bool ok = mbar_wait(&S.mbar[buf], (uint32_t)(k >> 1) & 1u);
+    if (k == 0) {
+      // the markers: to shared memory, then this thread's elimination masks
+      uint8_t* const es = &S.ess[0][0][0];
+      es[tid] = em[0];
+      if (tid + 256 < 343) es[tid + 256] = em[1];
+      has_ess = __syncthreads_or(em[0] | em[1]) != 0;
+      if (has_ess) ess_masks();
+    }
     // the previous phase's image copies must have left the image before it is rewritten
     if (kBulk && tid < 16) bulk_wait_read();
     if (__syncthreads_or(!ok)) {
@@ -598,6 +671,9 @@ __global__ void __launch_bounds__(256, 2)
     double* const vec = ph == 0 ? nullptr : ph == 1 ? o.vec_adj : ph == 2 ? o.vec_state : o.vec_param;
     const int after = next_phase(ph);
     const int after2 = after >= 0 ? next_phase(after) : -1;
+    // with its block, a phase's vector is the block's row sums (summed in the x stage)
+    const bool rows = vals != nullptr && vec != nullptr;
+    real rs[4] = {0, 0, 0, 0};
 
     if (vals != nullptr) {
       // z: T1[0..2] from the phase's fields
@@ -612,7 +688,7 @@ __global__ void __launch_bounds__(256, 2)
         else if (tid < 243) z_task<TR, BI>(W + 54 + zbase, &S.T1[2][zt1]);
       }
       __syncthreads();
-      if (vec == nullptr && tid == 0 && after2 >= 0) {
+      if ((vec == nullptr || rows) && tid == 0 && after2 >= 0) {
         fence_proxy_async();
         issue_fields(&tmap, S, buf, after2, e1, e2, e3);
       }
@@ -640,12 +716,39 @@ __global__ void __launch_bounds__(256, 2)
       // x: the tile image
       {
         const int r = xp3 * kT2P + xp2 * 9;
-        if (ph == PH_A) x_task<TK, TM, true>(&S.T2[0][r], &S.T2[1][r], img, pk, has_ess, zA, oA);
-        else if (ph == PH_WMM) x_task<TM, TM, false>(&S.T2[0][r], (const real*)nullptr, img, pk, false, 0u, 0u);
-        else x_task<TR, TM, true>(&S.T2[0][r], &S.T2[1][r], img, pk, has_ess, zC, 0u);
+        if (ph == PH_A) {
+          x_task<TK, TM, true, false>(&S.T2[0][r], &S.T2[1][r], img, pk, has_ess, zA, oA, rs);
+        } else if (ph == PH_WMM) {
+          if (rows) x_task<TM, TM, false, true>(&S.T2[0][r], (const real*)nullptr, img, pk, false, 0u, 0u, rs);
+          else x_task<TM, TM, false, false>(&S.T2[0][r], (const real*)nullptr, img, pk, false, 0u, 0u, rs);
+        } else {
+          if (rows) x_task<TR, TM, true, true>(&S.T2[0][r], &S.T2[1][r], img, pk, has_ess, zC, 0u, rs);
+          else x_task<TR, TM, true, false>(&S.T2[0][r], &S.T2[1][r], img, pk, has_ess, zC, 0u, rs);
+        }
+      }
+      // row sums over the column pairs p2 of each row r2 (lanes b2 .. b2 + n2 - 1 of the
+      // half-warp, summed in lane order into lane b2)
+      if (rows) {
+#pragma unroll
+        for (int r1 = 0; r1 < 4; ++r1) {
+          const real v = rs[r1];
+          const real a1 = __shfl_down_sync(0xffffffffu, v, 1);
+          const real a2 = __shfl_down_sync(0xffffffffu, v, 2);
+          const real a3 = __shfl_down_sync(0xffffffffu, v, 3);
+          const real a4 = __shfl_down_sync(0xffffffffu, v, 4);
+          const real s3 = (v + a1) + a2;
+          rs[r1] = (xp2 == 0 || xp2 == 8) ? (s3 + a3) + a4 : s3;
+        }
       }
       if (kBulk) fence_proxy_async();   // the image stores, before the async copies read them
       __syncthreads();
+      // the leaders' sums [r1][p3][r2] into the y buffer (free after the x stage); the sums
+      // over p3 finish at the end of the phase
+      if (rows && (xp2 == 0 || xp2 == 5 || xp2 == 8 || xp2 == 13)) {
+        const int r2 = pair_row_of(xp2);
+#pragma unroll
+        for (int r1 = 0; r1 < 4; ++r1) S.T2[0][r1 * 64 + xp3 * 4 + r2] = rs[r1];
+      }
       // stream the image out, run by run (four consecutive rows, one stretch of CSR)
       const real* O = reinterpret_cast<const real*>(img);
       if constexpr (kBulk) {
@@ -670,8 +773,8 @@ __global__ void __launch_bounds__(256, 2)
         }
       }
     }
-    if (vec != nullptr) {
-      // the vector: z (fields still resident), y, x
+    if (vec != nullptr && !rows) {
+      // the vector alone: z (fields still resident), y, x
       if (ph == PH_C) vec_z<PH_C, BI>(W, U1, tid);
       else if (ph == PH_WUM) vec_z<PH_WUM, BI>(W, U1, tid);
       else vec_z<PH_WMM, BI>(W, U1, tid);
@@ -688,21 +791,18 @@ __global__ void __launch_bounds__(256, 2)
         real y = ph == PH_C ? vec_x<PH_C>(U2, vr1, vr2, vr3, ihx, ihy, ihz)
                : ph == PH_WUM ? vec_x<PH_WUM>(U2, vr1, vr2, vr3, ihx, ihy, ihz)
                               : vec_x<PH_WMM>(U2, vr1, vr2, vr3, ihx, ihy, ihz);
-        if (ph == PH_C) {
-          const real src = (real)(L.hx * L.hy * L.hz) * src_1d_rt<real>(vr1, vl[0]) *
-                           src_1d_rt<real>(vr2, vl[1]) * src_1d_rt<real>(vr3, vl[2]);
-          y = fma((real)(-o.f), src, y);
-        }
-        const int gx = 4 * t1 + vr1, gy = 4 * t2 + vr2, gz = 4 * t3 + vr3;
-        if (gx < L.Nx && gy < L.Ny && gz < L.Nz) {
-          double v = (double)y;
-          if (o.zero_ess && ph != PH_WMM && S.ess[vr3 + 2][vr2 + 2][vr1 + 2]) v = 0.0;
-          vec[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)] = v;
-        }
+        write_vec(ph, y);
       }
     }
     // the y buffers are rewritten by the next phase
     __syncthreads();
+    if (rows && tid < 64) {
+      // row (vr1, vr2, vr3): its sums over the column pairs p3, in order
+      const real* part = &S.T2[0][vr1 * 64 + row_pair_base(vr3) * 4 + vr2];
+      real y = (part[0] + part[4]) + part[8];
+      if (row_stencil(vr3) == 5) y = (y + part[12]) + part[16];
+      write_vec(ph, y);
+    }
     ++k;
   }
   if (kBulk && tid < 16) bulk_wait_all();

@@ -145,6 +145,32 @@ def test_assembly_is_bit_reproducible(cuda):
         assert np.array_equal(va[s], vb[s])
 
 
+@pytest.mark.parametrize("blocks", [(), ("C",), ("Wum", "Wmm"), BLOCKS])
+def test_vectors_alone_and_with_their_blocks_agree(cuda, blocks):
+    """A vector assembled with its block (the block's row sums) and alone (its own
+    contractions), with the Dirichlet rows zeroed, against each other and the oracle."""
+    from hippymfem_b200 import BoxMesh, LatticePattern
+
+    n = (7, 6, 9)
+    mesh = BoxMesh(n, (1.0, 0.8, 1.2))
+    mo = q2.Lattice(n, (1.0, 0.8, 1.2))
+    pat = LatticePattern(mesh, with_transpose=False)
+    u, m, p = _point(mesh.ndof, 6)
+    ess = mo.boundary_dofs()
+    _, alone, _ = _device_assemble(mesh, pat, u, m, p, ess=ess, f=0.6, blocks=(), zero_ess=True)
+    vals, mixed, _ = _device_assemble(mesh, pat, u, m, p, ess=ess, f=0.6, blocks=blocks,
+                                      zero_ess=True)
+    _, rvecs = _oracle(mo, u, m, p, f=0.6)
+    for s in range(3):
+        r = rvecs[s].copy()
+        if s != 1:
+            r[ess] = 0.0
+        assert _rel(mixed[s], alone[s]) <= 1e-13, (s, _rel(mixed[s], alone[s]))
+        assert _rel(mixed[s], r) <= TOL, s
+    for b in blocks:
+        assert np.isfinite(vals[b]).all(), b
+
+
 def test_fp32_contractions_error_is_bounded(cuda):
     from hippymfem_b200 import BoxMesh, LatticePattern
 
