@@ -7,9 +7,9 @@ of ``include/hippymfem_b200.h``); importing this package fails if it is not buil
 
 from ._lib import HM_FP32, HM_FP64, NotConvergedError  # noqa: F401  (loads the library)
 from .mesh import BoxMesh, DirichletBC, Q2Space  # noqa: F401
-from .modeling import (BiLaplacianPrior, DiscreteStateObservation, Model,  # noqa: F401
-                       PointwiseStateObservation,
-                       ReducedHessian, observation_operator)
+from .modeling import (BiLaplacianPrior, DeviceCSR, DiscreteStateObservation,  # noqa: F401
+                       Model, PointwiseStateObservation, ReducedHessian,
+                       device_observation_operator, observation_operator)
 from .pattern import LatticePattern, build_tables  # noqa: F401
 from .problem import ADJOINT, NVAR, PARAMETER, STATE, PDEVariationalProblem  # noqa: F401
 from .sparse import CSRBlock, MatrixFreeJacobian, MixedPCGSolver, PCGSolver  # noqa: F401

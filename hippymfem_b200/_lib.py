@@ -57,6 +57,10 @@ SIGNATURES = {
     "hm_lattice_diag_A": (_i32, [_p, _p, _i32, _p, _p, _p]),
     "hm_csr_spmv": (_i32, [_i64, _p, _p, _p, _p, _p, _d, _d, _p]),
     "hm_csr_spmv_t": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _d, _d, _p]),
+    "hm_lattice_observation_workspace_bytes": (_i64, [_i64]),
+    "hm_lattice_observation": (_i32, [_p, _p, _i64, _p, _p, _p, _p, _p]),
+    "hm_csr_transpose_workspace_bytes": (_i64, [_i64]),
+    "hm_csr_transpose": (_i32, [_i64, _i64, _i64, _p, _p, _p, _p, _p, _p, _p, _p]),
     "hm_csr_diag": (_i32, [_i64, _p, _p, _p, _p]),
     "hm_pcg_workspace_bytes": (_i64, [_i64]),
     "hm_pcg": (_i32, [_i64, _p, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _d, _i32, _i32, _p, _p,

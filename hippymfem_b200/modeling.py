@@ -20,31 +20,38 @@ from ._lib import check, lib, ptr, stream_ptr
 from .problem import ADJOINT, PARAMETER, STATE
 
 
-def _lagrange3(x):
-    return np.stack([2.0 * (x - 0.5) * (x - 1.0), -4.0 * x * (x - 1.0), 2.0 * x * (x - 0.5)], -1)
+def device_observation_operator(mesh, points):
+    """``B`` on the device (``hm_lattice_observation``): row ``o`` holds the 27 Q2 basis
+    values at ``points[o]`` in the element containing it (pointwiseObservation.py:94-170).
+    Points outside the box raise ``ValueError``, as the reference's ``missing="raise"``."""
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+    npts = pts.shape[0]
+    dev = mesh.device
+    P = torch.as_tensor(pts, device=dev)
+    indptr = torch.empty(npts + 1, dtype=torch.int32, device=dev)
+    indices = torch.empty(max(27 * npts, 1), dtype=torch.int32, device=dev)
+    values = torch.empty(max(27 * npts, 1), dtype=torch.float64, device=dev)
+    work = torch.empty(lib.hm_lattice_observation_workspace_bytes(npts), dtype=torch.uint8,
+                       device=dev)
+    rc = lib.hm_lattice_observation(mesh.handle, ptr(P), npts, ptr(indptr), ptr(indices),
+                                    ptr(values), ptr(work), stream_ptr())
+    if rc == _lib.HM_ERR_RANGE:
+        bad = ~np.all(np.isfinite(pts) & (pts >= 0.0) & (pts <= np.asarray(mesh.L)), axis=1)
+        raise ValueError("%d observation target(s) are outside the mesh, e.g. %s"
+                         % (int(bad.sum()), pts[bad][:3].tolist()))
+    check(rc, "hm_lattice_observation")
+    return DeviceCSR.from_device(indptr, indices[:27 * npts], values[:27 * npts],
+                                 (npts, mesh.ndof))
 
 
 def observation_operator(mesh, points):
-    """Host CSR ``B``: row ``o`` holds the 27 Q2 basis values of the element that
-    contains ``points[o]`` (clamped into the box)."""
-    pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
-    h = np.asarray(mesh.h)
-    n = np.asarray(mesh.n)
-    e = np.clip(np.floor(pts / h).astype(np.int64), 0, n - 1)
-    xi = pts / h - e
-    B1 = [_lagrange3(xi[:, d]) for d in range(3)]
-    Nx, Ny, _ = mesh.N
-    a = np.arange(27)
-    a1, a2, a3 = a % 3, (a // 3) % 3, a // 9
-    cols = ((2 * e[:, 0:1] + a1) + Nx * ((2 * e[:, 1:2] + a2) + Ny * (2 * e[:, 2:3] + a3)))
-    vals = B1[0][:, a1] * B1[1][:, a2] * B1[2][:, a3]
-    rows = np.repeat(np.arange(len(pts)), 27)
-    return sp.csr_matrix((vals.reshape(-1), (rows, cols.reshape(-1))),
-                         shape=(len(pts), mesh.ndof))
+    """Host (scipy) copy of ``device_observation_operator(mesh, points)``."""
+    return device_observation_operator(mesh, points).to_scipy()
 
 
 class DeviceCSR:
-    """A general (rectangular) CSR matrix on the device, applied by ``hm_csr_spmv``."""
+    """A general (rectangular) CSR matrix on the device, applied by ``hm_csr_spmv``;
+    ``transpose()`` by ``hm_csr_transpose``."""
 
     def __init__(self, M, device):
         M = sp.csr_matrix(M)
@@ -53,6 +60,35 @@ class DeviceCSR:
         self.indptr = torch.as_tensor(M.indptr.astype(np.int32), device=device)
         self.indices = torch.as_tensor(M.indices.astype(np.int32), device=device)
         self.values = torch.as_tensor(M.data.astype(np.float64), device=device)
+
+    @classmethod
+    def from_device(cls, indptr, indices, values, shape):
+        self = cls.__new__(cls)
+        self.shape = (int(shape[0]), int(shape[1]))
+        self.indptr, self.indices, self.values = indptr, indices, values
+        return self
+
+    @property
+    def nnz(self):
+        return int(self.values.numel())
+
+    def transpose(self):
+        nrow, ncol = self.shape
+        dev = self.values.device
+        nnz = self.nnz
+        tindptr = torch.empty(ncol + 1, dtype=torch.int32, device=dev)
+        tindices = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        tvalues = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+        work = torch.empty(lib.hm_csr_transpose_workspace_bytes(ncol), dtype=torch.uint8,
+                           device=dev)
+        check(lib.hm_csr_transpose(nrow, ncol, nnz, ptr(self.indptr), ptr(self.indices),
+                                   ptr(self.values), ptr(tindptr), ptr(tindices), ptr(tvalues),
+                                   ptr(work), stream_ptr()), "hm_csr_transpose")
+        return DeviceCSR.from_device(tindptr, tindices[:nnz], tvalues[:nnz], (ncol, nrow))
+
+    def to_scipy(self):
+        return sp.csr_matrix((self.values.cpu().numpy(), self.indices.cpu().numpy(),
+                              self.indptr.cpu().numpy()), shape=self.shape)
 
     def mult(self, x, y, alpha=1.0, beta=0.0):
         check(lib.hm_csr_spmv(self.shape[0], ptr(self.indptr), ptr(self.indices),
@@ -70,14 +106,25 @@ class DiscreteStateObservation:
         if noise_variance == 0:
             raise ZeroDivisionError("noise_variance must not be 0; use 1.0 for a deterministic "
                                     "inverse problem")
-        self.Bh = sp.csr_matrix(B)
-        self.B = DeviceCSR(self.Bh, device)
-        self.Bt = DeviceCSR(self.Bh.T.tocsr(), device)
-        nobs = self.Bh.shape[0]
-        self.d = (torch.as_tensor(np.asarray(data, dtype=np.float64), device=device)
-                  if data is not None else torch.zeros(nobs, dtype=torch.float64, device=device))
+        self.B = B if isinstance(B, DeviceCSR) else DeviceCSR(B, device)
+        self.Bt = self.B.transpose()
+        self._Bh = None
+        nobs = self.B.shape[0]
+        if isinstance(data, torch.Tensor):
+            self.d = data.to(device=device, dtype=torch.float64).clone()
+        elif data is not None:
+            self.d = torch.as_tensor(np.asarray(data, dtype=np.float64), device=device)
+        else:
+            self.d = torch.zeros(nobs, dtype=torch.float64, device=device)
         self.Bu = torch.zeros(nobs, dtype=torch.float64, device=device)
         self.noise_variance = float(noise_variance)
+
+    @property
+    def Bh(self):
+        """Host (scipy) copy of ``B``."""
+        if self._Bh is None:
+            self._Bh = self.B.to_scipy()
+        return self._Bh
 
     def cost(self, x):
         self.B.mult(x[STATE], self.Bu)
@@ -113,7 +160,7 @@ class DiscreteStateObservation:
 def PointwiseStateObservation(Vh, obs_points, data=None, noise_variance=None):
     """Misfit for pointwise observations of the state at ``obs_points``."""
     mesh = Vh.mesh
-    return DiscreteStateObservation(observation_operator(mesh, obs_points), data,
+    return DiscreteStateObservation(device_observation_operator(mesh, obs_points), data,
                                     noise_variance, device=mesh.device)
 
 

@@ -125,8 +125,7 @@ class _Workspace:
                     for k in ("u", "p", "uh", "ph", "zero", "r1", "r2", "r3", "y")}
         # the misfit keeps scratch of its own: one per workspace (slots run concurrently)
         mis = ms.misfit
-        self.misfit = DiscreteStateObservation(mis.Bh, mis.d.cpu().numpy(), mis.noise_variance,
-                                               device=dev)
+        self.misfit = DiscreteStateObservation(mis.B, mis.d, mis.noise_variance, device=dev)
         self.nbytes = ms.footprint(precision, multigrid)
         self.in_use = False
         self.last_used = 0.0

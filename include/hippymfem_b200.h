@@ -279,6 +279,31 @@ int hm_pcg_mg(hm_mg* mg, const double* d_b, double* d_x, double rtol, int maxite
               int check_every, void* d_work, int* iterations, double* relres, void* stream);
 int hm_pcg_plan_set_mg(hm_pcg_plan* plan, hm_mg* mg);
 
+/* ---------------------------------------------------------------- observations
+ * The pointwise observation operator B (npts x ndof) of the lattice's Q2 space: row o
+ * holds the 27 basis values at d_points[3 o .. 3 o + 2] in the element containing it,
+ * columns ascending; d_indptr[o] = 27 o.  Replaces the reference's
+ * PointwiseObservation._build (modeling/pointwiseObservation.py:94-170; MFEM FindPoints
+ * and the element shape functions) for a uniform box.  Targets outside the box (beyond
+ * 1e-12 of an element) or not finite return HM_ERR_RANGE, as the reference's
+ * missing="raise" raises ValueError (:106-112); their rows are zeros.  d_work: at least
+ * hm_lattice_observation_workspace_bytes(npts).  Synchronises with the stream to read
+ * the range flag. */
+int64_t hm_lattice_observation_workspace_bytes(int64_t npts);
+int hm_lattice_observation(const hm_lattice* h, const double* d_points, int64_t npts,
+                           int32_t* d_indptr, int32_t* d_indices, double* d_vals,
+                           void* d_work, void* stream);
+/* The transpose of an nrow x ncol CSR matrix with nnz entries, as CSR (ncol + 1 row
+ * pointers, rows ordered by source row): B^T for the adjoint source and W_uu of the
+ * pointwise misfit (modeling/misfit.py:65-110, PointwiseObservation.multTranspose
+ * :210-224).  Deterministic whatever the order of its atomics.  Column indices outside
+ * [0, ncol) or row pointers outside [0, nnz] return HM_ERR_RANGE.  d_work: at least
+ * hm_csr_transpose_workspace_bytes(ncol).  Synchronises with the stream. */
+int64_t hm_csr_transpose_workspace_bytes(int64_t ncol);
+int hm_csr_transpose(int64_t nrow, int64_t ncol, int64_t nnz, const int32_t* d_indptr,
+                     const int32_t* d_indices, const double* d_vals, int32_t* d_tindptr,
+                     int32_t* d_tindices, double* d_tvals, void* d_work, void* stream);
+
 /* deterministic FP64 dot product into *d_out (a fixed-order two-pass reduction) */
 int64_t hm_dot_workspace_bytes(int64_t n);
 int hm_dot(int64_t n, const double* d_x, const double* d_y, double* d_out, void* d_work,

@@ -49,7 +49,7 @@ def test_matrix_free_hessian_matches_assembled(cuda):
     out = []
     for mf in (False, True):
         mesh, V, prob, x, rng = _point((8, 7, 6), seed=3)
-        pts = interior_points(128, seed=5)
+        pts = interior_points(128, seed=5) * np.array([1.0, 0.8, 1.2])   # inside the box
         misfit = PointwiseStateObservation(V, pts, data=np.zeros(128), noise_variance=1e-4)
         model = Model(prob, None, misfit)
         u, p = V.vector(), V.vector()
