@@ -78,6 +78,7 @@ SIGNATURES = {
     "hm_mg_setup": (_i32, [_p, _p, _p, _p, _p]),
     "hm_mg_apply": (_i32, [_p, _p, _p, _p]),
     "hm_mg_levels": (_i32, [_p]),
+    "hm_mg_set_tail_nodes": (_i32, [_p, _i64]),
     "hm_mg_destroy": (_i32, [_p]),
     "hm_pcg_mg": (_i32, [_p, _p, _p, _d, _i32, _i32, _p, _p, _p, _p]),
     "hm_pcg_plan_set_mg": (_i32, [_p, _p]),

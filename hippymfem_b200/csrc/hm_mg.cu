@@ -51,6 +51,7 @@ struct hm_mg {
   int degree, coarse_degree;
   double* scratch;       // partial sums of the set-up's inner products, eigenvalue state
   const uint8_t* checked_ess;   // the markers last found to be the whole boundary
+  int tail_first;        // first level of the one-CTA tail (nlev: none)
 };
 
 namespace hm {
@@ -61,16 +62,14 @@ __device__ __forceinline__ bool on_boundary(int i, int j, int k, int Nx, int Ny,
   return i == 0 || j == 0 || k == 0 || i == Nx - 1 || j == Ny - 1 || k == Nz - 1;
 }
 
-// y = A_l x for a Q1 level: node-centric, identity on the boundary, boundary values of
+// (A_l x)[n] for a Q1 level: node-centric, identity on the boundary, boundary values of
 // x taken as zero in the interior rows
-__global__ void __launch_bounds__(256) k_q1_apply(MGLevel lv, const double* __restrict__ x,
-                                                  double* __restrict__ y) {
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= lv.nodes) return;
+__device__ __forceinline__ double q1_apply_at(const MGLevel& lv, const double* __restrict__ x,
+                                              int64_t n) {
   const int i = (int)(n % lv.Nx);
   const int64_t t = n / lv.Nx;
   const int j = (int)(t % lv.Ny), k = (int)(t / lv.Ny);
-  if (on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz)) { y[n] = x[n]; return; }
+  if (on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz)) return x[n];
   // 1D element matrices: k = [1 -1; -1 1] / h, m = [2 1; 1 2] h / 6
   const double kx[2] = {1.0 / lv.hx, -1.0 / lv.hx}, ky[2] = {1.0 / lv.hy, -1.0 / lv.hy},
                kz[2] = {1.0 / lv.hz, -1.0 / lv.hz};
@@ -111,7 +110,12 @@ __global__ void __launch_bounds__(256) k_q1_apply(MGLevel lv, const double* __re
             }
         acc = fma(c, s, acc);
       }
-  y[n] = acc;
+  return acc;
+}
+__global__ void __launch_bounds__(256) k_q1_apply(MGLevel lv, const double* __restrict__ x,
+                                                  double* __restrict__ y) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n < lv.nodes) y[n] = q1_apply_at(lv, x, n);
 }
 
 __global__ void k_q1_diag(MGLevel lv, double* __restrict__ diag) {
@@ -161,14 +165,12 @@ __global__ void k_coef_coarsen(MGLevel f, MGLevel c, const double* __restrict__ 
 
 // b_c = R r_f (full weighting, the transpose of trilinear interpolation); 0 on the
 // coarse boundary
-__global__ void k_restrict(MGLevel f, MGLevel c, const double* __restrict__ rf,
-                           double* __restrict__ bc) {
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= c.nodes) return;
+__device__ __forceinline__ double restrict_at(const MGLevel& f, const MGLevel& c,
+                                              const double* __restrict__ rf, int64_t n) {
   const int i = (int)(n % c.Nx);
   const int64_t t = n / c.Nx;
   const int j = (int)(t % c.Ny), k = (int)(t / c.Ny);
-  if (on_boundary(i, j, k, c.Nx, c.Ny, c.Nz)) { bc[n] = 0.0; return; }
+  if (on_boundary(i, j, k, c.Nx, c.Ny, c.Nz)) return 0.0;
   const double w[3] = {0.5, 1.0, 0.5};
   double s = 0.0;
 #pragma unroll
@@ -180,14 +182,18 @@ __global__ void k_restrict(MGLevel f, MGLevel c, const double* __restrict__ rf,
 #pragma unroll
       for (int di = 0; di < 3; ++di) s = fma(wjk * w[di], rf[row + 2 * i + di - 1], s);
     }
-  bc[n] = s;
+  return s;
+}
+__global__ void k_restrict(MGLevel f, MGLevel c, const double* __restrict__ rf,
+                           double* __restrict__ bc) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n < c.nodes) bc[n] = restrict_at(f, c, rf, n);
 }
 
 // x_f += P x_c (trilinear); fine boundary nodes untouched
-__global__ void k_prolong_add(MGLevel f, MGLevel c, const double* __restrict__ xc,
-                              double* __restrict__ xf) {
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= f.nodes) return;
+__device__ __forceinline__ void prolong_add_at(const MGLevel& f, const MGLevel& c,
+                                               const double* __restrict__ xc,
+                                               double* __restrict__ xf, int64_t n) {
   const int i = (int)(n % f.Nx);
   const int64_t t = n / f.Nx;
   const int j = (int)(t % f.Ny), k = (int)(t / f.Ny);
@@ -201,6 +207,11 @@ __global__ void k_prolong_add(MGLevel f, MGLevel c, const double* __restrict__ x
       for (int di = 0; di < ni; ++di)
         s += xc[(ci0 + di) + (int64_t)c.Nx * ((cj0 + dj) + (int64_t)c.Ny * (ck0 + dk))];
   xf[n] += wi * wj * wk * s;
+}
+__global__ void k_prolong_add(MGLevel f, MGLevel c, const double* __restrict__ xc,
+                              double* __restrict__ xf) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n < f.nodes) prolong_add_at(f, c, xc, xf, n);
 }
 
 // Chebyshev-Jacobi: start (r = b - t, or r = b with t == nullptr; d = r / (theta diag);
@@ -234,6 +245,82 @@ __global__ void k_cheb_step(int64_t n, double* __restrict__ x, double* __restric
 __global__ void k_cheb_finish(int64_t n, double* __restrict__ x, const double* __restrict__ d) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] += d[i];
+}
+
+// ---- the small levels of a cycle in one CTA
+// The Q1 levels from the first with at most kTailNodes nodes down to the coarsest hold a
+// few thousand nodes together; launched level by level they cost ~14 launches per level
+// and 2 per step of the coarse solve, each mostly launch latency.  One CTA runs that
+// whole part of the V-cycle (the same smoothing, restriction and prolongation, node for
+// node, with block barriers where the launches were).
+constexpr int kTailMax = 8;
+constexpr int64_t kTailNodes = 5000;
+constexpr int kTailThreads = 512;
+struct MGTail {
+  MGLevel lv[kTailMax];
+  int count;
+};
+// Chebyshev smoothing of level lv inside the CTA (as smooth() launches it)
+__device__ void tail_smooth(const MGLevel& lv, bool zero_x, bool want_r, int degree) {
+  const int64_t n = lv.nodes;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const double* __restrict__ b = lv.b;
+  double* __restrict__ x = lv.x;
+  double* __restrict__ r = lv.r;
+  double* __restrict__ d = lv.d;
+  double* __restrict__ t = lv.t;
+  const double* __restrict__ diag = lv.diag;
+  const double inv_theta = 1.0 / lv.cheb[0];
+  if (!zero_x) {
+    for (int64_t i = tid; i < n; i += nt) t[i] = q1_apply_at(lv, x, i);
+    __syncthreads();
+  }
+  for (int64_t i = tid; i < n; i += nt) {
+    const double ri = zero_x ? b[i] : b[i] - t[i];
+    r[i] = ri;
+    d[i] = inv_theta * ri / diag[i];
+    if (zero_x) x[i] = 0.0;
+  }
+  __syncthreads();
+  for (int k = 1; k <= degree; ++k) {
+    const bool last = k == degree;
+    if (last && !want_r) {
+      for (int64_t i = tid; i < n; i += nt) x[i] += d[i];
+      __syncthreads();
+      break;
+    }
+    for (int64_t i = tid; i < n; i += nt) t[i] = q1_apply_at(lv, d, i);
+    __syncthreads();
+    const double c1 = lv.cheb[1 + k], c2 = lv.cheb[1 + kChebMax + k];
+    for (int64_t i = tid; i < n; i += nt) {
+      const double di = d[i];
+      x[i] += di;
+      const double ri = r[i] - t[i];
+      r[i] = ri;
+      if (!last) d[i] = fma(c1, di, c2 * ri / diag[i]);
+    }
+    __syncthreads();
+  }
+}
+// the V-cycle from T.lv[0] (right-hand side in its b, result in its x) to the coarsest
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(const __grid_constant__ MGTail T) {
+  __shared__ MGLevel L[kTailMax];
+  if (threadIdx.x < (unsigned)T.count) L[threadIdx.x] = T.lv[threadIdx.x];
+  __syncthreads();
+  const int nl = T.count;
+  for (int l = 0; l + 1 < nl; ++l) {
+    tail_smooth(L[l], true, true, L[l].degree);
+    for (int64_t i = threadIdx.x; i < L[l + 1].nodes; i += blockDim.x)
+      L[l + 1].b[i] = restrict_at(L[l], L[l + 1], L[l].r, i);
+    __syncthreads();
+  }
+  tail_smooth(L[nl - 1], true, false, L[nl - 1].degree);
+  for (int l = nl - 2; l >= 0; --l) {
+    for (int64_t i = threadIdx.x; i < L[l].nodes; i += blockDim.x)
+      prolong_add_at(L[l], L[l + 1], L[l + 1].x, L[l].x, i);
+    __syncthreads();
+    tail_smooth(L[l], false, false, L[l].degree);
+  }
 }
 
 // set-up: a deterministic pseudo-random start vector (0 on the boundary), partial sums of
@@ -369,6 +456,13 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
 
 int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_t s) {
   int rc;
+  if (l == mg->tail_first && b == mg->lv[l].b && x == mg->lv[l].x) {
+    MGTail T{};
+    T.count = mg->nlev - l;
+    for (int q = 0; q < T.count; ++q) T.lv[q] = mg->lv[l + q];
+    k_mg_tail<<<1, kTailThreads, 0, s>>>(T);
+    return HM_OK;
+  }
   if (l == mg->nlev - 1) return smooth(mg, l, b, x, true, false, mg->coarse_degree, clean, s);
   MGLevel& lv = mg->lv[l];
   MGLevel& cv = mg->lv[l + 1];
@@ -377,6 +471,14 @@ int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_
   if ((rc = vcycle(mg, l + 1, cv.b, cv.x, clean, s))) return rc;
   k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, cv.x, x);
   return smooth(mg, l, b, x, false, false, mg->degree, clean, s);
+}
+
+// the one-CTA tail: the Q1 levels (l >= 1) of at most max_nodes nodes, at most kTailMax
+// of them (max_nodes = 0: none)
+void set_tail(hm_mg* mg, int64_t max_nodes) {
+  mg->tail_first = mg->nlev;
+  for (int l = mg->nlev - 1; l >= 1 && mg->lv[l].nodes <= max_nodes && mg->nlev - l <= kTailMax; --l)
+    mg->tail_first = l;
 }
 
 // the level hierarchy of a lattice (no memory touched)
@@ -449,6 +551,7 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
   mg->degree = degree;
   mg->coarse_degree = coarse_degree;
   mg->nlev = plan_levels(*L, mg->lv, 16);
+  set_tail(mg, kTailNodes);
   double* w = static_cast<double*>(work);
   auto take = [&](int64_t n) { double* p = w; w += n; return p; };
   mg->scratch = take(3 * kMGBlocks + 64);
@@ -525,6 +628,12 @@ extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const doubl
     k_mg_cheb_coeffs<<<1, 32, 0, s>>>(eig, coarsest ? 64.0 : 4.0, lv.degree, lv.cheb);
   }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+extern "C" int hm_mg_set_tail_nodes(hm_mg* mg, int64_t max_nodes) {
+  if (!mg || max_nodes < 0) return HM_ERR_ARG;
+  set_tail(mg, max_nodes);
+  return HM_OK;
 }
 
 extern "C" int hm_mg_apply(hm_mg* mg, const double* r, double* z, void* stream) {

@@ -316,6 +316,11 @@ class Multigrid:
         check(lib.hm_mg_apply(self._mg, ptr(r), ptr(z), stream_ptr(stream)), "hm_mg_apply")
         return z
 
+    def set_tail_nodes(self, max_nodes):
+        """Levels of at most ``max_nodes`` nodes run as one CTA-wide kernel (0: none)."""
+        check(lib.hm_mg_set_tail_nodes(self._mg, int(max_nodes)), "hm_mg_set_tail_nodes")
+        return self
+
     def close(self):
         if self._mg:
             lib.hm_mg_destroy(self._mg)

@@ -46,6 +46,22 @@ def test_vcycle_is_symmetric_and_positive(cuda):
     assert float(torch.dot(u, Vu)) > 0 and float(torch.dot(v, Vv)) > 0
 
 
+@pytest.mark.parametrize("n,L", [((64, 32, 32), (1.0, 0.5, 0.5)), ((16, 8, 12), (1.0, 0.6, 0.9))])
+def test_one_cta_tail_matches_the_level_by_level_cycle(cuda, n, L):
+    """The small levels run as one CTA-wide kernel: the same cycle as their level-by-level
+    launches (the same arithmetic node for node), at every tail size."""
+    from hippymfem_b200.sparse import Multigrid
+
+    mesh, V, prob, m, A = _jacobian(n, L)
+    r = _interior(mesh, V, prob.bc0.mask, 7)
+    mg = Multigrid(mesh).setup(A.jac, A.ess, A._diag)
+    ref = mg.set_tail_nodes(0).apply(r, V.vector())
+    for nodes in (5000, 40000, 10 ** 9):
+        z = mg.set_tail_nodes(nodes).apply(r, V.vector())
+        err = float((z - ref).abs().max() / ref.abs().max())
+        assert err <= 1e-14, (nodes, err)
+
+
 @pytest.mark.parametrize("n", [(12, 12, 12), (32, 32, 32)])
 def test_mg_pcg_matches_jacobi_pcg_in_few_iterations(cuda, n):
     from hippymfem_b200.sparse import MGPCGSolver, PCGSolver
