@@ -37,6 +37,8 @@ struct MGLevel {
   double* cheb;          // Chebyshev on the device: [0] theta (d0 = r / (theta diag)),
                          // [1 + k] c1_k, [1 + kChebMax + k] c2_k (d = c1 d + c2 r / diag)
   int degree;
+  double* cinv;          // coarsest level with few interior nodes: the inverse of its
+                         // interior block (row-major), solved exactly; else nullptr
 };
 constexpr int kChebMax = 40;
 
@@ -247,6 +249,67 @@ __global__ void k_cheb_finish(int64_t n, double* __restrict__ x, const double* _
     x[i] += d[i];
 }
 
+// ---- exact solve of a small coarsest level
+// Interior node q of a level <-> (1 + q % (Nx-2), 1 + (q / (Nx-2)) % (Ny-2), ...).
+constexpr int kCoarseDirectMax = 64;
+__device__ __forceinline__ int64_t interior_node(const MGLevel& lv, int q) {
+  const int ax = lv.Nx - 2, ay = lv.Ny - 2;
+  return (1 + q % ax) + (int64_t)lv.Nx * ((1 + (q / ax) % ay) + (int64_t)lv.Ny * (1 + q / (ax * ay)));
+}
+__host__ __device__ inline int interior_count(const MGLevel& lv) {
+  return (lv.Nx - 2) * (lv.Ny - 2) * (lv.Nz - 2);
+}
+// set-up (one CTA): the interior block column by column (the operator on unit vectors in
+// lv.t), then its inverse by Gauss-Jordan elimination (SPD: no pivoting), into lv.cinv
+__global__ void __launch_bounds__(256) k_coarse_factor(MGLevel lv) {
+  __shared__ double A[kCoarseDirectMax][kCoarseDirectMax + 1];
+  const int n = interior_count(lv);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int64_t i = tid; i < lv.nodes; i += nt) lv.t[i] = 0.0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (tid == 0) lv.t[interior_node(lv, j)] = 1.0;
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) A[i][j] = q1_apply_at(lv, lv.t, interior_node(lv, i));
+    __syncthreads();
+    if (tid == 0) lv.t[interior_node(lv, j)] = 0.0;
+    __syncthreads();
+  }
+  for (int k = 0; k < n; ++k) {
+    const double p = A[k][k];
+    __syncthreads();
+    if (tid == 0) A[k][k] = 1.0;
+    __syncthreads();
+    for (int j = tid; j < n; j += nt) A[k][j] = A[k][j] / p;
+    __syncthreads();
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e % n;
+      if (i != k && j != k) A[i][j] = fma(-A[i][k], A[k][j], A[i][j]);
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += nt)
+      if (i != k) A[i][k] = -A[i][k] * A[k][k];
+    __syncthreads();
+  }
+  for (int e = tid; e < n * n; e += nt) lv.cinv[e] = A[e / n][e % n];
+}
+// x = A_l^{-1} b for the small coarsest level, inside one CTA (x zero on the boundary)
+__device__ void coarse_direct(const MGLevel& lv, const double* __restrict__ b, double* __restrict__ x) {
+  const int n = interior_count(lv);
+  for (int64_t i = threadIdx.x; i < lv.nodes; i += blockDim.x) x[i] = 0.0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double acc = 0.0;
+    for (int j = 0; j < n; ++j) acc = fma(lv.cinv[i * n + j], b[interior_node(lv, j)], acc);
+    x[interior_node(lv, i)] = acc;
+  }
+  __syncthreads();
+}
+__global__ void __launch_bounds__(256) k_coarse_solve(MGLevel lv, const double* __restrict__ b,
+                                                      double* __restrict__ x) {
+  coarse_direct(lv, b, x);
+}
+
 // ---- the small levels of a cycle in one CTA
 // The Q1 levels from the first with at most kTailNodes nodes down to the coarsest hold a
 // few thousand nodes together; launched level by level they cost ~14 launches per level
@@ -254,7 +317,7 @@ __global__ void k_cheb_finish(int64_t n, double* __restrict__ x, const double* _
 // whole part of the V-cycle (the same smoothing, restriction and prolongation, node for
 // node, with block barriers where the launches were).
 constexpr int kTailMax = 8;
-constexpr int64_t kTailNodes = 5000;
+constexpr int64_t kTailNodes = 1000;
 constexpr int kTailThreads = 512;
 struct MGTail {
   MGLevel lv[kTailMax];
@@ -314,7 +377,8 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const __grid_constant_
       L[l + 1].b[i] = restrict_at(L[l], L[l + 1], L[l].r, i);
     __syncthreads();
   }
-  tail_smooth(L[nl - 1], true, false, L[nl - 1].degree);
+  if (L[nl - 1].cinv) coarse_direct(L[nl - 1], L[nl - 1].b, L[nl - 1].x);
+  else tail_smooth(L[nl - 1], true, false, L[nl - 1].degree);
   for (int l = nl - 2; l >= 0; --l) {
     for (int64_t i = threadIdx.x; i < L[l].nodes; i += blockDim.x)
       prolong_add_at(L[l], L[l + 1], L[l + 1].x, L[l].x, i);
@@ -463,7 +527,13 @@ int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_
     k_mg_tail<<<1, kTailThreads, 0, s>>>(T);
     return HM_OK;
   }
-  if (l == mg->nlev - 1) return smooth(mg, l, b, x, true, false, mg->coarse_degree, clean, s);
+  if (l == mg->nlev - 1) {
+    if (mg->lv[l].cinv) {
+      k_coarse_solve<<<1, 256, 0, s>>>(mg->lv[l], b, x);
+      return HM_OK;
+    }
+    return smooth(mg, l, b, x, true, false, mg->coarse_degree, clean, s);
+  }
   MGLevel& lv = mg->lv[l];
   MGLevel& cv = mg->lv[l + 1];
   if ((rc = smooth(mg, l, b, x, true, true, mg->degree, clean, s))) return rc;
@@ -534,7 +604,8 @@ extern "C" int64_t hm_mg_workspace_bytes(const hm_lattice* h) {
   if (!L) return 0;
   MGLevel lv[16];
   const int nl = plan_levels(*L, lv, 16);
-  int64_t doubles = 3 * L->ndof + 3 * kMGBlocks + 64 + nl * (2 * kChebMax + 8);
+  int64_t doubles = 3 * L->ndof + 3 * kMGBlocks + 64 + nl * (2 * kChebMax + 8) +
+                    kCoarseDirectMax * kCoarseDirectMax + 8;
   for (int l = 1; l < nl; ++l) doubles += lv[l].elems + 6 * lv[l].nodes + 8;
   return doubles * (int64_t)sizeof(double);
 }
@@ -566,7 +637,15 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
     lv.diag = take(lv.nodes);
     lv.x = take(lv.nodes); lv.b = take(lv.nodes); lv.r = take(lv.nodes);
     lv.d = take(lv.nodes); lv.t = take(lv.nodes);
+    lv.cinv = nullptr;
     w += 8;
+  }
+  z.cinv = nullptr;
+  // an exact coarse solve when the coarsest Q1 level has few interior nodes
+  if (mg->nlev > 1) {
+    MGLevel& c = mg->lv[mg->nlev - 1];
+    const int ni = interior_count(c);
+    if (ni >= 1 && ni <= kCoarseDirectMax) c.cinv = take(kCoarseDirectMax * kCoarseDirectMax);
   }
   *out = mg;
   return HM_OK;
@@ -626,6 +705,7 @@ extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const doubl
     const bool coarsest = l == mg->nlev - 1;
     lv.degree = coarsest ? mg->coarse_degree : mg->degree;
     k_mg_cheb_coeffs<<<1, 32, 0, s>>>(eig, coarsest ? 64.0 : 4.0, lv.degree, lv.cheb);
+    if (coarsest && lv.cinv) k_coarse_factor<<<1, 256, 0, s>>>(lv);
   }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
