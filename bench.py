@@ -53,10 +53,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", type=int, default=2000,
                     help="requests of the serving trace (0: skip)")
-    ap.add_argument("--config", choices=("main", "precision", "differentiation"), default="main",
+    ap.add_argument("--config", choices=("main", "precision", "differentiation", "solve"),
+                    default="main",
                     help="precision: 128^3, FP32 contractions and mixed-precision Hessian "
                          "actions against FP64; differentiation: 32^3 finite-difference "
-                         "checks of the autograd wrappers")
+                         "checks of the autograd wrappers; solve: one incremental solve "
+                         "(FP64 multigrid-PCG, rtol 1e-12) at --n, repeated")
     return ap.parse_args()
 
 
@@ -734,6 +736,48 @@ def run_differentiation(a, n=32, ndir=16, h=1e-6):
     print(json.dumps(line), flush=True)
 
 
+def run_solve(a):
+    """One incremental solve A x = b at n^3 (the matrix-free FP64 Jacobian at the
+    benchmark field, multigrid-PCG to rtol 1e-12, graph-replayed in a side stream),
+    warm-up then --steps timed solves with CUDA events."""
+    import torch
+
+    from hippymfem_b200 import BoxMesh, DirichletBC, PDEVariationalProblem, Q2Space
+    from hippymfem_b200.sparse import MGPCGSolver
+    from hippymfem_b200.synthetic import log_conductivity
+
+    mesh = BoxMesh(a.n)
+    V = Q2Space(mesh)
+    prob = PDEVariationalProblem([V, V, V], f=1.0, bc=DirichletBC(V), solver_tolerance=1e-12,
+                                 matrix_free_solves=True)
+    m = V.project(lambda x: log_conductivity(x, seed=0, sigma=0.1))
+    A, _ = prob._jacobian([None, m, None])
+    b = torch.as_tensor(np.random.default_rng(1).standard_normal(mesh.ndof),
+                        device=mesh.device).masked_fill_(prob.bc0.mask, 0.0)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        solver = MGPCGSolver(A, rel_tolerance=1e-12)
+        x = V.vector()
+        for _ in range(max(a.warmup, 1)):
+            solver.solve(x, b)
+        s.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(a.steps):
+            solver.solve(x, b)
+        e1.record(s)
+        s.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    line = {"metric": "incremental solves/s (FP64 multigrid-PCG, rtol 1e-12)",
+            "value": 1e3 / ms, "unit": "solves/s", "ms_per_solve": ms,
+            "iterations": solver.last.iterations, "relres": solver.last.relres,
+            "steps": a.steps, "warmup": a.warmup,
+            "config": {"workload": "Q2 hex %d^3 Jacobian solve at the benchmark field" % a.n,
+                       "dofs": mesh.ndof},
+            "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -742,6 +786,8 @@ def main():
         run_precision(a)
     elif a.config == "differentiation":
         run_differentiation(a)
+    elif a.config == "solve":
+        run_solve(a)
     else:
         run_ours(a)
 
