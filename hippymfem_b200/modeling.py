@@ -20,11 +20,36 @@ from ._lib import check, lib, ptr, stream_ptr
 from .problem import ADJOINT, PARAMETER, STATE
 
 
-def device_observation_operator(mesh, points):
+def targets_in_box(mesh, points):
+    """Mask of the targets inside the box: the test ``hm_lattice_observation`` applies,
+    ``-1e-12 <= x / h <= n + 1e-12`` on every axis (the same IEEE division), finite."""
+    pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+    s = pts / np.asarray(mesh.h, dtype=np.float64)
+    n = np.asarray(mesh.n, dtype=np.float64)
+    return np.all((s >= -1e-12) & (s <= n + 1e-12), axis=1)
+
+
+def device_observation_operator(mesh, points, missing="raise"):
     """``B`` on the device (``hm_lattice_observation``): row ``o`` holds the 27 Q2 basis
-    values at ``points[o]`` in the element containing it (pointwiseObservation.py:94-170).
-    Points outside the box raise ``ValueError``, as the reference's ``missing="raise"``."""
+    values at the o-th target in the element containing it (pointwiseObservation.py:94-170).
+    Targets outside the box follow the reference's ``missing`` policy (:53-57, :104-112):
+    ``"raise"`` raises ``ValueError``; ``"warn"`` prints a warning and ``"ignore"`` says
+    nothing, and both leave those targets out (``B`` has a row per target inside, in
+    target order; their indices are ``B.owned_targets``)."""
+    if missing not in ("raise", "warn", "ignore"):
+        raise ValueError("missing must be 'raise', 'warn' or 'ignore', got %r" % (missing,))
     pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+    inside = targets_in_box(mesh, pts)
+    owned = np.nonzero(inside)[0]
+    if owned.size < pts.shape[0]:
+        bad = pts[~inside]
+        msg = ("%d observation target(s) are outside the mesh, e.g. %s"
+               % (bad.shape[0], bad[:3].tolist()))
+        if missing == "raise":
+            raise ValueError(msg)
+        if missing == "warn":
+            print("warning: " + msg, flush=True)
+        pts = np.ascontiguousarray(pts[owned])
     npts = pts.shape[0]
     dev = mesh.device
     P = torch.as_tensor(pts, device=dev)
@@ -35,18 +60,18 @@ def device_observation_operator(mesh, points):
                        device=dev)
     rc = lib.hm_lattice_observation(mesh.handle, ptr(P), npts, ptr(indptr), ptr(indices),
                                     ptr(values), ptr(work), stream_ptr())
-    if rc == _lib.HM_ERR_RANGE:
-        bad = ~np.all(np.isfinite(pts) & (pts >= 0.0) & (pts <= np.asarray(mesh.L)), axis=1)
-        raise ValueError("%d observation target(s) are outside the mesh, e.g. %s"
-                         % (int(bad.sum()), pts[bad][:3].tolist()))
+    if rc == _lib.HM_ERR_RANGE:   # targets_in_box applies the kernel's own test
+        raise ValueError("observation targets outside the mesh")
     check(rc, "hm_lattice_observation")
-    return DeviceCSR.from_device(indptr, indices[:27 * npts], values[:27 * npts],
-                                 (npts, mesh.ndof))
+    B = DeviceCSR.from_device(indptr, indices[:27 * npts], values[:27 * npts],
+                              (npts, mesh.ndof))
+    B.owned_targets = owned
+    return B
 
 
-def observation_operator(mesh, points):
-    """Host (scipy) copy of ``device_observation_operator(mesh, points)``."""
-    return device_observation_operator(mesh, points).to_scipy()
+def observation_operator(mesh, points, missing="raise"):
+    """Host (scipy) copy of ``device_observation_operator(mesh, points, missing)``."""
+    return device_observation_operator(mesh, points, missing).to_scipy()
 
 
 class DeviceCSR:
@@ -157,11 +182,12 @@ class DiscreteStateObservation:
         return out
 
 
-def PointwiseStateObservation(Vh, obs_points, data=None, noise_variance=None):
-    """Misfit for pointwise observations of the state at ``obs_points``."""
+def PointwiseStateObservation(Vh, obs_points, data=None, noise_variance=None, missing="raise"):
+    """Misfit for pointwise observations of the state at ``obs_points`` (``data`` per
+    target inside the mesh; ``missing`` as for ``device_observation_operator``)."""
     mesh = Vh.mesh
-    return DiscreteStateObservation(device_observation_operator(mesh, obs_points), data,
-                                    noise_variance, device=mesh.device)
+    return DiscreteStateObservation(device_observation_operator(mesh, obs_points, missing),
+                                    data, noise_variance, device=mesh.device)
 
 
 class _BlockSolver:

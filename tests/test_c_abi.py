@@ -94,3 +94,18 @@ def test_ops_refuse_host_tensors():
 
     with pytest.raises(ValueError):
         ptr(torch.zeros(4, dtype=torch.float64))
+
+
+def test_observation_box_test_matches_the_kernel_rule():
+    """targets_in_box (host) applies -1e-12 <= x / h <= n + 1e-12 per axis, finite: the
+    targets it keeps are the ones hm_lattice_observation accepts."""
+    from types import SimpleNamespace
+
+    from hippymfem_b200.modeling import targets_in_box
+
+    mesh = SimpleNamespace(h=(0.25, 0.7 / 3, 1.3 / 5), n=(4, 3, 5))
+    pts = np.array([[0.0, 0.0, 0.0], [1.0, 0.7, 1.3], [1.0 + 1e-14, 0.1, 0.1],
+                    [1.0 + 1e-9, 0.1, 0.1], [-1e-9, 0.1, 0.1], [0.5, np.nan, 0.5],
+                    [0.5, np.inf, 0.5], [0.3, 0.3, 0.3]])
+    assert targets_in_box(mesh, pts).tolist() == [True, True, True, False, False, False,
+                                                 False, True]

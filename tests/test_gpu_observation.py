@@ -101,3 +101,29 @@ def test_misfit_gradient_uses_the_transpose(cuda):
     Bh = q2.observation_matrix(q2.Lattice((8, 7, 6)), pts)
     ref = Bh.T @ (Bh @ u.cpu().numpy() - d) / 0.04
     assert np.abs(g.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("missing", ["warn", "ignore"])
+def test_targets_outside_are_left_out_on_request(cuda, capsys, missing):
+    """missing="warn"/"ignore": B has a row per target inside the box, in target order
+    (pointwiseObservation.py:104-112); "warn" prints the reference's message."""
+    from hippymfem_b200 import BoxMesh, PointwiseStateObservation, Q2Space, device_observation_operator
+
+    mesh = BoxMesh((4, 3, 5), (1.0, 0.7, 1.3))
+    rng = np.random.default_rng(8)
+    pts = rng.random((40, 3)) * np.array([1.0, 0.7, 1.3])
+    pts[[3, 17, 30]] = [[1.5, 0.1, 0.1], [0.2, -0.1, 0.3], [np.nan, 0.2, 0.2]]
+    B = device_observation_operator(mesh, pts, missing=missing)
+    keep = np.setdiff1d(np.arange(40), [3, 17, 30])
+    assert np.array_equal(B.owned_targets, keep)
+    ref = device_observation_operator(mesh, pts[keep])
+    assert B.shape == (37, mesh.ndof)
+    assert np.array_equal(B.indices.cpu().numpy(), ref.indices.cpu().numpy())
+    assert np.array_equal(B.values.cpu().numpy(), ref.values.cpu().numpy())
+    out = capsys.readouterr().out
+    assert ("3 observation target(s) are outside the mesh" in out) == (missing == "warn")
+    mis = PointwiseStateObservation(Q2Space(mesh), pts, data=np.zeros(37), noise_variance=1.0,
+                                    missing=missing)
+    assert mis.B.shape == (37, mesh.ndof)
+    with pytest.raises(ValueError, match="missing must be"):
+        device_observation_operator(mesh, pts, missing="drop")
