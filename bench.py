@@ -9,13 +9,14 @@ adjoint A^T = A, C = dr/dm, W_um, W_mm) with the assembled vectors (residual, dR
 dR/du) into the diagonal-first CSR pattern, eliminated on the boundary.  ``value`` is
 Q2 elements assembled per second (whole job), device-timed with inputs resident.
 After the timed steps, Hessian actions (misfit 4096 pointwise observations, two
-matrix-free Jacobi-PCG solves at rtol 1e-12 each) are timed for H-applies/s and their
-p50/p99 latency.  ``e2e`` repeats the step through the public API with the fields copied
+matrix-free solves at rtol 1e-12 each: multigrid-PCG as the headline, Jacobi-PCG and
+mixed-precision Jacobi-PCG beside it) are timed for H-applies/s and their p50/p99
+latency.  ``e2e`` repeats the step through the public API with the fields copied
 from pinned host memory and the gradient dR/dm copied back, inside the timed region.
 
 Under torchrun (N > 1) every rank runs an independent replica of the workload (the
 path does not shard: one GPU per request stream); value = all ranks' elements / the
-slowest rank's time.  ``--impl reference`` times the reference's algorithm on the host
+slowest rank's time (every timing is the maximum over the ranks).  ``--impl reference`` times the reference's algorithm on the host
 cores instead (element blocks by forward-over-reverse AD in 2048-element windows and a
 bincount scatter, restated in oracle/; rank 0 only).
 """
@@ -60,6 +61,26 @@ def parse():
                          "checks of the autograd wrappers; solve: one incremental solve "
                          "(FP64 multigrid-PCG, rtol 1e-12) at --n, repeated")
     return ap.parse_args()
+
+
+# ------------------------------------------------------------------------ ranks
+def max_over_ranks(values, world, dev=None):
+    """Each value's maximum over the ranks (every rank calls this with the same number
+    of values, at the same point); the values themselves on one rank."""
+    vals = [float(v) for v in values]
+    if world == 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def whole_job_rate(units_per_rank, ms, world):
+    """Units per second of the whole job: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / (ms / 1000.0)
 
 
 # ------------------------------------------------------------------------ clocks
@@ -308,6 +329,7 @@ def run_ours(a):
     import hippymfem_b200 as hm
     from hippymfem_b200 import _lib
     from hippymfem_b200._lib import check, lib, ptr, stream_ptr
+    from hippymfem_b200.sparse import default_smoothing_degree
     from hippymfem_b200.synthetic import interior_points, log_conductivity, normal_vector
 
     dev = torch.device("cuda", local)
@@ -361,12 +383,9 @@ def run_ours(a):
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
     k_ms = statistics.mean(ev_k0[i].elapsed_time(ev_k1[i]) for i in range(a.steps))
-    if world > 1:
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms, k_ms = max_over_ranks([ms, k_ms], world, dev)
     assert int(status.item()) == 0, "non-finite values in the benchmark fields"
-    value = world * ne * a.steps / (ms / 1000.0)
+    value = whole_job_rate(ne * a.steps, ms, world)
 
     # roofline of the fused assembly kernel: bytes it must move per launch
     alg_bytes = 8 * nnz * 4 + 8 * nd * 3 + 8 * 216 * ne + 4 * (nd + 1) + nd
@@ -404,11 +423,8 @@ def run_ours(a):
     e1.record(stream)
     torch.cuda.synchronize()
     e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e_ms = float(tt.item())
-    e2e_value = world * ne * e_steps / (e_ms / 1000.0)
+    (e_ms,) = max_over_ranks([e_ms], world, dev)
+    e2e_value = whole_job_rate(ne * e_steps, e_ms, world)
     del prob
     torch.cuda.empty_cache()
 
@@ -502,6 +518,13 @@ def run_ours(a):
     del H, model, prob
     torch.cuda.empty_cache()
 
+    # the latency figures of the three solvers: each the maximum over the ranks
+    def lat_stats(ls):
+        return [statistics.mean(ls), float(np.percentile(ls, 50)), float(np.percentile(ls, 99))]
+
+    hs_mg, hs_j, hs_32 = (max_over_ranks(lat_stats(ls), world, dev) for ls in (lat_mg, lat, lat32))
+    mg_degree = default_smoothing_degree(mesh)
+
     serving = None
     if a.serving > 0 and world == 1:
         serving = run_serving(a.serving, dev)
@@ -521,7 +544,7 @@ def run_ours(a):
                        "elements": ne, "dofs": nd, "nnz_per_block": nnz,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs and outputs larger than L2 (4.3 GB written per step)"},
-            "dofs_per_s": world * nd * a.steps / (ms / 1000.0),
+            "dofs_per_s": whole_job_rate(nd * a.steps, ms, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": alg_bytes * TRAFFIC_PER_ALG_BYTE,
@@ -532,34 +555,31 @@ def run_ours(a):
                          "alg_bytes_per_launch": alg_bytes,
                          "step_alg_bytes": step_bytes,
                          "step_frac": step_bytes / (ms / a.steps / 1000.0) / 1e9 / peak},
-            "h_applies_per_s": world * 1000.0 / statistics.mean(lat_mg),
-            "latency_ms": {"p50": float(np.percentile(lat_mg, 50)),
-                           "p99": float(np.percentile(lat_mg, 99)),
+            "h_applies_per_s": whole_job_rate(1, hs_mg[0], world),
+            "latency_ms": {"p50": hs_mg[1], "p99": hs_mg[2],
                            "what": "one Hessian action (2 matrix-free FP64 solves, PCG with the "
                                    "lattice multigrid V-cycle, rtol 1e-12)"},
             "pcg_iterations": iters_mg,
-            "jacobi_fp64": {"h_applies_per_s": world * 1000.0 / statistics.mean(lat),
-                            "latency_ms": {"p50": float(np.percentile(lat, 50)),
-                                           "p99": float(np.percentile(lat, 99))},
+            "jacobi_fp64": {"h_applies_per_s": whole_job_rate(1, hs_j[0], world),
+                            "latency_ms": {"p50": hs_j[1], "p99": hs_j[2]},
                             "pcg_iterations": iters,
                             "what": "the same action with Jacobi-PCG (FP64, rtol 1e-12)"},
-            "mixed": {"h_applies_per_s": world * 1000.0 / statistics.mean(lat32),
-                      "latency_ms": {"p50": float(np.percentile(lat32, 50)),
-                                     "p99": float(np.percentile(lat32, 99))},
+            "mixed": {"h_applies_per_s": whole_job_rate(1, hs_32[0], world),
+                      "latency_ms": {"p50": hs_32[1], "p99": hs_32[2]},
                       "rel_err_vs_fp64": mixed_err,
-                      "speedup_vs_fp64_jacobi": statistics.mean(lat) / statistics.mean(lat32),
+                      "speedup_vs_fp64_jacobi": hs_j[0] / hs_32[0],
                       "pcg_iterations": iters32,
                       "what": "Jacobi-PCG with the recurrence in FP32, reliable updates to the "
                               "FP64 true residual (delta 0.1), rtol 1e-12"},
-            "multigrid": {"h_applies_per_s": world * 1000.0 / statistics.mean(lat_mg),
-                          "latency_ms": {"p50": float(np.percentile(lat_mg, 50)),
-                                         "p99": float(np.percentile(lat_mg, 99))},
+            "multigrid": {"h_applies_per_s": whole_job_rate(1, hs_mg[0], world),
+                          "latency_ms": {"p50": hs_mg[1], "p99": hs_mg[2]},
                           "rel_err_vs_jacobi": mg_err,
-                          "speedup_vs_fp64_jacobi": statistics.mean(lat) / statistics.mean(lat_mg),
+                          "speedup_vs_fp64_jacobi": hs_j[0] / hs_mg[0],
                           "pcg_iterations": iters_mg,
                           "what": "FP64 PCG preconditioned by the lattice multigrid V-cycle "
-                                  "(Q2 -> Q1 -> coarser Q1, Chebyshev-Jacobi degree 2), "
-                                  "rtol 1e-12"},
+                                  "(Q2 -> Q1 -> coarser Q1, Chebyshev-Jacobi degree %d, the coarsest "
+                                  "level solved exactly when it has at most 64 interior "
+                                  "nodes), rtol 1e-12" % mg_degree},
             "e2e": {"value": e2e_value, "unit": "elements/s",
                     "h2d_bytes_per_step": 3 * 8 * nd, "d2h_bytes_per_step": 8 * nd,
                     "steps": e_steps},
