@@ -274,9 +274,10 @@ int hm_mg_setup(hm_mg* mg, void* d_jac64, const uint8_t* d_ess, const double* d_
                 void* stream);
 int hm_mg_apply(hm_mg* mg, const double* d_r, double* d_z, void* stream);
 int hm_mg_levels(const hm_mg* mg);
-/* The Q1 levels with at most max_nodes nodes (5000 by default; 0: none) run as one
+/* The Q1 levels with at most max_nodes nodes (1000 by default; 0: none) run as one
  * CTA-wide kernel per cycle instead of level by level (the same arithmetic, node for
- * node; a few launches instead of ~14 per level and 2 per coarse-solve step). */
+ * node; one launch instead of ~14 per level).  Set it before a plan's first solve: a
+ * plan's captured iteration batches keep the launches they were captured with. */
 int hm_mg_set_tail_nodes(hm_mg* mg, int64_t max_nodes);
 int hm_mg_destroy(hm_mg* mg);
 int hm_pcg_mg(hm_mg* mg, const double* d_b, double* d_x, double rtol, int maxiter,
