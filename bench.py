@@ -391,7 +391,7 @@ def run_ours(a):
     alg_bytes = 8 * nnz * 4 + 8 * nd * 3 + 8 * 216 * ne + 4 * (nd + 1) + nd
     peak, peak_kind = peaks()
     achieved = alg_bytes / (k_ms / 1000.0) / 1e9
-    step_bytes = 8 * nnz * 4 + 8 * nd * 5            # survey's B_asm without the slot map
+    step_bytes = 8 * nnz * 4 + 8 * nd * 5            # 4 blocks, 3 fields in, 2 vectors out
 
     # ------------------------------------------------------------ e2e (public API)
     pin = [torch.empty(nd, dtype=torch.float64).pin_memory() for _ in range(3)]
