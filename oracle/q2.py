@@ -21,6 +21,11 @@ What each function follows in the reference (paths relative to the hIPPyMFEM tre
   fields from ``_eval_field`` (``kernel.py:378-394``), vectors as ``grad_block``
   (``kernel.py:1343-1355``); rows are the test slot and columns the trial slot
   (``kernel.py:1704-1710``).
+* :func:`element_blocks_fp32`, :func:`consistent_blocks` — the single-precision element
+  matrices of ``PRECISION="mixed"`` (``kernel.py:61-99, 1001-1007``) and
+  ``consistent_block`` (``kernel.py:1503-1571``): the single-precision block corrected by
+  one rank-one term per side so that its products with the constants are the
+  double-precision ones (``symmetric``: symmetrized first, symmetric to the last bit).
 * :func:`build_tables` — ``hippymfem/fem/patternbuild.py:209-253`` (the arrays of the
   sort route ``hippymfem/fem/pattern.py:548-663``): CSR over rows, diagonal first on a
   square shape, then ascending columns; ``slot[(e*ndt+a)*ndr+b]`` the CSR position of
@@ -172,6 +177,73 @@ def element_blocks(mesh, edofs, u, m, p, which=("A", "C", "Wum", "Wmm")):
         s = D * np.einsum("eqk,eqk->eq", gu, gp)
         X = s[:, :, None] * N[None]
         out["Wmm"] = np.matmul(X.transpose(0, 2, 1), N[None])
+    return out
+
+
+def element_blocks_fp32(mesh, edofs, u, m, p, which=("A", "C", "Wum", "Wmm")):
+    """The element matrices of :func:`element_blocks` with the element contractions in
+    single precision (weights, field gradients and tables rounded to float32, products
+    and sums in float32), returned in float64."""
+    N, G, _ = basis_tables()
+    f32 = np.float32
+    N32 = N.astype(f32)
+    Gp = (G / np.asarray(mesh.h)[None, None, :]).astype(f32)
+    D, gu, gp = _weights(mesh, edofs, u, m, p)
+    D, gu, gp = D.astype(f32), gu.astype(f32), gp.astype(f32)
+    out = {}
+    if "A" in which:
+        A = np.zeros((D.shape[0], 27, 27), dtype=f32)
+        for k in range(3):
+            X = D[:, :, None] * Gp[None, :, :, k]
+            A = A + np.matmul(X.transpose(0, 2, 1), Gp[None, :, :, k])
+        out["A"] = A
+    for name, g in (("C", gu), ("Wum", gp)):
+        if name in which:
+            R = np.einsum("eq,eqk,qak->eqa", D, g, Gp)
+            out[name] = np.matmul(R.transpose(0, 2, 1), N32[None])
+    if "Wmm" in which:
+        s = D * np.einsum("eqk,eqk->eq", gu, gp)
+        X = s[:, :, None] * N32[None]
+        out["Wmm"] = np.matmul(X.transpose(0, 2, 1), N32[None])
+    return {k: v.astype(np.float64) for k, v in out.items()}
+
+
+SYMMETRIC_BLOCKS = ("A", "Wmm")
+
+
+def consistent_blocks(mesh, edofs, u, m, p, which=("A", "C", "Wum", "Wmm")):
+    """``consistent_block`` (``kernel.py:1503-1571``) for the lattice's Q2 blocks: the
+    single-precision element matrix ``K`` corrected with ``V = 1 / sqrt(27)`` (the
+    normalized constants of a scalar Q2 element, ``_low_modes``) and the
+    double-precision products ``R_j = K64 V^T`` (one tangent) so that ``K' V^T = R_j``
+    and, two-sided, ``K'^T V^T = R_i``.  The symmetric blocks (A, W_mm) are symmetrized
+    first and returned symmetric to the last bit (both triangles from the upper one)."""
+    K32 = element_blocks_fp32(mesh, edofs, u, m, p, which)
+    K64 = element_blocks(mesh, edofs, u, m, p, which)
+    V = np.full((1, 27), 1.0 / np.sqrt(27.0))
+    iu = np.triu_indices(27)
+    out = {}
+    for name in which:
+        K = K32[name]
+        Rj = K64[name] @ V.T                                         # (ne, 27, 1)
+        if name in SYMMETRIC_BLOCKS:
+            K = 0.5 * (K + K.transpose(0, 2, 1))
+            Dj = Rj - K @ V.T
+            U = Dj @ V
+            S = V @ Dj                                               # (ne, 1, 1)
+            W = V.T @ (0.5 * (S + S.transpose(0, 2, 1))) @ V
+            M = K + (U + U.transpose(0, 2, 1)) - 0.5 * (W + W.transpose(0, 2, 1))
+            up = M[:, iu[0], iu[1]]
+            M = np.zeros_like(M)
+            M[:, iu[0], iu[1]] = up
+            M[:, iu[1], iu[0]] = up
+            out[name] = M
+        else:
+            Ri = K64[name].transpose(0, 2, 1) @ V.T
+            Dj = Rj - K @ V.T
+            Di = Ri - K.transpose(0, 2, 1) @ V.T
+            out[name] = (K + Dj @ V + V.T @ Di.transpose(0, 2, 1)
+                         - V.T @ (V @ Dj) @ V)
     return out
 
 

@@ -169,3 +169,33 @@ def test_hessian_action_by_finite_differences():
     h = 1e-5
     fd = (gradient(m0 + h * x)[0] - gradient(m0 - h * x)[0]) / (2 * h)
     assert np.linalg.norm(fd - Hx) <= 1e-6 * np.linalg.norm(Hx)
+
+
+def test_consistent_blocks_are_exact_on_the_constants():
+    """consistent_block (kernel.py:1503-1571) restated: the single-precision element
+    matrices err by ~1e-7; corrected, their products with the constants (and, two-sided,
+    their transposes') equal the double-precision ones to rounding, A and W_mm are
+    symmetric to the last bit, and the entries stay within the single-precision error."""
+    mesh = q2.Lattice((3, 4, 2), (1.0, 0.8, 1.1))
+    E = mesh.edofs()
+    rng = np.random.default_rng(12)
+    u, p = rng.standard_normal(mesh.ndof), rng.standard_normal(mesh.ndof)
+    m = 0.5 * rng.standard_normal(mesh.ndof)
+    K64 = q2.element_blocks(mesh, E, u, m, p)
+    K32 = q2.element_blocks_fp32(mesh, E, u, m, p)
+    Kc = q2.consistent_blocks(mesh, E, u, m, p)
+    one = np.ones(27)
+    for name in ("A", "C", "Wum", "Wmm"):
+        scale = np.abs(K64[name]).max()
+        err32 = np.abs(K32[name] - K64[name]).max() / scale
+        assert 1e-9 < err32 < 1e-5, (name, err32)              # single precision
+        assert np.abs(Kc[name] - K64[name]).max() / scale < 10 * err32
+        d64 = K64[name] @ one
+        assert np.abs(Kc[name] @ one - d64).max() <= 1e-13 * scale, name
+        if name in q2.SYMMETRIC_BLOCKS:
+            assert np.array_equal(Kc[name], Kc[name].transpose(0, 2, 1)), name
+        else:
+            t64 = K64[name].transpose(0, 2, 1) @ one
+            assert np.abs(Kc[name].transpose(0, 2, 1) @ one - t64).max() <= 1e-13 * scale
+        # the uncorrected block's row sums carry its single-precision error
+        assert np.abs(K32[name] @ one - d64).max() > 1e3 * np.abs(Kc[name] @ one - d64).max()
