@@ -14,7 +14,8 @@ stretch of the global ones, with the same columns shifted by a constant node off
 
 ``SlabPartition`` holds the geometry, ``exchange_planes`` the halo exchange over
 ``torch.distributed`` (NCCL for device tensors, gloo for host tensors), and
-``assemble_slab`` runs an assembler on the local lattice and returns the owned stretch.
+``assemble_slab`` runs an assembler on the local lattice and returns the owned stretch,
+``hypre_arrays`` the row pointers and global columns hypre takes with it.
 ``device_slab_assembler`` is the fused CUDA assembler (``hm_lattice_quadrature`` +
 ``hm_lattice_assemble`` on the local lattice)."""
 
@@ -158,6 +159,27 @@ def assemble_slab(part, rank, u, m, p, ess, assembler, f=1.0, group=None):
     s0, s1 = part.owned_global_csr(rank)
     assert s1 - s0 == b - a, "local and global row stretches differ"
     return owned_blocks, owned_vectors, (s0, s1), part.owned_global_rows(rank)
+
+
+def hypre_arrays(part, rank, local_indptr, local_indices):
+    """The arrays the reference hands hypre for rank's rows (``fem/parmat.py:106-171``,
+    ``HypreParMatrix(comm, nrow, rglob, cglob, [I, J, D, rows])``): ``I`` the row
+    pointers of the owned rows from 0 (int32), ``J`` their global column indices (int64:
+    the local lattice's columns shifted by its first node plane), and ``rows`` the
+    partition ``[first row, last row + 1]``; ``D`` is the owned stretch that
+    ``assemble_slab`` returns.  Works on numpy arrays or tensors."""
+    r0, r1 = part.owned_local_rows(rank)
+    l0, _ = part.local_planes(rank)
+    ip = local_indptr[r0:r1 + 1]
+    a, b = int(ip[0]), int(ip[-1])
+    if isinstance(ip, torch.Tensor):
+        I = (ip - a).to(torch.int32)
+        J = local_indices[a:b].to(torch.int64) + l0 * part.plane
+    else:
+        I = (np.asarray(ip, dtype=np.int64) - a).astype(np.int32)
+        J = np.asarray(local_indices[a:b], dtype=np.int64) + l0 * part.plane
+    g0, g1 = part.owned_global_rows(rank)
+    return I, J, np.array([g0, g1], dtype=np.int64)
 
 
 def device_slab_assembler(n, L, u, m, p, ess, f=1.0):

@@ -126,3 +126,27 @@ def test_partition_geometry():
         assert plane_csr_offset(mo.N, k) == indptr[k * plane]
     with pytest.raises(ValueError):
         SlabPartition((2, 2, 3), (1, 1, 1), 4)
+
+
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_hypre_arrays_are_the_global_rows(world):
+    """Each rank's row pointers and global columns (from its local lattice's pattern)
+    are the global pattern's rows, diagonal first as hypre keeps them."""
+    from hippymfem_b200.shard import SlabPartition, hypre_arrays
+
+    n, L = (4, 3, 8), (1.0, 0.6, 1.1)
+    part = SlabPartition(n, L, world)
+    mo = q2.Lattice(n, L)
+    E = mo.edofs()
+    gptr, gind = q2.build_tables(E, E, mo.ndof, mo.ndof, True)[:2]
+    for r in range(world):
+        nl, Ll = part.local_box(r)
+        ml = q2.Lattice(nl, Ll)
+        El = ml.edofs()
+        lptr, lind = q2.build_tables(El, El, ml.ndof, ml.ndof, True)[:2]
+        I, J, rows = hypre_arrays(part, r, lptr, lind)
+        g0, g1 = rows
+        assert I.dtype == np.int32 and J.dtype == np.int64
+        assert np.array_equal(I, gptr[g0:g1 + 1] - gptr[g0])
+        assert np.array_equal(J, gind[gptr[g0]:gptr[g1]])
+        assert np.all(J[I[:-1]] == np.arange(g0, g1))          # diagonal first
