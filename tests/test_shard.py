@@ -150,3 +150,19 @@ def test_hypre_arrays_are_the_global_rows(world):
         assert np.array_equal(I, gptr[g0:g1 + 1] - gptr[g0])
         assert np.array_equal(J, gind[gptr[g0]:gptr[g1]])
         assert np.all(J[I[:-1]] == np.arange(g0, g1))          # diagonal first
+
+
+def test_hypre_arrays_from_tensors_match_numpy():
+    from hippymfem_b200.shard import SlabPartition, hypre_arrays
+
+    n, L = (3, 3, 6), (1.0, 1.0, 1.0)
+    part = SlabPartition(n, L, 3)
+    nl, Ll = part.local_box(1)
+    ml = q2.Lattice(nl, Ll)
+    El = ml.edofs()
+    lptr, lind = q2.build_tables(El, El, ml.ndof, ml.ndof, True)[:2]
+    In, Jn, rn = hypre_arrays(part, 1, lptr, lind)
+    It, Jt, rt = hypre_arrays(part, 1, torch.as_tensor(lptr), torch.as_tensor(lind))
+    assert It.dtype == torch.int32 and Jt.dtype == torch.int64
+    assert np.array_equal(It.numpy(), In) and np.array_equal(Jt.numpy(), Jn)
+    assert np.array_equal(rt, rn)
