@@ -38,8 +38,8 @@ if ROOT not in sys.path:
 
 METRIC = "Q2 elems/s, H-applies/s at 64^3 vs plain FP64; p50/p99 batched-solve latency"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM bytes per algorithmic byte of k_tile_assemble<double>, from one ncu capture at 48^3
-# (profiles/k_tile_assemble_48cube.md)
+# DRAM bytes per algorithmic byte of k_tile_assemble<double>, from one ncu capture of the
+# kernel at 48^3 (dram__bytes_read.sum + dram__bytes_write.sum over the bytes it must move)
 TRAFFIC_PER_ALG_BYTE = 2030.9 / 2043.7
 
 

@@ -3,7 +3,7 @@
 Run in a container that holds the hIPPyMFEM source tree (it is not needed anywhere
 else; the fixtures it writes are committed):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the hIPPyMFEM source tree>
 
 It loads ``hippymfem/fem/_patternkernels.py`` by file path (numba + numpy only; the rest
 of the package needs MFEM/JAX/MPI, which are absent) and drives its three table passes
@@ -114,4 +114,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the hIPPyMFEM source tree>")
+    main(sys.argv[1])
