@@ -154,9 +154,10 @@ def peaks():
 
 
 # ------------------------------------------------------------------ CPU baselines
-def cpu_port_baseline(budget_s=12.0):
-    """The oracle's closed-form assembly of every block (oracle/q2.py) on a 16^3 sample
-    of the per-element work, bincount scatter and elimination included."""
+def cpu_port_baseline(budget_s=12.0, n_sample=32):
+    """The oracle's closed-form assembly of every block (oracle/q2.py) on a 32^3 sample
+    of the per-element work (a working set well beyond the host caches, as the 64^3 one
+    is), bincount scatter and elimination included."""
     from oracle import q2
 
     try:
@@ -164,7 +165,7 @@ def cpu_port_baseline(budget_s=12.0):
         cores = max([i.get("num_threads", 1) for i in threadpool_info()] + [1])
     except Exception:                                     # noqa: BLE001
         cores = os.cpu_count() or 1
-    mesh = q2.Lattice(16)
+    mesh = q2.Lattice(n_sample)
     E = mesh.edofs()
     rng = np.random.default_rng(0)
     u, m, p = (rng.standard_normal(mesh.ndof) for _ in range(3))
@@ -180,13 +181,15 @@ def cpu_port_baseline(budget_s=12.0):
         done += mesh.ne
     dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": "elements/s", "cores": int(cores), "kind": "port",
-            "sample": "oracle closed-form assembly of A, C, Wum, Wmm + vectors on 16^3 "
-                      "(4096 elements) repeated for %.1f s" % dt}
+            "sample": "oracle closed-form assembly of A, C, Wum, Wmm + vectors on %d^3 "
+                      "(%d elements) repeated for %.1f s" % (n_sample, mesh.ne, dt)}
 
 
-def reference_step_fn(n_sample=16):
-    """One step of the reference's host algorithm on a 16^3 sample: blocks by AD in
-    2048-element windows (oracle/ad.py) + bincount scatter + folded elimination."""
+def reference_step_fn(n_sample=32):
+    """One step of the reference's host algorithm on a 32^3 sample of the 64^3 workload
+    (32,768 elements, 16.97 M entries per block: a working set beyond the host caches,
+    as the full size is): blocks by AD in 2048-element windows (oracle/ad.py) + bincount
+    scatter + folded elimination."""
     from oracle import ad, q2
 
     mesh = q2.Lattice(n_sample)
@@ -228,10 +231,10 @@ def run_reference(a):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "Q2 hex linearization-point assembly (A, C, Wum, Wmm + "
                                    "vectors), reference algorithm on the host",
-                       "mesh": "16^3 sample of the 64^3 per-element work", "precision": "fp64"},
+                       "mesh": "32^3 sample of the 64^3 per-element work", "precision": "fp64"},
             "cpu_baseline": {"value": v, "unit": "elements/s", "cores": torch.get_num_threads(),
                              "kind": "port",
-                             "sample": "16^3 (4096 elements) per step: torch.func "
+                             "sample": "32^3 (32768 elements) per step: torch.func "
                                        "forward-over-reverse AD in 2048-element windows "
                                        "+ bincount scatter + elimination"},
             "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0,

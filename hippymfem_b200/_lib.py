@@ -79,9 +79,21 @@ SIGNATURES = {
     "hm_mg_apply": (_i32, [_p, _p, _p, _p]),
     "hm_mg_levels": (_i32, [_p]),
     "hm_mg_set_tail_nodes": (_i32, [_p, _i64]),
+    "hm_mg_set_fused": (_i32, [_p, _i32]),
     "hm_mg_destroy": (_i32, [_p]),
     "hm_pcg_mg": (_i32, [_p, _p, _p, _d, _i32, _i32, _p, _p, _p, _p]),
     "hm_pcg_plan_set_mg": (_i32, [_p, _p]),
+    "hm_lattice_dof_permutation": (_i32, [_p, _p, _p, _p]),
+    "hm_lattice_caller_map": (_i32, [_p, _p, _p, _p, _p, _p, _p]),
+    "hm_gather_f64": (_i32, [_i64, _p, _p, _p, _p]),
+    "hm_lattice_element_blocks": (_i32, [_p, _p, _i32, _i64, _i64, _p, _p, _p, _p, _p, _p]),
+    "hm_hessian_workspace_bytes": (_i64, [_i64, _i64]),
+    "hm_hessian_create": (_i32, [_p, _p, _p, _p, _p, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _d,
+                                 _p, _p, _p, _p]),
+    "hm_hessian_apply": (_i32, [_p, _p, _p, _d, _i32, _p, _p]),
+    "hm_hessian_destroy": (_i32, [_p]),
+    "hm_lattice_consistent_workspace_bytes": (_i64, [_p]),
+    "hm_lattice_assemble_consistent": (_i32, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "hm_dot_workspace_bytes": (_i64, [_i64]),
     "hm_dot": (_i32, [_i64, _p, _p, _p, _p, _p]),
 }

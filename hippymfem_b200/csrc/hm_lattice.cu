@@ -228,11 +228,14 @@ __device__ __forceinline__ real dbq_rt(int q, int a) {
 }
 
 // ESS: zero x on the Dirichlet nodes on the fly (callers whose x is already zero there
-// -- every vector inside the lattice solves -- skip the markers)
-template <typename real, typename vec, bool ESS = true>
+// -- every vector inside the lattice solves -- skip the markers).  CHEB: the input is the
+// first Chebyshev direction d = b / (theta diag) of a smoother started from zero,
+// formed on the fly from b (xin), the Jacobi diagonal and theta = cheb[0].
+template <typename real, typename vec, bool ESS = true, bool CHEB = false>
 __global__ void __launch_bounds__(256, 2)
     k_elem_apply(Lattice L, const real* __restrict__ Dq, const uint8_t* __restrict__ ess,
-                 const vec* __restrict__ xin, real* __restrict__ Ye) {
+                 const vec* __restrict__ xin, real* __restrict__ Ye,
+                 const double* __restrict__ cdiag = nullptr, const double* __restrict__ cheb = nullptr) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int k = lane / 3, t = lane - 3 * k;                 // element slot, Gauss slice
@@ -245,6 +248,7 @@ __global__ void __launch_bounds__(256, 2)
   const int ez = (int)(exy / (unsigned)L.ny), ey = (int)(exy - (unsigned)ez * (unsigned)L.ny);
   const unsigned n0 = (unsigned)(2 * ex) + (unsigned)L.Nx * ((unsigned)(2 * ey) + (unsigned)L.Ny * (unsigned)(2 * ez));
   const unsigned nsy = (unsigned)L.Nx, nsz = (unsigned)L.Nx * (unsigned)L.Ny;
+  const double inv_theta = CHEB ? 1.0 / __ldg(cheb) : 0.0;
   // z interpolation onto slice t, one node plane a3 at a time: Xb[a2][a1], Xd[a2][a1]
   real Xb[9], Xd[9];
 #pragma unroll
@@ -253,7 +257,11 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       const unsigned n = n0 + (unsigned)(i % 3) + nsy * (unsigned)(i / 3) + nsz * (unsigned)a3;
-      const real xv = live ? (real)__ldg(xin + n) : (real)0;
+      real xv = (real)0;
+      if (live) {
+        if constexpr (CHEB) xv = (real)(inv_theta * (double)__ldg(xin + n) / __ldg(cdiag + n));
+        else xv = (real)__ldg(xin + n);
+      }
       const bool fixed = ESS && ess != nullptr && live && __ldg(ess + n) != 0;
       const real x = fixed ? (real)0 : xv;
       Xb[i] = a3 == 0 ? b3 * x : fma(b3, x, Xb[i]);
@@ -343,12 +351,26 @@ __device__ __forceinline__ void axis_elems(int i, int nel, int& e0, int& a0, int
   else { e0 = (i >> 1) - 1; a0 = 2; cnt = 2; }   // elements i/2-1 (a=2), i/2 (a=0)
 }
 
-template <typename real, typename vec>
+// OUT selects what is written for each node's product y (FP64 only for OUT != 0), with
+// c.b the smoother's right-hand side, c.diag the Jacobi diagonal, theta = c.cheb[0]:
+//   0  yout = y
+//   1  the first smoothing step from zero (the input was d = b / (theta diag)):
+//      c.r = b - y, c.x = d
+//   2  one smoothing step from c.x (the input): c.x += (b - y) / (theta diag), in place
+//      (this pass reads no x but the Dirichlet nodes' own)
+struct ChebOut {
+  const double* b;
+  const double* diag;
+  const double* cheb;
+  double* r;
+  double* x;
+};
+template <typename real, typename vec, int OUT = 0>
 __global__ void __launch_bounds__(256)
     k_node_gather(Lattice L, const real* __restrict__ Ye, const uint8_t* __restrict__ ess,
                   const vec* __restrict__ xin, vec* __restrict__ yout,
                   const vec* __restrict__ dotw, double* __restrict__ part,
-                  double* __restrict__ sc, unsigned* __restrict__ counter) {
+                  double* __restrict__ sc, unsigned* __restrict__ counter, ChebOut c = {}) {
   const unsigned per_row = (unsigned)L.nx + 1u;                  // pairs + the last node
   const unsigned rows = (unsigned)L.Ny * (unsigned)L.Nz;
   const unsigned task = blockIdx.x * blockDim.x + threadIdx.x;
@@ -378,13 +400,35 @@ __global__ void __launch_bounds__(256)
           acc1 += Ye[(size_t)(1u + a23) * ne + erow + m];
         }
       }
-    const double y0 = f0 ? (double)xin[n0] : (double)acc0;
-    yout[n0] = (vec)y0;
-    if (dotw) dot = (double)dotw[n0] * y0;
-    if (!last) {
-      const double y1 = f1 ? (double)xin[n0 + 1] : (double)acc1;
-      yout[n0 + 1] = (vec)y1;
-      if (dotw) dot = fma((double)dotw[n0 + 1], y1, dot);
+    if constexpr (OUT == 0) {
+      const double y0 = f0 ? (double)xin[n0] : (double)acc0;
+      yout[n0] = (vec)y0;
+      if (dotw) dot = (double)dotw[n0] * y0;
+      if (!last) {
+        const double y1 = f1 ? (double)xin[n0 + 1] : (double)acc1;
+        yout[n0 + 1] = (vec)y1;
+        if (dotw) dot = fma((double)dotw[n0 + 1], y1, dot);
+      }
+    } else {
+      const double inv_theta = 1.0 / c.cheb[0];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && last) break;
+        const unsigned nn = n0 + (unsigned)h;
+        const bool fx = h ? f1 : f0;
+        const double acc = (double)(h ? acc1 : acc0);
+        const double bn = c.b[nn];
+        if constexpr (OUT == 1) {
+          const double d = inv_theta * bn / c.diag[nn];
+          const double y = fx ? d : acc;
+          c.r[nn] = bn - y;
+          c.x[nn] = d;
+        } else {
+          const double xn = c.x[nn];
+          const double y = fx ? xn : acc;
+          c.x[nn] = xn + inv_theta * (bn - y) / c.diag[nn];
+        }
+      }
     }
   }
   if (part != nullptr) {
@@ -510,6 +554,36 @@ static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const
     k_elem_apply<real, vec, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
   k_node_gather<real, vec><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, x, y, dotw, part, part != nullptr ? sc : nullptr, counter);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+// One Chebyshev-Jacobi smoothing step of degree 1 on the lattice operator (FP64, every
+// vector zero on the Dirichlet nodes), the operator pass and the vector update fused:
+//   from zero:  x = d = b / (theta diag),  r = b - A d          (pre-smoothing)
+//   from x:     x += (b - A x) / (theta diag)                   (post-smoothing)
+// the same arithmetic as the start / step / finish kernels of the multigrid smoother.
+int hm_launch_cheb1_from_zero(const Lattice& L, void* jac, const uint8_t* ess, const double* b,
+                              const double* diag, const double* cheb, double* x, double* r,
+                              void* stream) {
+  double* Dq = static_cast<double*>(jac);
+  double* Ye = Dq + L.ne * 27;
+  const int64_t warps = (L.ne + 9) / 10;
+  k_elem_apply<double, double, false, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(
+      L, Dq, ess, b, Ye, diag, cheb);
+  ChebOut c{b, diag, cheb, r, x};
+  k_node_gather<double, double, 1><<<gather_blocks(L), 256, 0, S_(stream)>>>(
+      L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+int hm_launch_cheb1_from_x(const Lattice& L, void* jac, const uint8_t* ess, const double* b,
+                           const double* diag, const double* cheb, double* x, void* stream) {
+  double* Dq = static_cast<double*>(jac);
+  double* Ye = Dq + L.ne * 27;
+  const int64_t warps = (L.ne + 9) / 10;
+  k_elem_apply<double, double, false><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
+  ChebOut c{b, diag, cheb, nullptr, x};
+  k_node_gather<double, double, 2><<<gather_blocks(L), 256, 0, S_(stream)>>>(
+      L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 

@@ -54,6 +54,7 @@ struct hm_mg {
   double* scratch;       // partial sums of the set-up's inner products, eigenvalue state
   const uint8_t* checked_ess;   // the markers last found to be the whole boundary
   int tail_first;        // first level of the one-CTA tail (nlev: none)
+  int fused;             // degree-1 smoothing steps fused with their operator pass
 };
 
 namespace hm {
@@ -65,13 +66,13 @@ __device__ __forceinline__ bool on_boundary(int i, int j, int k, int Nx, int Ny,
 }
 
 // (A_l x)[n] for a Q1 level: node-centric, identity on the boundary, boundary values of
-// x taken as zero in the interior rows
-__device__ __forceinline__ double q1_apply_at(const MGLevel& lv, const double* __restrict__ x,
-                                              int64_t n) {
+// x taken as zero in the interior rows; x given by xv(node)
+template <typename XV>
+__device__ __forceinline__ double q1_apply_with(const MGLevel& lv, int64_t n, XV xv) {
   const int i = (int)(n % lv.Nx);
   const int64_t t = n / lv.Nx;
   const int j = (int)(t % lv.Ny), k = (int)(t / lv.Ny);
-  if (on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz)) return x[n];
+  if (on_boundary(i, j, k, lv.Nx, lv.Ny, lv.Nz)) return xv(n);
   // 1D element matrices: k = [1 -1; -1 1] / h, m = [2 1; 1 2] h / 6
   const double kx[2] = {1.0 / lv.hx, -1.0 / lv.hx}, ky[2] = {1.0 / lv.hy, -1.0 / lv.hy},
                kz[2] = {1.0 / lv.hz, -1.0 / lv.hz};
@@ -86,7 +87,7 @@ __device__ __forceinline__ double q1_apply_at(const MGLevel& lv, const double* _
       for (int di = 0; di < 3; ++di) {
         const int ii = i + di - 1, jj = j + dj - 1, kk = k + dk - 1;
         xs[dk][dj][di] = on_boundary(ii, jj, kk, lv.Nx, lv.Ny, lv.Nz)
-                             ? 0.0 : x[ii + (int64_t)lv.Nx * (jj + (int64_t)lv.Ny * kk)];
+                             ? 0.0 : xv(ii + (int64_t)lv.Nx * (jj + (int64_t)lv.Ny * kk));
       }
   double acc = 0.0;
 #pragma unroll
@@ -113,6 +114,32 @@ __device__ __forceinline__ double q1_apply_at(const MGLevel& lv, const double* _
         acc = fma(c, s, acc);
       }
   return acc;
+}
+__device__ __forceinline__ double q1_apply_at(const MGLevel& lv, const double* __restrict__ x,
+                                              int64_t n) {
+  return q1_apply_with(lv, n, [&](int64_t m) { return x[m]; });
+}
+// A Chebyshev-Jacobi step of degree 1 of a Q1 level with its operator pass (the same
+// arithmetic as k_cheb_start / k_cheb_step / k_cheb_finish around k_q1_apply):
+//   from zero (pre-smoothing):  x = d = b / (theta diag),  r = b - A d
+//   from xin (post-smoothing):  xout = xin + (b - A xin) / (theta diag)   (xout != xin)
+__global__ void __launch_bounds__(256) k_q1_cheb1_from_zero(MGLevel lv, const double* __restrict__ b) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= lv.nodes) return;
+  const double inv_theta = 1.0 / lv.cheb[0];
+  const double* __restrict__ diag = lv.diag;
+  const double t = q1_apply_with(lv, n, [&](int64_t m) { return inv_theta * b[m] / diag[m]; });
+  lv.x[n] = inv_theta * b[n] / diag[n];
+  lv.r[n] = b[n] - t;
+}
+__global__ void __launch_bounds__(256) k_q1_cheb1_from_x(MGLevel lv, const double* __restrict__ b,
+                                                         const double* __restrict__ xin,
+                                                         double* __restrict__ xout) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= lv.nodes) return;
+  const double inv_theta = 1.0 / lv.cheb[0];
+  const double t = q1_apply_at(lv, xin, n);
+  xout[n] = xin[n] + inv_theta * (b[n] - t) / lv.diag[n];
 }
 __global__ void __launch_bounds__(256) k_q1_apply(MGLevel lv, const double* __restrict__ x,
                                                   double* __restrict__ y) {
@@ -518,8 +545,12 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
   return HM_OK;
 }
 
-int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_t s) {
+// The V-cycle from level l for A_l x = b.  *out: where the result lies -- x, except
+// for a Q1 level whose fused post-smoothing writes it to the level's lv.t.
+int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_t s,
+           double** out) {
   int rc;
+  *out = x;
   if (l == mg->tail_first && b == mg->lv[l].b && x == mg->lv[l].x) {
     MGTail T{};
     T.count = mg->nlev - l;
@@ -536,10 +567,30 @@ int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_
   }
   MGLevel& lv = mg->lv[l];
   MGLevel& cv = mg->lv[l + 1];
-  if ((rc = smooth(mg, l, b, x, true, true, mg->degree, clean, s))) return rc;
+  // degree 1 fused with the operator: on level 0 when every vector is zero on the
+  // Dirichlet nodes (inside the solves), on a Q1 level when its own buffers carry it
+  const bool fuse = mg->fused && mg->degree == 1 &&
+                    (l == 0 ? clean : (b == lv.b && x == lv.x));
+  if (fuse && l == 0) {
+    if ((rc = hm_launch_cheb1_from_zero(mg->L, mg->jac, mg->ess, b, lv.diag, lv.cheb, x, lv.r,
+                                        (void*)s)))
+      return rc;
+  } else if (fuse) {
+    k_q1_cheb1_from_zero<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, b);
+  } else if ((rc = smooth(mg, l, b, x, true, true, mg->degree, clean, s))) {
+    return rc;
+  }
   k_restrict<<<blocks_for(cv.nodes), 256, 0, s>>>(lv, cv, lv.r, cv.b);
-  if ((rc = vcycle(mg, l + 1, cv.b, cv.x, clean, s))) return rc;
-  k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, cv.x, x);
+  double* xc = nullptr;
+  if ((rc = vcycle(mg, l + 1, cv.b, cv.x, clean, s, &xc))) return rc;
+  k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, xc, x);
+  if (fuse && l == 0)
+    return hm_launch_cheb1_from_x(mg->L, mg->jac, mg->ess, b, lv.diag, lv.cheb, x, (void*)s);
+  if (fuse) {
+    k_q1_cheb1_from_x<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, b, x, lv.t);
+    *out = lv.t;
+    return HM_OK;
+  }
   return smooth(mg, l, b, x, false, false, mg->degree, clean, s);
 }
 
@@ -592,7 +643,8 @@ __global__ void k_count_mismatch(Lattice L, const uint8_t* __restrict__ ess, uns
 
 // inside the MG-PCG, whose residuals are zero on the Dirichlet nodes
 int hm_mg_vcycle(hm_mg* mg, const double* r, double* z, void* stream) {
-  return vcycle(mg, 0, r, z, true, S_(stream));
+  double* out = nullptr;
+  return vcycle(mg, 0, r, z, true, S_(stream), &out);
 }
 const double* hm_mg_level0_diag(const hm_mg* mg) { return mg->lv[0].diag; }
 void* hm_mg_jac(const hm_mg* mg) { return mg->jac; }
@@ -623,6 +675,7 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
   mg->coarse_degree = coarse_degree;
   mg->nlev = plan_levels(*L, mg->lv, 16);
   set_tail(mg, kTailNodes);
+  mg->fused = 1;
   double* w = static_cast<double*>(work);
   auto take = [&](int64_t n) { double* p = w; w += n; return p; };
   mg->scratch = take(3 * kMGBlocks + 64);
@@ -716,9 +769,16 @@ extern "C" int hm_mg_set_tail_nodes(hm_mg* mg, int64_t max_nodes) {
   return HM_OK;
 }
 
+extern "C" int hm_mg_set_fused(hm_mg* mg, int fused) {
+  if (!mg) return HM_ERR_ARG;
+  mg->fused = fused != 0;
+  return HM_OK;
+}
+
 extern "C" int hm_mg_apply(hm_mg* mg, const double* r, double* z, void* stream) {
   if (!mg || !r || !z || !mg->jac) return HM_ERR_ARG;
-  const int rc = vcycle(mg, 0, r, z, false, S_(stream));
+  double* out = nullptr;
+  const int rc = vcycle(mg, 0, r, z, false, S_(stream), &out);
   if (rc) return rc;
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }

@@ -844,6 +844,13 @@ extern "C" int hm_pcg_plan_create(const hm_lattice* h, void* jac64, void* jac32,
   return HM_OK;
 }
 
+int hm_plan_buffers(const hm_pcg_plan* p, double** b, double** x) {
+  if (!p || !b || !x) return HM_ERR_ARG;
+  *b = p->b;
+  *x = p->x;
+  return HM_OK;
+}
+
 extern "C" int hm_pcg_plan_set_mg(hm_pcg_plan* p, hm_mg* mg) {
   if (!p || (mg && p->jac32 != nullptr)) return HM_ERR_ARG;
   if (p->graph.exec) {

@@ -508,12 +508,26 @@ __global__ void __launch_bounds__(256, 2)
         gz < L.Nz)
       em[h] = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
   }
-  // CSR offsets of the rows (0, r2, r3): the lattice pattern's (the indptr the caller
-  // passes), computed rather than loaded
+  // CSR offsets of the rows (0, r2, r3): the lattice pattern's, computed rather than
+  // loaded.  The caller's indptr is loaded at the same rows and compared once the first
+  // fields have landed (the load's latency hidden behind theirs): a pattern other than
+  // the lattice's is rejected (HM_STATUS_RANGE, nothing written by this tile).
+  int32_t given = 0, expect = 0;
   if (tid < 16) {
     const int r2 = tid & 3, r3 = tid >> 2;
     const int gy = 4 * t2 + r2, gz = 4 * t3 + r3;
-    S.rowptr[tid] = (gy < L.Ny && gz < L.Nz) ? (int32_t)row_start(L, 4 * t1, gy, gz) : 0;
+    const bool live = gy < L.Ny && gz < L.Nz;
+    expect = live ? (int32_t)row_start(L, 4 * t1, gy, gz) : 0;
+    S.rowptr[tid] = expect;
+    given = (live && indptr != nullptr)
+                ? __ldg(indptr + (4 * t1 + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)))
+                : expect;
+  } else if (tid == 16 && indptr != nullptr && t1 == L.tx - 1 && t2 == L.ty - 1 &&
+             t3 == L.tz - 1) {
+    // the last tile also checks the total
+    expect = (int32_t)(stencil_prefix(L.Nx, L.Nx) * stencil_prefix(L.Ny, L.Ny) *
+                       stencil_prefix(L.Nz, L.Nz));
+    given = __ldg(indptr + L.ndof);
   }
   if (clipped && tid < 12) {
     const int d = tid / 4, r = tid % 4;
@@ -656,9 +670,11 @@ __global__ void __launch_bounds__(256, 2)
     }
     // the previous phase's image copies must have left the image before it is rewritten
     if (kBulk && tid < 16) bulk_wait_read();
-    if (__syncthreads_or(!ok)) {
+    const bool foreign = k == 0 && given != expect;
+    if (__syncthreads_or(!ok || foreign)) {
+      const bool pattern_bad = __syncthreads_or(foreign) != 0;
       if (tid == 0) {
-        atomicOr(&g_device_status, HM_STATUS_TIMEOUT);
+        atomicOr(&g_device_status, pattern_bad ? HM_STATUS_RANGE : HM_STATUS_TIMEOUT);
         // the other buffer's copy, if one is in flight, before the CTA leaves
         const int nx = next_phase(ph);
         if (nx >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
@@ -854,7 +870,8 @@ int launch_assemble_t(const Lattice& L, const void* quad, const int32_t* indptr,
   if (cudaGetDevice(&dev) != cudaSuccess) return HM_ERR_CUDA;
   {
     std::lock_guard<std::mutex> g(mu);
-    if (dev < 64 && !configured[dev]) {
+    if (dev < 0 || dev >= 64) return HM_ERR_UNSUPPORTED;
+    if (!configured[dev]) {
       if (cudaFuncSetAttribute(k_tile_assemble<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem) != cudaSuccess)
         return HM_ERR_CUDA;

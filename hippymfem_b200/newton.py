@@ -21,9 +21,15 @@ from .problem import ADJOINT, PARAMETER, STATE
 
 
 def ReducedSpaceNewtonCG_ParameterList():
+    """The reference's parameters and defaults (NewtonCG.py:79-130).  With
+    ``cg_reorthogonalize`` the Hessian actions of a Newton step's CG take their
+    incremental solves to ``min(cg_incremental_tolerance, tolcg / 1000)`` and the prior's
+    solves in its preconditioner to ``min(cg_preconditioner_tolerance, tolcg / 1000)``
+    where that is looser than their own; 0 keeps their own."""
     return {"rel_tolerance": 1e-6, "abs_tolerance": 1e-12, "gdm_tolerance": 1e-18,
             "max_iter": 20, "globalization": "LS", "print_level": 0, "GN_iter": 5,
             "cg_coarse_tolerance": 0.5, "cg_max_iter": 100, "cg_reorthogonalize": True,
+            "cg_incremental_tolerance": 1e-6, "cg_preconditioner_tolerance": 1e-6,
             "LS": {"c_armijo": 1e-4, "max_backtracking_iter": 10}}
 
 
@@ -36,6 +42,37 @@ class _Identity:
     def solve(self, x, b):
         x.copy_(b)
         return x
+
+
+class _LooserSolves:
+    """A solver whose PCG solves stop at ``tol`` while it is used, where that is looser
+    than their own tolerance (the prior's R^{-1} = A^{-1} M A^{-1} as a Newton-CG
+    preconditioner)."""
+
+    def __init__(self, solver, tol):
+        self.solver, self.tol = solver, float(tol)
+
+    def _pcgs(self):
+        out = []
+        for name in ("Asolver", "Msolver"):
+            inner = getattr(self.solver, name, None)
+            pcg = getattr(inner, "pcg", None)
+            if pcg is not None:
+                out.append(pcg)
+        return out
+
+    def solve(self, x, b):
+        saved = []
+        for pcg in self._pcgs():
+            own = pcg.parameters["rel_tolerance"]
+            if own < self.tol:
+                saved.append((pcg, own))
+                pcg.parameters["rel_tolerance"] = self.tol
+        try:
+            return self.solver.solve(x, b)
+        finally:
+            for pcg, own in saved:
+                pcg.parameters["rel_tolerance"] = own
 
 
 class CGSolverSteihaug:
@@ -192,6 +229,7 @@ class ReducedSpaceNewtonCG:
         x_star = [model.generate_vector(STATE), model.generate_vector(PARAMETER), None]
         cost_old = model.cost(x)[0]
         cost_new = cost_old
+        reorth = bool(p["cg_reorthogonalize"])
         gradnorm = gradnorm_ini = float("nan")
         tol = abs_tol
         while self.it < p["max_iter"] and not self.converged:
@@ -210,9 +248,16 @@ class ReducedSpaceNewtonCG:
             self.it += 1
             tolcg = min(p["cg_coarse_tolerance"], math.sqrt(gradnorm / gradnorm_ini))
             H = ReducedHessian(model)
+            inc = float(p.get("cg_incremental_tolerance") or 0.0)
+            if reorth and inc > 0.0:
+                H.set_accuracy(min(inc, 1e-3 * tolcg))
+            prec = model.Rsolver() if model.prior is not None else None
+            ptol = float(p.get("cg_preconditioner_tolerance") or 0.0)
+            if prec is not None and reorth and ptol > 0.0:
+                prec = _LooserSolves(prec, min(ptol, 1e-3 * tolcg))
             solver = CGSolverSteihaug()
             solver.set_operator(H)
-            solver.set_preconditioner(model.Rsolver() if model.prior is not None else None)
+            solver.set_preconditioner(prec)
             solver.parameters.update({"rel_tolerance": tolcg, "max_iter": p["cg_max_iter"],
                                       "zero_initial_guess": True,
                                       "reorthogonalize": bool(p["cg_reorthogonalize"])})
@@ -223,20 +268,18 @@ class ReducedSpaceNewtonCG:
                 model, x, x_star, mhat, mg_mhat, cost_old, c_armijo=p["LS"]["c_armijo"],
                 max_backtracking=p["LS"]["max_backtracking_iter"],
                 gdm_tolerance=p["gdm_tolerance"])
+            cost_new = cost[0]                      # the last trial's, accepted or not
             if accepted:
-                cost_old = cost_new = cost[0]
+                cost_old = cost_new
             self.history.append({"it": self.it, "cg_it": H.ncalls, "cost": cost[0],
                                  "misfit": cost[2], "reg": cost[1], "gdm": mg_mhat,
                                  "gradnorm": gradnorm, "alpha": alpha, "tolcg": tolcg})
             if p["print_level"] >= 0:
-                h = self.history[-1]
-                if self.it == 1:
-                    print("\n%3s %5s %15s %15s %15s %15s %14s %14s %14s"
-                          % ("It", "cg_it", "cost", "misfit", "reg", "(g,dm)", "||g||", "alpha",
-                             "tolcg"), flush=True)
-                print("%3d %5d %15e %15e %15e %15e %14e %14e %14e"
-                      % (h["it"], h["cg_it"], h["cost"], h["misfit"], h["reg"], h["gdm"],
-                         h["gradnorm"], h["alpha"], h["tolcg"]), flush=True)
+                print("newton %2d: cg %3d  cost %.8e (misfit %.6e, reg %.6e)  (g,dm) %+.3e  "
+                      "|g| %.3e  alpha %.4g  tolcg %.3e"
+                      % tuple(self.history[-1][k] for k in ("it", "cg_it", "cost", "misfit",
+                                                             "reg", "gdm", "gradnorm", "alpha",
+                                                             "tolcg")), flush=True)
             if self.callback:
                 self.callback(self.it, x)
             if n_back == p["LS"]["max_backtracking_iter"]:

@@ -205,3 +205,207 @@ def device_slab_assembler(n, L, u, m, p, ess, f=1.0):
     if int(status.item()) != 0:
         raise RuntimeError("non-finite values in the fields")
     return pat.indptr, blocks, {0: vecs[0], 1: vecs[1], 2: vecs[2]}
+
+
+# ------------------------------------------------------------- sharded Hessian action
+# The reduced-Hessian action (modeling/reducedHessian.py:87-131) over the same z-slabs.
+# Every operator of the action is a vector assembly on rank's lattice (its slab and one
+# element layer below) from node values on its planes: the Jacobian apply, the second-
+# order products from the directional data (C mhat, W_um mhat, W_mm mhat), the
+# transposed ones as dR/dm with the direction in the adjoint or state slot, and the
+# misfit's W_uu from the observations inside rank's elements.  So one exchange of the
+# input's halo planes (exchange_planes) precedes each, and the owned rows of its result
+# are complete -- the hypre ParCSR halo of the reference's true-dof route
+# (fem/tdofassemble.py:657-724, common/parvector.py:107-146) moved to the inputs.  The
+# incremental solves are Jacobi-PCG over the slabs; each inner product is the sum, in
+# plane order, of per-node-plane partial sums gathered from all ranks, so the action is
+# bit for bit the same on any number of ranks (a plane's partial is computed alike
+# wherever it lives).
+
+def plane_partials(a, b):
+    """Per-node-plane partial sums of a . b for owned-plane arrays (planes, nodes)."""
+    return (a * b).sum(dim=1)
+
+
+def sharded_dot(part, a, b, group=None):
+    """a . b over all ranks' owned planes, summed plane by plane in order."""
+    pp = plane_partials(a, b)
+    if part.world == 1:
+        return float(pp.sum())
+    sizes = [part.owned_planes(r)[1] - part.owned_planes(r)[0] for r in range(part.world)]
+    width = max(sizes)
+    mine = torch.zeros(width, dtype=pp.dtype, device=pp.device)
+    mine[:pp.numel()] = pp
+    bufs = [torch.empty(width, dtype=pp.dtype, device=pp.device) for _ in sizes]
+    dist.all_gather(bufs, mine, group=group)
+    return float(torch.cat([b[:s] for b, s in zip(bufs, sizes)]).sum())
+
+
+class ShardedHessian:
+    """The misfit part of ``ReducedHessian.mult`` (TrueHessian; ``gauss_newton``:
+    GNHessian) at the point ``(u, m, p)`` over the slabs of ``part``; every vector is
+    rank's owned planes, shape ``(planes, nodes per plane)``.
+
+    ``ops``: rank's local operators, an object with
+    ``set_point(u, m, p, ess)`` (local node values), ``apply_A(x) -> y`` (the eliminated
+    Jacobian), ``diag_A() -> d``, ``dir_products(mhat) -> (C mhat, W_um mhat, W_mm mhat)``
+    (rows of C and W_um zeroed on the Dirichlet nodes), ``grad_m(u, p) -> dR/dm`` at
+    ``(u, m, p)`` with the point's ``m``, and ``wuu(x) -> W_uu x`` -- all on rank's
+    local lattice (vectors of its local planes, flattened)."""
+
+    def __init__(self, part, rank, ops, u, m, p, ess, rtol=1e-12, max_iter=20000,
+                 gauss_newton=False, group=None):
+        self.part, self.rank, self.ops, self.group = part, rank, ops, group
+        self.rtol, self.max_iter, self.gauss_newton = float(rtol), int(max_iter), gauss_newton
+        self.shape = tuple(u.shape)
+        self.ess = ess.to(torch.bool)
+        loc = [self.halo(t) for t in (u, m, p)]
+        self.ess_local = self.halo(ess.to(torch.int32)).to(torch.bool)
+        self.u, self.m, self.p = loc
+        ops.set_point(loc[0], loc[1], loc[2], self.ess_local)
+        self.diag = self.own(ops.diag_A())
+        self.iterations = []
+
+    def halo(self, owned):
+        return exchange_planes(owned, self.part, self.rank, self.group).reshape(-1)
+
+    def own(self, local):
+        r0, r1 = self.part.owned_local_rows(self.rank)
+        return local[r0:r1].reshape(self.shape)
+
+    def apply_A(self, x):
+        return self.own(self.ops.apply_A(self.halo(x)))
+
+    def dot(self, a, b):
+        return sharded_dot(self.part, a, b, self.group)
+
+    def solve(self, b):
+        """A x = b (b zero on the Dirichlet nodes) by Jacobi-PCG from zero to ||r|| <=
+        rtol ||b||; the iteration count is kept."""
+        x = torch.zeros_like(b)
+        bb = self.dot(b, b)
+        if bb == 0.0:
+            self.iterations.append(0)
+            return x
+        r = b.clone()
+        z = r / self.diag
+        d = z.clone()
+        rz = self.dot(r, z)
+        tol2 = self.rtol * self.rtol * bb
+        for it in range(1, self.max_iter + 1):
+            q = self.apply_A(d)
+            alpha = rz / self.dot(d, q)
+            x.add_(d, alpha=alpha)
+            r.add_(q, alpha=-alpha)
+            if self.dot(r, r) <= tol2:
+                self.iterations.append(it)
+                return x
+            z = r / self.diag
+            rz_new = self.dot(r, z)
+            d.mul_(rz_new / rz).add_(z)
+            rz = rz_new
+        raise RuntimeError("sharded PCG did not reach rtol %g in %d iterations"
+                           % (self.rtol, self.max_iter))
+
+    def mult(self, x):
+        """y = H x on rank's owned planes (collective: every rank calls it)."""
+        ops = self.ops
+        xl = self.halo(x)
+        c, wum, wmm = (self.own(v) for v in ops.dir_products(xl))
+        uhat = self.solve(c.masked_fill(self.ess, 0.0))
+        rhs = self.own(ops.wuu(self.halo(uhat)))
+        if not self.gauss_newton:
+            rhs = rhs - wum
+        phat = self.solve(rhs.masked_fill(self.ess, 0.0))
+        y = self.own(ops.grad_m(self.u, self.halo(phat.masked_fill(self.ess, 0.0))))
+        if not self.gauss_newton:
+            y = y + wmm - self.own(ops.grad_m(self.halo(uhat), self.p))
+        return y
+
+
+def local_points(part, rank, points):
+    """The observation targets inside rank's local elements, in its lattice's
+    coordinates, and their indices (the element of a target as the global lattice
+    assigns it)."""
+    pts = np.asarray(points, dtype=np.float64)
+    ze0, ze1 = part.local_elements(rank)
+    hz = part.h[2]
+    ez = np.clip(np.floor(pts[:, 2] / hz).astype(np.int64), 0, part.n[2] - 1)
+    keep = np.flatnonzero((ez >= ze0) & (ez < ze1))
+    loc = pts[keep].copy()
+    loc[:, 2] -= ze0 * hz
+    return loc, keep
+
+
+class DeviceSlabOps:
+    """``ShardedHessian``'s local operators on the GPU: rank's lattice as a ``BoxMesh``
+    and the library's kernels (matrix-free Jacobian, directional quadrature data and the
+    fused vector assembly, the device observation operator)."""
+
+    def __init__(self, part, rank, points, noise_variance, device):
+        from .mesh import BoxMesh
+        from .modeling import device_observation_operator
+        n, L = part.local_box(rank)
+        self.mesh = BoxMesh(n, L, device=device)
+        loc, _ = local_points(part, rank, points)
+        self.nobs = len(loc)
+        self.B = device_observation_operator(self.mesh, loc) if self.nobs else None
+        self.Bt = self.B.transpose() if self.nobs else None
+        self.inv_noise = 1.0 / float(noise_variance)
+        self.quad = torch.empty(self.mesh.quad_bytes() // 8, dtype=torch.float64, device=device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+
+    def _quadrature(self, u, m, p, mhat=None):
+        from . import _lib
+        from ._lib import check, lib, ptr, stream_ptr
+        if mhat is None:
+            check(lib.hm_lattice_quadrature(self.mesh.handle, ptr(u), ptr(m), ptr(p), _lib.HM_FP64,
+                                            ptr(self.quad), ptr(self.status), stream_ptr()))
+        else:
+            check(lib.hm_lattice_quadrature_dir(self.mesh.handle, ptr(u), ptr(m), ptr(p), ptr(mhat),
+                                                _lib.HM_FP64, ptr(self.quad), ptr(self.status),
+                                                stream_ptr()))
+
+    def _vectors(self, slots, f=0.0):
+        from . import _lib
+        from ._lib import check, lib, ptr, stream_ptr
+        out = {s: torch.empty(self.mesh.ndof, dtype=torch.float64, device=self.quad.device)
+               for s in slots}
+        check(lib.hm_lattice_assemble(self.mesh.handle, ptr(self.quad), _lib.HM_FP64, None,
+                                      ptr(self.marker), float(f), None, None, None, None,
+                                      ptr(out.get(0)), ptr(out.get(1)), ptr(out.get(2)), 0,
+                                      stream_ptr()))
+        return out
+
+    def set_point(self, u, m, p, ess):
+        from .sparse import MatrixFreeJacobian
+        self.u, self.m, self.p = u.contiguous(), m.contiguous(), p.contiguous()
+        self.marker = ess.to(torch.uint8).contiguous()
+        self.mask = ess
+        self._quadrature(self.u, self.m, self.p)
+        self.A = MatrixFreeJacobian(self.mesh, self.quad, self.marker)
+
+    def apply_A(self, x):
+        y = torch.empty_like(x)
+        return self.A.mult(x.contiguous(), y)
+
+    def diag_A(self):
+        return self.A.diagonal()
+
+    def dir_products(self, mhat):
+        self._quadrature(self.u, self.m, self.p, mhat.contiguous())
+        v = self._vectors((0, 1, 2))
+        return (v[2].masked_fill(self.mask, 0.0), v[0].masked_fill(self.mask, 0.0), v[1])
+
+    def grad_m(self, u, p):
+        self._quadrature(u.contiguous(), self.m, p.contiguous())
+        return self._vectors((1,))[1]
+
+    def wuu(self, x):
+        if not self.nobs:
+            return torch.zeros_like(x)
+        bu = torch.empty(self.nobs, dtype=torch.float64, device=x.device)
+        self.B.mult(x.contiguous(), bu)
+        y = torch.empty_like(x)
+        self.Bt.mult(bu, y, alpha=self.inv_noise)
+        return y

@@ -332,6 +332,12 @@ class Multigrid:
         check(lib.hm_mg_set_tail_nodes(self._mg, int(max_nodes)), "hm_mg_set_tail_nodes")
         return self
 
+    def set_fused(self, fused):
+        """Degree-1 smoothing steps fused with their operator pass (the default), or
+        launched step by step; the same arithmetic either way."""
+        check(lib.hm_mg_set_fused(self._mg, int(bool(fused))), "hm_mg_set_fused")
+        return self
+
     def close(self):
         if self._mg:
             lib.hm_mg_destroy(self._mg)

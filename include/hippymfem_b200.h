@@ -132,7 +132,12 @@ int hm_lattice_quadrature_dir(const hm_lattice* h, const double* d_u, const doub
  * NULL: dR/du (STATE), dR/dm (PARAMETER), dR/dp (ADJOINT, the residual with source f);
  * with zero_ess_vectors the STATE and ADJOINT ones are zeroed on d_ess.  The value
  * arrays and d_quad must be 16-byte aligned (HM_ERR_ARG otherwise; cudaMalloc and
- * torch allocations are).  Replaces setLinearizationPoint's shared pass (modeling/PDEVariationalProblem.py:
+ * torch allocations are).  d_indptr must be the lattice pattern's (required when a
+ * block is asked for, else it may be NULL); the kernel compares it with the lattice's
+ * row offsets, and a tile that finds another pattern writes nothing and sets
+ * HM_STATUS_RANGE in the library's status word (hm_device_status).  For a caller's own
+ * dof numbering, assemble in the lattice pattern and map the values with
+ * hm_lattice_caller_map + hm_gather_f64.  Replaces setLinearizationPoint's shared pass (modeling/PDEVariationalProblem.py:
  * 1372-1482), _jacobian (:542), _residual (:423), element_matrices_many /
  * element_vectors (hippymfem/fem/kernel.py:2048,2070) and the scatter
  * ScatterPattern.data (hippymfem/fem/pattern.py:749-791). */
@@ -178,6 +183,61 @@ int hm_lattice_residual_noalloc(const hm_lattice* h, const double* d_u, const do
                                 double* d_vec_state, double* d_vec_param,
                                 double* d_vec_adjoint, int zero_ess_vectors,
                                 uint32_t* d_status, void* stream);
+
+/* Constant-exact single-precision blocks: the reference's mixed-precision element
+ * matrices with consistent_block (hippymfem/fem/kernel.py:1503-1571).  Each element
+ * matrix of the blocks whose pointer is not NULL is contracted in FP32 from the FP64
+ * quadrature data d_quad (rounded to FP32) and corrected in FP64 by one rank-one term
+ * per side so that its products with the element's constants are the FP64 ones (A and
+ * Wmm symmetrized first and symmetric to the bit); the corrected matrices are summed
+ * into the lattice pattern entry by entry in a fixed element order, with the folded
+ * elimination of hm_lattice_assemble on d_ess.  The assembled blocks are then exact on
+ * the constants (A 1 = 0 before elimination) to FP64 rounding.  d_work:
+ * hm_lattice_consistent_workspace_bytes (one block's element matrices, FP64). */
+int64_t hm_lattice_consistent_workspace_bytes(const hm_lattice* h);
+int hm_lattice_assemble_consistent(const hm_lattice* h, const double* d_quad,
+                                   const uint8_t* d_ess, double* d_vals_A, double* d_vals_C,
+                                   double* d_vals_Wum, double* d_vals_Wmm, void* d_work,
+                                   void* stream);
+
+/* ------------------------------------------------------ the caller's dof numbering
+ * The lattice numbers its Q2 dofs lexicographically; a caller whose space numbers them
+ * otherwise (MFEM's element-to-dof table, hippymfem/fem/elementbatch.py:528-565, with
+ * MFEM's element-local order) keeps its numbering:
+ *
+ * hm_lattice_dof_permutation (host memory): perm[n] = the caller's dof at lattice node
+ *   n, from the caller's element dof table cdofs (ne x 27, its elements in the lattice's
+ *   element order e = ex + nx (ey + ny ez)) and local[a] = the caller's element-local
+ *   slot of lattice-local dof a = a1 + 3 a2 + 9 a3 (NULL: the same order).  HM_ERR_ARG
+ *   when the table puts two dofs at one node or is not a bijection onto [0, ndof),
+ *   HM_ERR_RANGE for a dof outside it.
+ * hm_lattice_caller_map (device): d_src_pos[s] = the lattice-pattern position of entry s
+ *   of the caller's pattern (d_cindptr / d_cindices: the arrays hm_pattern_build gives
+ *   for the caller's table, the reference's ScatterPattern arrays, fem/pattern.py:
+ *   548-663); the block values then reach the caller's CSR (the data array its
+ *   HypreParMatrix aliases, fem/parmat.py:106-171) by hm_gather_f64(nnz, d_src_pos,
+ *   lattice_vals, caller_vals).  A pattern that does not match sets HM_STATUS_RANGE in
+ *   *d_status.
+ * hm_gather_f64: d_dst[i] = d_src[d_idx[i]], i < n.  Vectors into the lattice:
+ *   idx = perm; back to the caller: idx = perm's inverse. */
+int hm_lattice_dof_permutation(const hm_lattice* h, const int64_t* cdofs, const int32_t* local,
+                               int32_t* perm);
+int hm_lattice_caller_map(const hm_lattice* h, const int32_t* d_perm, const int32_t* d_cindptr,
+                          const int32_t* d_cindices, int32_t* d_src_pos, uint32_t* d_status,
+                          void* stream);
+int hm_gather_f64(int64_t n, const int32_t* d_idx, const double* d_src, double* d_dst,
+                  void* stream);
+
+/* The element matrices of a point: for elements e0 .. e0 + count - 1, the (27 x 27)
+ * matrices of A, C, Wum and Wmm (each output may be NULL) from the quadrature data of
+ * hm_lattice_quadrature, FP64, at d_X[(e - e0) * 729 + local[a] * 27 + local[b]] (row:
+ * test dof a, column: trial dof b; local: host array, NULL for the lattice order).
+ * Not on the fused path (the assembly never forms them): the export of
+ * QuadratureKernel.element_matrices / element_matrices_chunks
+ * (hippymfem/fem/kernel.py:1964-2068) for inspection and parity checks. */
+int hm_lattice_element_blocks(const hm_lattice* h, const void* d_quad, int precision, int64_t e0,
+                              int64_t count, const int32_t* local, double* d_A, double* d_C,
+                              double* d_Wum, double* d_Wmm, void* stream);
 
 /* ----------------------------------------------------------------- sparse / solve
  * y = alpha * M x + beta * y for a CSR block (hypre's Mult, apply_ij). */
@@ -279,10 +339,44 @@ int hm_mg_levels(const hm_mg* mg);
  * node; one launch instead of ~14 per level).  Set it before a plan's first solve: a
  * plan's captured iteration batches keep the launches they were captured with. */
 int hm_mg_set_tail_nodes(hm_mg* mg, int64_t max_nodes);
+/* With smoothing degree 1 (the default from a million dofs up) each smoothing step runs
+ * as one pass with its level's operator: on level 0 inside the solves (every vector
+ * zero on the Dirichlet nodes) the Q2 operator's two kernels carry the Chebyshev update,
+ * on the Q1 levels one kernel does both; the arithmetic is the step-by-step one, bit for
+ * bit (fused = 1, the default).  fused = 0 launches the steps one by one.  Set it before
+ * a plan's first solve, as the tail. */
+int hm_mg_set_fused(hm_mg* mg, int fused);
 int hm_mg_destroy(hm_mg* mg);
 int hm_pcg_mg(hm_mg* mg, const double* d_b, double* d_x, double rtol, int maxiter,
               int check_every, void* d_work, int* iterations, double* relres, void* stream);
 int hm_pcg_plan_set_mg(hm_pcg_plan* plan, hm_mg* mg);
+
+/* The reduced-Hessian action ReducedHessian.mult (hippymfem/modeling/reducedHessian.py:
+ * 87-131) at an assembled linearization point, misfit part (the caller adds R x of its
+ * prior, as the reference's TrueHessian does unless misfit_only):
+ *   uhat = A^{-1} C x,  phat = A^{-T} (W_uu uhat - W_um x),  y = W_mm x + C^T phat - W_mu uhat
+ * (GNHessian, y = C^T phat, when d_vals_Wum and d_vals_Wmm are NULL); the right-hand
+ * sides zeroed on d_ess as solveIncremental does (modeling/PDEVariationalProblem.py:
+ * 1583-1609).  Blocks: CSR values on the lattice pattern (d_indptr, d_indices, d_tpos of
+ * hm_lattice_transpose_map).  W_uu = B^T B / noise_variance (misfit.py:102-110) from the
+ * observation operator B (nobs x ndof) and its transpose (hm_csr_transpose); nobs = 0:
+ * no misfit term.  The two solves run on `plan` (its FP64, multigrid or mixed-precision
+ * PCG, from zero, to rtol) through the plan's own right-hand side and solution buffers,
+ * which the action overwrites.  d_work: hm_hessian_workspace_bytes(ndof, nobs).
+ * iterations (may be NULL): the two solves' iteration counts.  One action at a time per
+ * object (it shares the plan). */
+typedef struct hm_hessian hm_hessian;
+int64_t hm_hessian_workspace_bytes(int64_t ndof, int64_t nobs);
+int hm_hessian_create(const hm_lattice* h, const int32_t* d_indptr, const int32_t* d_indices,
+                      const int32_t* d_tpos, const double* d_vals_C, const double* d_vals_Wum,
+                      const double* d_vals_Wmm, int64_t nobs, const int32_t* d_B_indptr,
+                      const int32_t* d_B_indices, const double* d_B_vals,
+                      const int32_t* d_Bt_indptr, const int32_t* d_Bt_indices,
+                      const double* d_Bt_vals, double noise_variance, const uint8_t* d_ess,
+                      hm_pcg_plan* plan, void* d_work, hm_hessian** out);
+int hm_hessian_apply(hm_hessian* H, const double* d_x, double* d_y, double rtol, int maxiter,
+                     int* iterations, void* stream);
+int hm_hessian_destroy(hm_hessian* H);
 
 /* ---------------------------------------------------------------- observations
  * The pointwise observation operator B (npts x ndof) of the lattice's Q2 space: row o

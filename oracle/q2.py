@@ -339,6 +339,67 @@ def csr(pattern, data, shape):
     return sp.csr_matrix((np.array(data), indices.copy(), indptr.copy()), shape=shape)
 
 
+def elements_of_nodes(mesh, nodes):
+    """The elements holding any of the lattice ``nodes`` (ascending element ids): the
+    only elements whose element matrices reach those rows."""
+    Nx, Ny, _ = mesh.N
+    nodes = np.asarray(nodes, dtype=np.int64)
+    idx = (nodes % Nx, (nodes // Nx) % Ny, nodes // (Nx * Ny))
+    out = set()
+    for i, j, k in zip(*idx):
+        per_axis = []
+        for c, n in zip((i, j, k), mesh.n):
+            cand = (c // 2,) if c % 2 else (c // 2 - 1, c // 2)
+            per_axis.append([e for e in cand if 0 <= e < n])
+        for ez in per_axis[2]:
+            for ey in per_axis[1]:
+                for ex in per_axis[0]:
+                    out.add(ex + mesh.n[0] * (ey + mesh.n[1] * ez))
+    return np.array(sorted(out), dtype=np.int64)
+
+
+def assembled_rows(mesh, u, m, p, rows, ess_mask=None, f=1.0, which=("A", "C", "Wum", "Wmm")):
+    """Selected rows of the assembled blocks and vectors, from the elements around them
+    only: the same scatter (``pattern.py:749-791``), folded elimination
+    (``csrassemble.py:164-270``, ``bcs.py:13-30``) and vector assembly
+    (``pattern.py:1186-1233``) as the whole-mesh functions, restricted to ``rows`` so
+    that a large lattice can be checked in seconds.
+
+    Returns ``(blocks, vectors)``: ``blocks[name] = (keys, values)`` with
+    ``keys = row * ndof + col`` ascending; ``vectors[slot]`` the vector at ``rows``
+    (not zeroed on the essential dofs)."""
+    rows = np.unique(np.asarray(rows, dtype=np.int64))
+    elems = elements_of_nodes(mesh, rows)
+    E = mesh.edofs()[elems]
+    nd = mesh.ndof
+    want = np.isin(E, rows)                                      # (ne_sub, 27) test dofs kept
+    er, ea = np.nonzero(want)
+    r = E[er, ea]                                                # row of each kept (e, a)
+    blocks = {}
+    for name in which:
+        K = element_blocks(mesh, E, u, m, p, (name,))[name]      # (ne_sub, 27, 27)
+        keys = (r[:, None] * nd + E[er]).reshape(-1)
+        vals = K[er, ea, :].reshape(-1)
+        uk, inv = np.unique(keys, return_inverse=True)
+        acc = np.bincount(inv.reshape(-1), weights=vals, minlength=len(uk))
+        rr, cc = uk // nd, uk % nd
+        pol_rows, pol_cols, diag = ELIMINATION[name]
+        if ess_mask is not None:
+            kill = np.zeros(len(uk), dtype=bool)
+            if pol_rows:
+                kill |= ess_mask[rr]
+            if pol_cols:
+                kill |= ess_mask[cc]
+            acc[kill] = 0.0
+            if diag is not None:
+                acc[kill & (rr == cc) & ess_mask[rr]] = diag
+        blocks[name] = (uk, acc)
+    ev = element_vectors(mesh, E, u, m, p, f)
+    pos = np.searchsorted(rows, r)
+    vectors = {s: np.bincount(pos, weights=ev[s][er, ea], minlength=len(rows)) for s in ev}
+    return blocks, vectors
+
+
 # ------------------------------------------------------------------- observations
 def observation_matrix(mesh, points):
     """Pointwise observation operator ``B``: row ``o`` holds the Q2 basis values at

@@ -109,3 +109,40 @@ def test_observation_box_test_matches_the_kernel_rule():
                     [0.5, np.inf, 0.5], [0.3, 0.3, 0.3]])
     assert targets_in_box(mesh, pts).tolist() == [True, True, True, False, False, False,
                                                  False, True]
+
+
+def test_dof_permutation_from_a_caller_table():
+    """hm_lattice_dof_permutation (host): the permuted fixture's table (random global
+    numbering, random element-local order) gives back its global permutation; a table
+    that puts two dofs at one node, or a bad local order, is refused."""
+    from hippymfem_b200 import _lib
+    from hippymfem_b200._lib import hptr
+
+    z = load_golden("pattern_q2_permuted_3x3x2.npz")
+    mo = q2.Lattice((3, 3, 2))
+    rng = np.random.default_rng(20261203)           # the fixture's generator, in its order
+    perm = rng.permutation(mo.ndof)
+    local_fix = rng.permutation(27)
+    tp = np.ascontiguousarray(z["tdofs"], dtype=np.int64)
+    assert np.array_equal(perm[mo.edofs()][:, local_fix], tp)
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib.hm_lattice_create(3, 3, 2, 1.0, 1.0, 1.0, ctypes.byref(h)))
+    try:
+        local = np.ascontiguousarray(np.argsort(local_fix), dtype=np.int32)
+        out = np.empty(mo.ndof, dtype=np.int32)
+        _lib.check(_lib.lib.hm_lattice_dof_permutation(h, hptr(tp), hptr(local), hptr(out)))
+        assert np.array_equal(out, perm)
+        bad = tp.copy()
+        bad[0, 0], bad[0, 1] = bad[0, 1], bad[0, 0]          # two dofs swapped in one element
+        with pytest.raises(ValueError):
+            _lib.check(_lib.lib.hm_lattice_dof_permutation(h, hptr(bad), hptr(local), hptr(out)))
+        dup = local.copy()
+        dup[1] = dup[0]
+        with pytest.raises(ValueError):
+            _lib.check(_lib.lib.hm_lattice_dof_permutation(h, hptr(tp), hptr(dup), hptr(out)))
+        big = tp.copy()
+        big[2, 3] = mo.ndof
+        with pytest.raises(IndexError):
+            _lib.check(_lib.lib.hm_lattice_dof_permutation(h, hptr(big), hptr(local), hptr(out)))
+    finally:
+        _lib.lib.hm_lattice_destroy(h)

@@ -150,3 +150,34 @@ def test_c_abi_mg_pcg_matches_the_plan(cuda):
                         ctypes.byref(rr), stream_ptr()))
     assert it.value == s.last.iterations
     assert torch.equal(x, ref)
+
+
+@pytest.mark.parametrize("n,L", [((32, 16, 24), (1.0, 0.5, 0.75)), ((16, 16, 16), (1.0, 1.0, 1.0))])
+def test_fused_degree_one_smoothing_is_the_step_by_step_cycle(cuda, n, L):
+    """With smoothing degree 1 each step runs fused with its level's operator pass (on
+    level 0 inside the solves, where every vector is zero on the Dirichlet nodes): the
+    V-cycle and a whole MG-PCG solve are bit for bit those of the step-by-step launches."""
+    import ctypes
+
+    from hippymfem_b200._lib import check, lib, ptr, stream_ptr
+    from hippymfem_b200.sparse import Multigrid
+
+    mesh, V, prob, m, A = _jacobian(n, L, seed=3)
+    r = _interior(mesh, V, prob.bc0.mask, 8)
+    mg = Multigrid(mesh, degree=1).setup(A.jac, A.ess, A._diag)
+    zf = mg.set_fused(True).apply(r, V.vector())
+    zs = mg.set_fused(False).apply(r, V.vector())
+    assert torch.equal(zf, zs)
+    work = torch.empty(lib.hm_pcg_workspace_bytes(mesh.ndof) // 8 + 1, dtype=torch.float64,
+                       device=cuda)
+    out = []
+    for fused in (True, False):
+        mg.set_fused(fused)
+        x = V.vector()
+        it, rr = ctypes.c_int(), ctypes.c_double()
+        check(lib.hm_pcg_mg(mg._mg, ptr(r), ptr(x), 1e-12, 200, 4, ptr(work), ctypes.byref(it),
+                            ctypes.byref(rr), stream_ptr()))
+        out.append((x, it.value, rr.value))
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+    assert torch.equal(out[0][0], out[1][0])
+    assert out[0][2] <= 1e-12

@@ -121,3 +121,35 @@ def test_newton_cg_converges(cuda):
     model.solveAdj(x[2], x)
     gn = model.evalGradientParameter(x, g)
     assert gn <= 1e-5 * solver.history[0]["gradnorm"]
+
+
+def test_newton_cg_iterates_match_the_oracle_restatement(cuda):
+    """The device Newton-CG against the oracle's restatement of ReducedSpaceNewtonCG._solve_ls
+    (NewtonCG.py:262-375) with its Steihaug CG and Armijo step, on the same data, every
+    solve direct in the oracle: step by step the same CG counts, step lengths and
+    termination reason, and cost, |g| and (g, dm) to 1e-8."""
+    from hippymfem_b200.newton import ReducedSpaceNewtonCG, ReducedSpaceNewtonCG_ParameterList
+    from hippymfem_b200.synthetic import interior_points
+
+    from oracle import newton as on
+
+    n = 8
+    mesh, V, prob, model = _inverse_problem(n)
+    prm = ReducedSpaceNewtonCG_ParameterList()
+    prm.update({"print_level": -1, "rel_tolerance": 1e-6, "max_iter": 25,
+                "cg_incremental_tolerance": 0.0, "cg_preconditioner_tolerance": 0.0})
+    solver = ReducedSpaceNewtonCG(model, prm)
+    x = [V.vector(), V.vector(), V.vector()]
+    solver.solve(x)
+    ref = on.InverseProblem(n, interior_points(64, seed=2), model.misfit.d.cpu().numpy(),
+                            model.misfit.noise_variance, gamma=0.05, delta=0.5)
+    m, hist, reason, converged = on.newton_cg_ls(ref, np.zeros(ref.nd), rel_tolerance=1e-6,
+                                                 max_iter=25)
+    assert (solver.reason, solver.converged) == (reason, converged)
+    assert len(solver.history) == len(hist) >= 3
+    for a, b in zip(solver.history, hist):
+        assert a["cg_it"] == b["cg_it"] and a["alpha"] == b["alpha"], (a, b)
+        for k in ("cost", "misfit", "reg", "gradnorm"):
+            assert abs(a[k] - b[k]) <= 1e-8 * abs(b[k]), (k, a, b)
+        assert abs(a["gdm"] - b["gdm"]) <= 1e-8 * abs(b["gdm"]) + 1e-14, (a, b)
+    assert np.linalg.norm(x[1].cpu().numpy() - m) <= 1e-7 * np.linalg.norm(m)

@@ -42,3 +42,37 @@ def test_slab_stretches_equal_the_global_assembly(cuda):
             assert torch.equal(lv[s][r0:r1], gv[s][g0:g1]), (r, s)
         covered += s1 - s0
     assert covered == gb["A"].numel()
+
+
+def test_device_slab_operators_give_the_hessian_action(cuda):
+    """ShardedHessian with the CUDA slab operators (matrix-free Jacobian, directional
+    quadrature data, fused vector assembly, device observation operator) on one rank:
+    the oracle's TrueHessian restatement to the solve tolerance.  The decomposition over
+    several ranks is tested with gloo on the CPU (bit for bit against one rank)."""
+    from hippymfem_b200.shard import DeviceSlabOps, ShardedHessian, SlabPartition
+    from oracle import q2
+
+    n, L = (6, 5, 7), (1.0, 0.8, 1.3)
+    mo = q2.Lattice(n, L)
+    rng = np.random.default_rng(43)
+    u, p = rng.standard_normal(mo.ndof), rng.standard_normal(mo.ndof)
+    m = 0.4 * rng.standard_normal(mo.ndof)
+    x = rng.standard_normal(mo.ndof)
+    ess = np.zeros(mo.ndof, np.int32)
+    ess[mo.boundary_dofs()] = 1
+    pts = 0.05 + 0.9 * rng.random((30, 3)) * np.asarray(L)
+    part = SlabPartition(n, L, 1)
+    shape = (mo.N[2], -1)
+    own = [torch.as_tensor(a.reshape(shape).copy(), device=cuda) for a in (u, m, p, ess, x)]
+    ops = DeviceSlabOps(part, 0, pts, 1e-3, cuda)
+    H = ShardedHessian(part, 0, ops, *own[:4], rtol=1e-13)
+    y = H.mult(own[4]).reshape(-1).cpu().numpy()
+    E = mo.edofs()
+    nd = mo.ndof
+    mask = ess.astype(bool)
+    pat = q2.build_tables(E, E, nd, nd, True)
+    blk = q2.element_blocks(mo, E, u, m, p)
+    blocks = {k: q2.csr(pat, q2.assemble_block(k, pat, blk[k], mask), (nd, nd)) for k in blk}
+    B = q2.observation_matrix(mo, pts)
+    yref, _ = q2.hessian_apply(blocks, x, np.flatnonzero(mask), Wuu=(B.T @ B) / 1e-3, rtol=1e-13)
+    assert np.linalg.norm(y - yref) <= 1e-9 * np.linalg.norm(yref)

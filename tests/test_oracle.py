@@ -199,3 +199,31 @@ def test_consistent_blocks_are_exact_on_the_constants():
             assert np.abs(Kc[name].transpose(0, 2, 1) @ one - t64).max() <= 1e-13 * scale
         # the uncorrected block's row sums carry its single-precision error
         assert np.abs(K32[name] @ one - d64).max() > 1e3 * np.abs(Kc[name] @ one - d64).max()
+
+
+def test_assembled_rows_equal_the_whole_mesh_assembly():
+    """The row-restricted oracle (used to check the 64^3 benchmark assembly on a sample of
+    its rows) gives exactly the rows of the whole-mesh scatter, elimination and vector
+    assembly."""
+    mesh = q2.Lattice((4, 3, 5), (1.0, 0.7, 1.3))
+    E = mesh.edofs()
+    nd = mesh.ndof
+    rng = np.random.default_rng(21)
+    u, m, p = rng.standard_normal(nd), 0.3 * rng.standard_normal(nd), rng.standard_normal(nd)
+    ess = np.zeros(nd, bool)
+    ess[mesh.boundary_dofs()] = True
+    pat = q2.build_tables(E, E, nd, nd, True)
+    blk = q2.element_blocks(mesh, E, u, m, p)
+    ev = q2.element_vectors(mesh, E, u, m, p, 1.3)
+    rows = np.unique(np.concatenate([rng.choice(nd, 60, replace=False), mesh.boundary_dofs()[:9]]))
+    got_b, got_v = q2.assembled_rows(mesh, u, m, p, rows, ess, 1.3)
+    row_of = np.repeat(np.arange(nd), np.diff(pat[0]))
+    sel = np.isin(row_of, rows)
+    keys = row_of[sel] * nd + pat[1][sel]
+    order = np.argsort(keys)
+    for name in ("A", "C", "Wum", "Wmm"):
+        full = q2.assemble_block(name, pat, blk[name], ess)
+        assert np.array_equal(got_b[name][0], keys[order]), name
+        assert np.array_equal(got_b[name][1], full[sel][order]), name
+    for s in range(3):
+        assert np.array_equal(got_v[s], q2.assemble_vector(E, ev[s], nd)[rows]), s

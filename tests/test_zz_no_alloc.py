@@ -41,11 +41,22 @@ def _allocating(mesh, U, M, P, marker, f):
     return [o.cpu().numpy() for o in out]
 
 
-def test_noalloc_residual_matches_the_allocating_path_twice(cuda):
-    from hippymfem_b200 import BoxMesh, DirichletBC, Q2Space
+def _noalloc_call(mesh, U, M, P, f, marker, out, status):
     from hippymfem_b200._lib import check, lib, ptr, stream_ptr
 
-    mesh = BoxMesh((6, 5, 7), L=(1.0, 0.8, 1.2))
+    check(lib.hm_lattice_residual_noalloc(mesh.handle, ptr(U), ptr(M), ptr(P), f,
+                                          ptr(marker), ptr(out[0]), ptr(out[1]),
+                                          ptr(out[2]), 1, ptr(status), stream_ptr()),
+          "hm_lattice_residual_noalloc")
+
+
+@pytest.mark.parametrize("n,L", [((6, 5, 7), (1.0, 0.8, 1.2)),
+                                 ((16, 16, 32), (1.0, 1.0, 2.0))])   # exactly 8192 elements
+def test_noalloc_residual_matches_the_allocating_path_twice(cuda, n, L):
+    from hippymfem_b200 import BoxMesh, DirichletBC, Q2Space
+
+    mesh = BoxMesh(n, L=L)
+    assert mesh.ne <= 8192
     marker = DirichletBC(Q2Space(mesh)).marker
     nd = mesh.ndof
     for seed, f in ((1, 1.0), (2, -0.5)):
@@ -55,10 +66,7 @@ def test_noalloc_residual_matches_the_allocating_path_twice(cuda):
         out = [torch.full((nd,), float("nan"), dtype=torch.float64, device=cuda)
                for _ in range(3)]
         status = torch.zeros(1, dtype=torch.int32, device=cuda)
-        check(lib.hm_lattice_residual_noalloc(mesh.handle, ptr(U), ptr(M), ptr(P), f,
-                                              ptr(marker), ptr(out[0]), ptr(out[1]),
-                                              ptr(out[2]), 1, ptr(status), stream_ptr()),
-              "hm_lattice_residual_noalloc")
+        _noalloc_call(mesh, U, M, P, f, marker, out, status)
         torch.cuda.synchronize()
         assert int(status.item()) == 0
         ref = _allocating(mesh, U, M, P, marker, f)
@@ -66,6 +74,31 @@ def test_noalloc_residual_matches_the_allocating_path_twice(cuda):
             got = got.cpu().numpy()
             assert np.isfinite(got).all()
             assert np.abs(got - want).max() <= TOL * np.abs(want).max()
+
+
+def test_noalloc_call_takes_no_device_memory(cuda):
+    """Once the library's code and its fixed array are resident (a first call), a call
+    changes neither the device's free memory nor torch's allocations."""
+    from hippymfem_b200 import BoxMesh
+
+    mesh = BoxMesh((10, 9, 8))
+    nd = mesh.ndof
+    rng = np.random.default_rng(3)
+    U, M, P = (torch.as_tensor(rng.standard_normal(nd), device=cuda) for _ in range(3))
+    M = 0.2 * M
+    out = [torch.empty(nd, dtype=torch.float64, device=cuda) for _ in range(3)]
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    _noalloc_call(mesh, U, M, P, 1.0, None, out, status)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(3):
+        _noalloc_call(mesh, U, M, P, 1.0, None, out, status)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+    assert int(status.item()) == 0
 
 
 def test_noalloc_rejects_a_lattice_beyond_its_scratch(cuda):
