@@ -162,12 +162,20 @@ def assemble_slab(part, rank, u, m, p, ess, assembler, f=1.0, group=None):
 
 
 def hypre_arrays(part, rank, local_indptr, local_indices):
-    """The arrays the reference hands hypre for rank's rows (``fem/parmat.py:106-171``,
-    ``HypreParMatrix(comm, nrow, rglob, cglob, [I, J, D, rows])``): ``I`` the row
-    pointers of the owned rows from 0 (int32), ``J`` their global column indices (int64:
-    the local lattice's columns shifted by its first node plane), and ``rows`` the
-    partition ``[first row, last row + 1]``; ``D`` is the owned stretch that
-    ``assemble_slab`` returns.  Works on numpy arrays or tensors."""
+    """Rank's rows of the assembled global matrix as a row-partitioned ParCSR: ``I`` the
+    row pointers of the owned rows from 0 (int32), ``J`` their global column indices
+    (int64: the local lattice's columns shifted by its first node plane) and ``rows``
+    the partition ``[first row, last row + 1]``; the values ``D`` are the owned stretch
+    that ``assemble_slab`` returns.  These are the arguments of
+    ``mfem.HypreParMatrix(comm, nrow, rglob, cglob, [I, J, D, rows])``, but not what the
+    reference's ``local_par_matrix`` (``fem/parmat.py:106-171``) passes: there each rank
+    hands hypre a block-diagonal matrix over its own local dofs and the true-dof route
+    (``fem/tdofassemble.py``) forms ``P^T A P`` from it.  Here the rows are already the
+    assembled global rows (an owned row holds columns of the neighbouring slabs), in the
+    lattice's node numbering and partitioned by z-slab node planes, so the result replaces
+    the whole true-dof assembly, and the vectors it multiplies must use the same slab
+    partition and numbering (``SlabPartition.owned_global_rows``).  Works on numpy
+    arrays or tensors."""
     r0, r1 = part.owned_local_rows(rank)
     l0, _ = part.local_planes(rank)
     ip = local_indptr[r0:r1 + 1]
@@ -182,27 +190,41 @@ def hypre_arrays(part, rank, local_indptr, local_indices):
     return I, J, np.array([g0, g1], dtype=np.int64)
 
 
-def device_slab_assembler(n, L, u, m, p, ess, f=1.0):
-    """The fused CUDA assembly of a lattice (the tensors on its device)."""
+_SLAB_CACHE = {}
+
+
+def device_slab_assembler(n, L, u, m, p, ess, f=1.0, check_finite=True):
+    """The fused CUDA assembly of a lattice (the tensors on its device).  The mesh, its
+    pattern and the buffers are kept per (n, L, device), so a Newton loop assembles again
+    without rebuilding the pattern or allocating; the returned blocks and vectors are
+    those buffers, overwritten by the next call on the same lattice.  With
+    ``check_finite`` the status word is read (one synchronisation)."""
     from . import _lib
     from ._lib import check, lib, ptr, stream_ptr
     from .mesh import BoxMesh
     from .pattern import LatticePattern
 
     dev = u.device
-    mesh = BoxMesh(n, L, device=dev)
-    pat = LatticePattern(mesh, with_transpose=False)
-    quad = torch.empty(mesh.quad_bytes() // 8, dtype=torch.float64, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    key = (tuple(n), tuple(L), str(dev))
+    c = _SLAB_CACHE.get(key)
+    if c is None:
+        mesh = BoxMesh(n, L, device=dev)
+        c = _SLAB_CACHE[key] = {
+            "mesh": mesh, "pat": LatticePattern(mesh, with_transpose=False),
+            "quad": torch.empty(mesh.quad_bytes() // 8, dtype=torch.float64, device=dev),
+            "status": torch.zeros(1, dtype=torch.int32, device=dev),
+            "blocks": {k: torch.empty(mesh.nnz, dtype=torch.float64, device=dev) for k in BLOCKS},
+            "vecs": [torch.empty(mesh.ndof, dtype=torch.float64, device=dev) for _ in range(3)]}
+    mesh, pat, quad, status = c["mesh"], c["pat"], c["quad"], c["status"]
+    blocks, vecs = c["blocks"], c["vecs"]
     marker = ess.to(device=dev, dtype=torch.uint8).contiguous()
+    status.zero_()
     check(lib.hm_lattice_quadrature(mesh.handle, ptr(u), ptr(m), ptr(p), _lib.HM_FP64,
                                     ptr(quad), ptr(status), stream_ptr()), "hm_lattice_quadrature")
-    blocks = {k: torch.empty(mesh.nnz, dtype=torch.float64, device=dev) for k in BLOCKS}
-    vecs = [torch.empty(mesh.ndof, dtype=torch.float64, device=dev) for _ in range(3)]
     check(lib.hm_lattice_assemble(mesh.handle, ptr(quad), _lib.HM_FP64, ptr(pat.indptr),
                                   ptr(marker), float(f), *(ptr(blocks[k]) for k in BLOCKS),
                                   *(ptr(v) for v in vecs), 1, stream_ptr()), "hm_lattice_assemble")
-    if int(status.item()) != 0:
+    if check_finite and int(status.item()) != 0:
         raise RuntimeError("non-finite values in the fields")
     return pat.indptr, blocks, {0: vecs[0], 1: vecs[1], 2: vecs[2]}
 
