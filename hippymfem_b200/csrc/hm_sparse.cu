@@ -9,6 +9,7 @@
 #include <new>
 #include <cmath>
 #include <type_traits>
+#include <vector>
 
 #include "hm_common.cuh"
 #include "hm_internal.h"
@@ -889,4 +890,194 @@ extern "C" int hm_pcg_plan_solve(hm_pcg_plan* p, double rtol, double delta, int 
 extern "C" int hm_pcg_plan_destroy(hm_pcg_plan* p) {
   delete p;
   return HM_OK;
+}
+
+// ------------------------------------------------------------------- solve groups
+// Several FP64 solve plans of one lattice size solved together: every plan's iteration
+// batch is one branch of a single CUDA graph (one launch runs the batches of all
+// plans, concurrently on the device), and one host synchronisation per batch reads
+// every plan's convergence.  Each branch launches exactly the kernels its plan launches
+// alone, on its own buffers, and a converged plan's iterate is frozen (its step length
+// is zero), so every result is the one the plan gives solved alone, bit for bit.
+struct hm_pcg_group {
+  std::vector<hm_pcg_plan*> plans;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int check_every = 1;
+  ~hm_pcg_group() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    for (auto s : side) cudaStreamDestroy(s);
+  }
+};
+
+namespace {
+struct PlanBufs {
+  double *r, *z, *p, *q, *pq_part, *sc, *part;
+  unsigned* cnt;
+};
+PlanBufs plan_bufs(const hm_pcg_plan* pl) {
+  const int64_t n = pl->L.ndof;
+  double* w = static_cast<double*>(pl->work);
+  PlanBufs b;
+  b.r = w; b.z = w + n; b.p = w + 2 * n; b.q = w + 3 * n;
+  b.pq_part = w + 4 * n;
+  b.sc = b.pq_part + pq_slots(n);
+  b.part = b.sc + SC_N;
+  b.cnt = reinterpret_cast<unsigned*>(b.part + 3 * kReduceBlocks);
+  return b;
+}
+
+// a plan's solve up to its first convergence check (x from zero), as its own solve does
+int group_init(hm_pcg_plan* pl, double rtol, cudaStream_t s) {
+  const int64_t n = pl->L.ndof;
+  const PlanBufs B = plan_bufs(pl);
+  PcgOp o{n, nullptr, nullptr, nullptr, &pl->L, pl->jac64, HM_FP64, pl->ess};
+  if (cudaMemsetAsync(pl->x, 0, sizeof(double) * n, s) != cudaSuccess ||
+      cudaMemsetAsync(B.cnt, 0, 2 * sizeof(unsigned), s) != cudaSuccess)
+    return HM_ERR_CUDA;
+  int rc = hm_launch_ess_take_b(pl->L, o.ess, pl->b, pl->x, (void*)s);
+  if (rc) return rc;
+  int64_t np = 0;
+  if ((rc = op_apply(o, pl->x, B.q, nullptr, &np, (void*)s))) return rc;
+  if (pl->mg != nullptr) {
+    k_pcg_mg_init<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, pl->b, B.q, B.r, B.part);
+    if ((rc = hm_mg_vcycle(pl->mg, B.r, B.z, (void*)s))) return rc;
+    k_dot_partial_t<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.r, B.z, B.part);
+    k_pcg_init_final<<<1, 1024, 0, s>>>(B.part, B.sc, rtol);
+    if (cudaMemcpyAsync(B.p, B.z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return HM_ERR_CUDA;
+  } else {
+    k_pcg_init<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, pl->b, B.q, pl->diag, B.r, B.z,
+                                                               B.p, B.part);
+    k_pcg_init_final<<<1, 1024, 0, s>>>(B.part, B.sc, rtol);
+  }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+// `count` iterations of a plan, the same launches as its own solve's batches
+int group_batch(hm_pcg_plan* pl, int count, cudaStream_t s) {
+  const int64_t n = pl->L.ndof;
+  const PlanBufs B = plan_bufs(pl);
+  PcgOp o{n, nullptr, nullptr, nullptr, &pl->L, pl->jac64, HM_FP64, pl->ess};
+  if (pl->mg == nullptr)
+    return pcg_batch<double>(o, pl->diag, pl->x, B.r, B.z, B.p, B.q, B.pq_part, B.sc, B.part,
+                             B.cnt, count, s);
+  int64_t np = 0;
+  for (int j = 0; j < count; ++j) {
+    bool fused = false;
+    int e = op_apply(o, B.p, B.q, B.pq_part, &np, (void*)s, B.sc, B.cnt, &fused);
+    if (e) return e;
+    if (!fused) k_pcg_alpha<<<1, 1024, 0, s>>>(B.pq_part, np, B.sc);
+    k_pcg_update_rr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.sc, pl->x, B.r, B.p, B.q, B.part);
+    if ((e = hm_mg_vcycle(pl->mg, B.r, B.z, (void*)s))) return e;
+    k_pcg_rz_beta<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.r, B.z, B.part, B.cnt + 1, B.sc);
+    k_pcg_pupdate<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.sc, B.z, B.p);
+  }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" int hm_pcg_group_create(hm_pcg_plan** plans, int count, hm_pcg_group** out) {
+  if (!plans || count < 1 || count > 64 || !out) return HM_ERR_ARG;
+  for (int i = 0; i < count; ++i) {
+    if (!plans[i] || plans[i]->jac32 != nullptr) return HM_ERR_ARG;   // FP64 plans only
+    if (plans[i]->check_every != plans[0]->check_every) return HM_ERR_ARG;
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return HM_ERR_ARG;
+  }
+  hm_pcg_group* g = new (std::nothrow) hm_pcg_group();
+  if (!g) return HM_ERR_NOMEM;
+  g->plans.assign(plans, plans + count);
+  g->check_every = plans[0]->check_every;
+  if (cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming) != cudaSuccess) {
+    delete g;
+    return HM_ERR_CUDA;
+  }
+  for (int i = 0; i < count; ++i) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+      delete g;
+      return HM_ERR_CUDA;
+    }
+    g->side.push_back(st);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      delete g;
+      return HM_ERR_CUDA;
+    }
+    g->join.push_back(ev);
+  }
+  *out = g;
+  return HM_OK;
+}
+
+extern "C" int hm_pcg_group_destroy(hm_pcg_group* g) {
+  delete g;
+  return HM_OK;
+}
+
+extern "C" int hm_pcg_group_solve(hm_pcg_group* g, double rtol, int maxiter, int* iterations,
+                                  double* relres, void* stream) {
+  if (!g || maxiter < 0 || !(rtol >= 0.0)) return HM_ERR_ARG;
+  cudaStream_t s = S_(stream);
+  const int k = (int)g->plans.size();
+  int rc;
+  for (int i = 0; i < k; ++i)
+    if ((rc = group_init(g->plans[i], rtol, s))) return rc;
+  std::vector<double> host((size_t)k * SC_N);
+  int it = 0;
+  bool all = false;
+  for (;;) {
+    for (int i = 0; i < k; ++i)
+      if (cudaMemcpyAsync(&host[(size_t)i * SC_N], plan_bufs(g->plans[i]).sc, SC_N * sizeof(double),
+                          cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return HM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HM_ERR_CUDA;
+    all = true;
+    for (int i = 0; i < k; ++i) all = all && host[(size_t)i * SC_N + SC_CONV] >= 0.0;
+    if (all || it >= maxiter) break;
+    const int count = it + g->check_every < maxiter ? g->check_every : maxiter - it;
+    if (s == nullptr || count != g->check_every) {
+      for (int i = 0; i < k; ++i)
+        if ((rc = group_batch(g->plans[i], count, s))) return rc;
+    } else {
+      if (g->exec == nullptr) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HM_ERR_CUDA;
+        int crc = cudaEventRecord(g->fork, s) == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+        for (int i = 0; i < k && crc == HM_OK; ++i) {
+          if (cudaStreamWaitEvent(g->side[i], g->fork, 0) != cudaSuccess) { crc = HM_ERR_CUDA; break; }
+          crc = group_batch(g->plans[i], count, g->side[i]);
+          if (crc == HM_OK && (cudaEventRecord(g->join[i], g->side[i]) != cudaSuccess ||
+                               cudaStreamWaitEvent(s, g->join[i], 0) != cudaSuccess))
+            crc = HM_ERR_CUDA;
+        }
+        const cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (crc != HM_OK || e != cudaSuccess) {
+          if (graph) cudaGraphDestroy(graph);
+          (void)cudaGetLastError();
+          return crc != HM_OK ? crc : HM_ERR_CUDA;
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&g->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+          g->exec = nullptr;
+          return HM_ERR_CUDA;
+        }
+      }
+      if (cudaGraphLaunch(g->exec, s) != cudaSuccess) return HM_ERR_CUDA;
+    }
+    it += count;
+  }
+  for (int i = 0; i < k; ++i) {
+    const double* h = &host[(size_t)i * SC_N];
+    const bool conv = h[SC_CONV] >= 0.0;
+    if (iterations) iterations[i] = conv ? (int)h[SC_CONV] : it;
+    if (relres) relres[i] = h[SC_BB] > 0.0 ? std::sqrt(h[SC_RR] / h[SC_BB]) : 0.0;
+  }
+  return all ? HM_OK : HM_ERR_NOCONV;
 }

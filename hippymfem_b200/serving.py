@@ -45,7 +45,7 @@ from ._lib import check, lib, ptr, stream_ptr
 from .mesh import BoxMesh, DirichletBC, Q2Space
 from .modeling import DiscreteStateObservation, PointwiseStateObservation
 from .problem import STATE
-from .sparse import SolvePlan
+from .sparse import SolveGroup, SolvePlan
 from .synthetic import field_params, interior_points
 
 
@@ -147,37 +147,36 @@ class _Workspace:
                                       ptr(state), ptr(param), ptr(adj), int(bool(zero_ess)),
                                       stream_ptr()), "hm_lattice_assemble")
 
-    def _solve(self, out, rhs, req):
-        self.plan.solve(out, rhs)
-        req.iterations.append(self.plan.last.iterations)
-
-    def forward(self, m, req):
+    # A request's work as a generator: it yields each solve it needs as (out, rhs) and
+    # is resumed once out holds A^{-1} rhs, so that the solves of several same-size
+    # requests can run as one group (SolveGroup); its return value is the result.
+    def forward_steps(self, m, req):
         v = self.vec
         z = v["zero"]
         self._quad(self.quad, z, m, z)
         self.plan.set_point(self.quad)
         self._vectors(self.quad, 1.0, adj=self.plan.b, zero_ess=True)
         self.plan.b.neg_()
-        self._solve(v["u"], self.plan.b, req)
+        yield v["u"], self.plan.b
         return v["u"]
 
-    def hessian(self, m, x, req):
+    def hessian_steps(self, m, x, req):
         v, mask, mis = self.vec, self.ms.bc.mask, self.misfit
-        u = self.forward(m, req)
+        u = yield from self.forward_steps(m, req)
         # adjoint: A^T p = -B^T (B u - d) / sigma^2
         mis.grad(STATE, [u, m, None], v["r1"])
         v["r1"].neg_().masked_fill_(mask, 0.0)
-        self._solve(v["p"], v["r1"], req)
+        yield v["p"], v["r1"]
         p = v["p"]
         # C x, W_um x, W_mm x from one directional pass (f = 0)
         self._quad(self.quad2, u, m, p, mhat=x)
         self._vectors(self.quad2, 0.0, state=v["r2"], param=v["y"], adj=v["r1"])
         v["r1"].masked_fill_(mask, 0.0)                       # C x, rows eliminated
         v["r2"].masked_fill_(mask, 0.0)                       # W_um x
-        self._solve(v["uh"], v["r1"], req)                    # A u^ = C x
+        yield v["uh"], v["r1"]                                # A u^ = C x
         mis.apply_ij(STATE, STATE, v["uh"], v["r3"])          # W_uu u^
         v["r3"].sub_(v["r2"]).masked_fill_(mask, 0.0)
-        self._solve(v["ph"], v["r3"], req)                    # A^T p^ = W_uu u^ - W_um x
+        yield v["ph"], v["r3"]                                # A^T p^ = W_uu u^ - W_um x
         # y = W_mm x + C^T p^ - W_mu u^
         self._quad(self.quad2, u, m, v["ph"].masked_fill_(mask, 0.0))
         self._vectors(self.quad2, 0.0, param=v["r3"])
@@ -186,6 +185,29 @@ class _Workspace:
         self._vectors(self.quad2, 0.0, param=v["r3"])
         v["y"].sub_(v["r3"])
         return v["y"]
+
+    def steps(self, req):
+        ms = self.ms
+        m = ms.field(req.seed)
+        if req.kind == "forward":
+            return self.forward_steps(m, req)
+        return self.hessian_steps(m, ms.direction(req.seed), req)
+
+    def _drive(self, gen, req):
+        try:
+            out, rhs = next(gen)
+            while True:
+                self.plan.solve(out, rhs)
+                req.iterations.append(self.plan.last.iterations)
+                out, rhs = gen.send(None)
+        except StopIteration as stop:
+            return stop.value
+
+    def forward(self, m, req):
+        return self._drive(self.forward_steps(m, req), req)
+
+    def hessian(self, m, x, req):
+        return self._drive(self.hessian_steps(m, x, req), req)
 
     def close(self):
         self.plan.close()
@@ -201,7 +223,8 @@ class Server:
     device memory)."""
 
     def __init__(self, slots=4, precision="mixed", rel_tolerance=1e-8, memory_budget=None,
-                 device=None, check_every=None, keep_results=True, multigrid=False):
+                 device=None, check_every=None, keep_results=True, multigrid=False,
+                 group_size=1):
         if multigrid and precision != "fp64":
             raise ValueError("the multigrid solves are FP64")
         self.multigrid = bool(multigrid)
@@ -217,6 +240,11 @@ class Server:
         self.keep_results = keep_results
         self.meshes = {}
         self.tuned = {}
+        # same-size batching (FP64 solves only): a slot takes up to group_size waiting
+        # requests of one size and kind and runs their solves as one group
+        self.group_size = max(1, int(group_size))
+        self.group_by_n = {}
+        self._groups = {}
         self._ws = {}            # (slot, n) -> _Workspace
         self._resident = 0
         self.peak_resident = 0
@@ -238,9 +266,16 @@ class Server:
             return int(self.fixed_check_every)
         return self.tuned.get(n, 16)
 
-    def autotune(self, sizes, candidates=(4, 8, 16, 32), reps=3):
+    def group_size_for(self, n):
+        if self.precision != "fp64":
+            return 1
+        return int(self.group_by_n.get(n, self.group_size))
+
+    def autotune(self, sizes, candidates=(4, 8, 16, 32), reps=3, group_candidates=()):
         """Pick the graph batch length per mesh size: the fastest forward solve (CUDA
-        events, in a side stream, after one warm-up that captures the graph)."""
+        events, in a side stream, after one warm-up that captures the graph).  With
+        ``group_candidates`` (FP64 servers) also the group size: the one whose grouped
+        forward requests take the least time per request."""
         stream = torch.cuda.Stream(device=self.device)
         for n in sizes:
             ms = self.mesh_state(n)
@@ -263,16 +298,81 @@ class Server:
                 if best is None or t < best[0]:
                     best = (t, ce)
             self.tuned[n] = best[1]
+            if group_candidates and self.precision == "fp64":
+                self.group_by_n[n] = self._tune_group(ms, best[1], group_candidates, reps,
+                                                      stream)
         return dict(self.tuned)
 
+    def _tune_group(self, ms, ce, group_candidates, reps, stream):
+        best = None
+        for k in group_candidates:
+            wss = [_Workspace(ms, self.precision, self.rtol, ce, self.multigrid)
+                   for _ in range(int(k))]
+            reqs = [Request("forward", ms.n, j) for j in range(int(k))]
+            grp = SolveGroup([w.plan for w in wss]) if k > 1 else None
+            with torch.cuda.stream(stream):
+                self._run_group_with(wss, reqs, grp)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    self._run_group_with(wss, reqs, grp)
+                e1.record(stream)
+            stream.synchronize()
+            t = e0.elapsed_time(e1) / (reps * int(k))
+            if grp is not None:
+                grp.close()
+            for w in wss:
+                w.close()
+            if best is None or t < best[0]:
+                best = (t, int(k))
+        return best[1]
+
+    def _run_group_with(self, wss, reqs, grp):
+        """The requests' work on their workspaces (one each): alone through the
+        workspace's own solves, or with every solve of the group as one SolveGroup."""
+        gens = [w.steps(r) for w, r in zip(wss, reqs)]
+        if grp is None:
+            return [wss[0]._drive(gens[0], reqs[0])]
+        cur = [next(g) for g in gens]
+        results = [None] * len(gens)
+        while True:
+            res = grp.solve([c[0] for c in cur], [c[1] for c in cur])
+            for r, pr in zip(reqs, res):
+                r.iterations.append(pr.iterations)
+            nxt = []
+            for j, g in enumerate(gens):
+                try:
+                    nxt.append(g.send(None))
+                except StopIteration as stop:
+                    results[j] = stop.value
+                    nxt.append(None)
+            if all(x is None for x in nxt):
+                return results
+            if any(x is None for x in nxt):
+                raise RuntimeError("the requests of a group took different numbers of solves")
+            cur = nxt
+
+    def _group(self, wss):
+        key = tuple(id(w) for w in wss)
+        grp = self._groups.get(key)
+        if grp is None:
+            grp = self._groups[key] = SolveGroup([w.plan for w in wss])
+        return grp
+
+    def _drop_groups(self, ws):
+        for key in [k for k in self._groups if id(ws) in k]:
+            self._groups.pop(key).close()
+
     # -- admission -------------------------------------------------------------------
-    def _acquire(self, slot, n):
-        """The slot's workspace for size n, created (and room made) when missing; blocks
-        while the budget has no room.  Under the lock."""
-        ws = self._ws.get((slot, n))
+    def _acquire(self, slot, n, j=0, block=True):
+        """The slot's j-th workspace for size n, ``(ws, None, True)``; when missing,
+        room is made for it (idle workspaces released, least recently used first) and
+        ``(None, bytes reserved, True)`` returned.  Without room it waits for some
+        (``block``) or returns ``(None, None, False)``.  Under the lock."""
+        ws = self._ws.get((slot, n, j))
         if ws is not None:
             ws.in_use = True
-            return ws, None
+            return ws, None, True
         need = self.mesh_state_locked(n).footprint(self.precision, self.multigrid)
         while self._resident + need > self.budget:
             idle = [(w.last_used, k) for k, w in self._ws.items() if not w.in_use]
@@ -280,15 +380,18 @@ class Server:
                 _, k = min(idle)
                 w = self._ws.pop(k)
                 self._resident -= w.nbytes
+                self._drop_groups(w)
                 w.close()
                 continue
+            if not block:
+                return None, None, False
             if self._resident == 0:
                 raise MemoryError("a workspace for n=%d needs %d bytes, more than the budget"
                                   % (n, need))
             self._lock.wait()
         self._resident += need
         self.peak_resident = max(self.peak_resident, self._resident)
-        return None, need
+        return None, need, True
 
     def mesh_state_locked(self, n):
         ms = self.meshes.get(n)
@@ -309,32 +412,56 @@ class Server:
                 if not pending:
                     return
                 req = pending.popleft()
-                ws, reserved = self._acquire(slot, req.n)
-            if ws is None:
-                ms = self.mesh_state(req.n)
-                with torch.cuda.stream(stream):
-                    ws = _Workspace(ms, self.precision, self.rtol, self.check_every(req.n),
-                                    self.multigrid)
-                ws.nbytes = reserved
-                ws.in_use = True
-                with self._lock:
-                    self._ws[(slot, req.n)] = ws
-            req.t_admit = time.perf_counter() - t0
-            req.slot = slot
-            ms = ws.ms
+                # the oldest request, and (FP64) up to group_size - 1 more of its size and
+                # kind that are waiting, taken in arrival order
+                group = [req]
+                kmax = self.group_size_for(req.n)
+                if kmax > 1:
+                    for other in pending:
+                        if len(group) >= kmax:
+                            break
+                        if other.n == req.n and other.kind == req.kind:
+                            group.append(other)
+                    for other in group[1:]:
+                        pending.remove(other)
+                got = []
+                for j, r in enumerate(group):
+                    ws, reserved, ok = self._acquire(slot, r.n, j, block=j == 0)
+                    if not ok:                    # no room for more: the rest waits
+                        for r2 in reversed(group[j:]):
+                            pending.appendleft(r2)
+                        group = group[:j]
+                        break
+                    got.append((ws, reserved))
+            wss = []
+            for j, (ws, reserved) in enumerate(got):
+                if ws is None:
+                    ms = self.mesh_state(req.n)
+                    with torch.cuda.stream(stream):
+                        ws = _Workspace(ms, self.precision, self.rtol, self.check_every(req.n),
+                                        self.multigrid)
+                    ws.nbytes = reserved
+                    ws.in_use = True
+                    with self._lock:
+                        self._ws[(slot, req.n, j)] = ws
+                wss.append(ws)
+            t_admit = time.perf_counter() - t0
+            for r in group:
+                r.t_admit, r.slot = t_admit, slot
             with torch.cuda.stream(stream):
-                m = ms.field(req.seed)
-                if req.kind == "forward":
-                    out = ws.forward(m, req)
-                else:
-                    out = ws.hessian(m, ms.direction(req.seed), req)
-                res = out.to("cpu", non_blocking=False) if self.keep_results else None
+                grp = self._group(wss) if len(wss) > 1 else None
+                outs = self._run_group_with(wss, group, grp)
+                res = [o.to("cpu", non_blocking=False) if self.keep_results else None
+                       for o in outs]
                 stream.synchronize()
-            req.result = res.numpy() if res is not None else None
-            req.t_done = time.perf_counter() - t0
+            t_done = time.perf_counter() - t0
+            for r, x in zip(group, res):
+                r.result = x.numpy() if x is not None else None
+                r.t_done = t_done
             with self._lock:
-                ws.in_use = False
-                ws.last_used = req.t_done
+                for ws in wss:
+                    ws.in_use = False
+                    ws.last_used = t_done
                 self._lock.notify_all()
 
     def run(self, requests):
@@ -383,6 +510,9 @@ class Server:
 
     def close(self):
         with self._lock:
+            for g in self._groups.values():
+                g.close()
+            self._groups.clear()
             for w in self._ws.values():
                 w.close()
             self._ws.clear()

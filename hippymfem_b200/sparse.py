@@ -293,6 +293,60 @@ class SolvePlan:
             pass
 
 
+class SolveGroup:
+    """Several FP64 ``SolvePlan``s of one lattice size solved together
+    (``hm_pcg_group_*``): each full batch of iterations of all plans is one CUDA graph,
+    one branch per plan, and one host synchronisation per batch checks them all.  Every
+    solution is bit for bit the plan's own solve's.  The plans' tolerances and iteration
+    limits are taken from the first plan."""
+
+    def __init__(self, plans):
+        if not plans:
+            raise ValueError("a solve group needs at least one plan")
+        if any(p.jac32 is not None for p in plans):
+            raise ValueError("solve groups take FP64 plans")
+        self.plans = list(plans)
+        arr = (ctypes.c_void_p * len(plans))(*[p._plan.value for p in plans])
+        self._g = ctypes.c_void_p()
+        check(lib.hm_pcg_group_create(arr, len(plans), ctypes.byref(self._g)),
+              "hm_pcg_group_create")
+        self.last = None
+
+    def solve(self, outs, rhss, stream=None):
+        """``outs[i] = A_i^{-1} rhss[i]`` for plan i (right-hand sides zero on the
+        Dirichlet nodes); returns the per-plan ``PCGResult``s."""
+        k = len(self.plans)
+        if len(outs) != k or len(rhss) != k:
+            raise ValueError("one right-hand side and one output per plan")
+        for p, rhs in zip(self.plans, rhss):
+            if rhs is not p.b:
+                p.b.copy_(rhs)
+        prm = self.plans[0].parameters
+        its = (ctypes.c_int * k)()
+        rr = (ctypes.c_double * k)()
+        rc = lib.hm_pcg_group_solve(self._g, prm["rel_tolerance"], prm["max_iter"], its, rr,
+                                    stream_ptr(stream))
+        self.last = [PCGResult(its[i], rr[i], rc == _lib.HM_OK) for i in range(k)]
+        for i, p in enumerate(self.plans):
+            p.last = self.last[i]
+        check(rc, "hm_pcg_group_solve")
+        for p, out in zip(self.plans, outs):
+            if out is not None and out is not p.x:
+                out.copy_(p.x)
+        return self.last
+
+    def close(self):
+        if self._g:
+            lib.hm_pcg_group_destroy(self._g)
+            self._g = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:                                   # noqa: BLE001
+            pass
+
+
 def default_smoothing_degree(mesh):
     """Chebyshev degree of the smoother when the caller gives none: 1 from a million dofs
     up, 2 below.  Measured on a B200 (FP64 multigrid-PCG to rtol 1e-12): at 64^3 degree 1

@@ -309,6 +309,23 @@ int hm_pcg_plan_solve(hm_pcg_plan* plan, double rtol, double delta, int max_upda
                       int maxiter, int* iterations, int* updates, double* relres, void* stream);
 int hm_pcg_plan_destroy(hm_pcg_plan* plan);
 
+/* A solve group: FP64 solve plans (Jacobi or multigrid; the same check_every) solved
+ * together, for a request loop that has several same-size solves ready at once -- the
+ * batched counterpart of one plan's solve.  Each plan's right-hand side is its d_b, its
+ * solution lands in its d_x (from zero, as hm_pcg_plan_solve).  Every full batch of
+ * iterations of all plans is one CUDA graph (captured on the first group solve in a
+ * stream other than the legacy default stream, each plan a branch of its own), and one
+ * host synchronisation per batch reads all plans' convergence.  A plan that has
+ * converged stops moving (its step lengths are zero), so each solution is bit for bit
+ * the one its plan gives solved alone.  iterations / relres: one per plan.  The plans
+ * may not be used elsewhere while the group solves; HM_ERR_NOCONV if any plan ends at
+ * maxiter. */
+typedef struct hm_pcg_group hm_pcg_group;
+int hm_pcg_group_create(hm_pcg_plan** plans, int count, hm_pcg_group** group);
+int hm_pcg_group_solve(hm_pcg_group* group, double rtol, int maxiter, int* iterations,
+                       double* relres, void* stream);
+int hm_pcg_group_destroy(hm_pcg_group* group);
+
 /* Geometric multigrid preconditioner for the lattice Jacobian, the structured-lattice
  * counterpart of the BoomerAMG preconditioner of the reference's solves
  * (algorithms/linSolvers.py:243-828): a symmetric V-cycle Q2 -> Q1 on the same elements

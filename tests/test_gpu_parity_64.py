@@ -127,7 +127,7 @@ def test_properties_over_all_rows_at_64_cubed(bench64):
     rowsum = torch.zeros(mesh.ndof, dtype=torch.float64, device=dev).index_add_(0, row_of, A)
     scale = A.abs().max()
     free = ~touches
-    assert int(free.sum()) > 0.9 * mesh.ndof
+    assert int(free.sum()) > 0.8 * mesh.ndof
     assert float(rowsum[free].abs().max() / scale) <= 1e-13
     tpos = pat.tpos.long()
     for b in ("A", "Wmm"):

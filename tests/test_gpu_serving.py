@@ -72,3 +72,46 @@ def test_admission_keeps_workspaces_within_the_budget(cuda):
     assert all(r.result is not None for r in reqs)
     assert srv.peak_resident <= budget
     srv.close()
+
+
+@pytest.mark.parametrize("multigrid", [True, False])
+def test_grouped_solves_equal_each_request_alone(cuda, multigrid):
+    """Same-size requests whose solves run as one group (SolveGroup: one CUDA graph per
+    batch of iterations, a branch per request) give each request's result and iteration
+    counts bit for bit as its solves alone; so does the server with groups."""
+    import torch
+
+    from hippymfem_b200.serving import Request, Server, _Workspace
+    from hippymfem_b200.sparse import SolveGroup
+
+    srv = Server(slots=1, precision="fp64", multigrid=multigrid, check_every=4, group_size=4)
+    ms = srv.mesh_state(12)
+    stream = torch.cuda.Stream()
+    for kind in ("forward", "hessian"):
+        wss = [_Workspace(ms, "fp64", 1e-8, 4, multigrid) for _ in range(3)]
+        reqs = [Request(kind, 12, 700 + j) for j in range(3)]
+        grp = SolveGroup([w.plan for w in wss])
+        with torch.cuda.stream(stream):
+            outs = [o.clone() for o in srv._run_group_with(wss, reqs, grp)]
+            again = [o.clone() for o in srv._run_group_with(wss, reqs, grp)]   # graph replayed
+        stream.synchronize()
+        solo = _Workspace(ms, "fp64", 1e-8, 4, multigrid)
+        for r, o, o2 in zip(reqs, outs, again):
+            ra = Request(kind, 12, r.seed)
+            with torch.cuda.stream(stream):
+                a = srv._run_group_with([solo], [ra], None)[0].clone()
+            stream.synchronize()
+            assert torch.equal(o, a) and torch.equal(o2, a), (kind, r.seed)
+            assert r.iterations[:len(ra.iterations)] == ra.iterations
+        grp.close()
+        for w in wss + [solo]:
+            w.close()
+    reqs = [Request("forward", 12, 800 + i, 0.0) for i in range(5)] + \
+        [Request("hessian", 8, 900 + i, 0.0) for i in range(3)]
+    srv.run(reqs)
+    alone = Server(slots=1, precision="fp64", multigrid=multigrid, check_every=4)
+    for r in reqs:
+        (a,) = alone.run([Request(r.kind, r.n, r.seed, 0.0)])
+        assert np.array_equal(r.result, a.result) and r.iterations == a.iterations
+    srv.close()
+    alone.close()

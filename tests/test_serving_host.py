@@ -39,20 +39,24 @@ def _server(budget, sizes):
     s.multigrid = False
     s.meshes = {n: _FakeMesh(b) for n, b in sizes.items()}
     s._ws = {}
+    s._groups = {}
     s._resident = 0
     s.peak_resident = 0
     s._lock = threading.Condition()
     return s
 
 
-def _admit(s, slot, n):
-    """As the worker does: reserve, then register a new workspace of the reserved size."""
+def _admit(s, slot, n, j=0, block=True):
+    """As the worker does: reserve, then register a new workspace of the reserved size
+    (the slot's j-th for size n: the members of a same-size group)."""
     with s._lock:
-        ws, reserved = s._acquire(slot, n)
+        ws, reserved, ok = s._acquire(slot, n, j, block=block)
+        if not ok:
+            return None, None
         if ws is None:
             ws = _FakeWorkspace(reserved)
             ws.in_use = True
-            s._ws[(slot, n)] = ws
+            s._ws[(slot, n, j)] = ws
     return ws, reserved
 
 
@@ -84,7 +88,7 @@ def test_idle_workspaces_are_evicted_least_recently_used_first():
     _release(s, w16, 3.0)                      # most recent
     _admit(s, 3, 24)                           # needs 60 of 100 with 90 resident: two go
     assert w12.closed and w8.closed and not w16.closed
-    assert set(s._ws) == {(2, 16), (3, 24)}
+    assert set(s._ws) == {(2, 16, 0), (3, 24, 0)}
     assert s._resident == 90
 
 
@@ -134,3 +138,17 @@ def test_poisson_trace_and_latency_stats():
     assert st["n"] == 100
     assert st["p50_ms"] == pytest.approx(50.5, rel=1e-9)
     assert st["requests_per_s"] == pytest.approx(100 / (0.99 + 0.1))
+
+
+def test_group_members_take_room_only_when_there_is_some():
+    """A group's further workspaces never wait for room: without it the member request
+    goes back to the queue; with it, each member has its own workspace."""
+    s = _server(100, {8: 40})
+    a, _ = _admit(s, 0, 8, 0)
+    b, _ = _admit(s, 0, 8, 1, block=False)
+    assert b is not None and b is not a and s._resident == 80
+    c, _ = _admit(s, 0, 8, 2, block=False)       # 120 > 100, nothing idle
+    assert c is None and s._resident == 80
+    _release(s, b, 1.0)
+    c, _ = _admit(s, 0, 8, 2, block=False)       # the idle member makes room
+    assert c is not None and b.closed and s._resident == 80
