@@ -44,10 +44,11 @@ int hm_launch_ess_take_b(const hm::Lattice& L, const uint8_t* ess, const double*
 // the right-hand side and solution buffers a solve plan was created with
 int hm_plan_buffers(const hm_pcg_plan* plan, double** b, double** x);
 // one Chebyshev-Jacobi step of degree 1 of the multigrid smoother on the lattice
-// operator, fused with the operator pass: from zero (x = b / (theta diag), r = b - A x)
-// or from x (x += (b - A x) / (theta diag)); theta = cheb[0]
+// operator, fused with the operator pass: from zero (x = b idiag / theta, r = b - A x)
+// or from x (x += (b - A x) idiag / theta); theta = cheb[0], idiag the reciprocal of the
+// Jacobi diagonal
 int hm_launch_cheb1_from_zero(const hm::Lattice& L, void* jac, const uint8_t* ess, const double* b,
-                              const double* diag, const double* cheb, double* x, double* r,
+                              const double* idiag, const double* cheb, double* x, double* r,
                               void* stream);
 int hm_launch_cheb1_from_x(const hm::Lattice& L, void* jac, const uint8_t* ess, const double* b,
-                           const double* diag, const double* cheb, double* x, void* stream);
+                           const double* idiag, const double* cheb, double* x, void* stream);

@@ -229,8 +229,8 @@ __device__ __forceinline__ real dbq_rt(int q, int a) {
 
 // ESS: zero x on the Dirichlet nodes on the fly (callers whose x is already zero there
 // -- every vector inside the lattice solves -- skip the markers).  CHEB: the input is the
-// first Chebyshev direction d = b / (theta diag) of a smoother started from zero,
-// formed on the fly from b (xin), the Jacobi diagonal and theta = cheb[0].
+// first Chebyshev direction d = b idiag / theta of a smoother started from zero, formed
+// on the fly from b (xin), the reciprocal Jacobi diagonal (cdiag) and theta = cheb[0].
 template <typename real, typename vec, bool ESS = true, bool CHEB = false>
 __global__ void __launch_bounds__(256, 2)
     k_elem_apply(Lattice L, const real* __restrict__ Dq, const uint8_t* __restrict__ ess,
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256, 2)
       const unsigned n = n0 + (unsigned)(i % 3) + nsy * (unsigned)(i / 3) + nsz * (unsigned)a3;
       real xv = (real)0;
       if (live) {
-        if constexpr (CHEB) xv = (real)(inv_theta * (double)__ldg(xin + n) / __ldg(cdiag + n));
+        if constexpr (CHEB) xv = (real)__dmul_rn(inv_theta * (double)__ldg(xin + n), __ldg(cdiag + n));
         else xv = (real)__ldg(xin + n);
       }
       const bool fixed = ESS && ess != nullptr && live && __ldg(ess + n) != 0;
@@ -352,11 +352,12 @@ __device__ __forceinline__ void axis_elems(int i, int nel, int& e0, int& a0, int
 }
 
 // OUT selects what is written for each node's product y (FP64 only for OUT != 0), with
-// c.b the smoother's right-hand side, c.diag the Jacobi diagonal, theta = c.cheb[0]:
+// c.b the smoother's right-hand side, c.diag the reciprocal of the Jacobi diagonal,
+// theta = c.cheb[0]:
 //   0  yout = y
-//   1  the first smoothing step from zero (the input was d = b / (theta diag)):
+//   1  the first smoothing step from zero (the input was d = b c.diag / theta):
 //      c.r = b - y, c.x = d
-//   2  one smoothing step from c.x (the input): c.x += (b - y) / (theta diag), in place
+//   2  one smoothing step from c.x (the input): c.x += (b - y) c.diag / theta, in place
 //      (this pass reads no x but the Dirichlet nodes' own)
 struct ChebOut {
   const double* b;
@@ -388,16 +389,34 @@ __global__ void __launch_bounds__(256)
     const unsigned ne = (unsigned)L.ne, nx = (unsigned)L.nx;
     const bool f0 = ess != nullptr && ess[n0];
     const bool f1 = !last && ess != nullptr && ess[n0 + 1];
-    real acc0 = 0, acc1 = 0;
-    for (int c3 = 0; c3 < cz; ++c3)
-      for (int c2 = 0; c2 < cy; ++c2) {
+    // every contribution is loaded before any is added (all twelve loads in flight at
+    // once), then summed in the fixed order (z, y element pairs, lower element first)
+    real v[4][3];
+#pragma unroll
+    for (int c3 = 0; c3 < 2; ++c3)
+#pragma unroll
+      for (int c2 = 0; c2 < 2; ++c2) {
+        const int c = 2 * c3 + c2;
+        const bool on = c3 < cz && c2 < cy;
         const unsigned a23 = 3u * (unsigned)(c2 ? 0 : ay0) + 9u * (unsigned)(c3 ? 0 : az0);
         const unsigned erow = nx * ((unsigned)(ey0 + c2) + (unsigned)L.ny * (unsigned)(ez0 + c3));
         // node 2m: element m-1 (a1 = 2) then element m (a1 = 0); node 2m+1: element m
-        if (m > 0) acc0 += Ye[(size_t)(2u + a23) * ne + erow + m - 1u];
-        if (!last) {
-          acc0 += Ye[(size_t)a23 * ne + erow + m];
-          acc1 += Ye[(size_t)(1u + a23) * ne + erow + m];
+        v[c][0] = (on && m > 0) ? Ye[(size_t)(2u + a23) * ne + erow + m - 1u] : (real)0;
+        v[c][1] = (on && !last) ? Ye[(size_t)a23 * ne + erow + m] : (real)0;
+        v[c][2] = (on && !last) ? Ye[(size_t)(1u + a23) * ne + erow + m] : (real)0;
+      }
+    real acc0 = 0, acc1 = 0;
+#pragma unroll
+    for (int c3 = 0; c3 < 2; ++c3)
+#pragma unroll
+      for (int c2 = 0; c2 < 2; ++c2) {
+        const int c = 2 * c3 + c2;
+        if (c3 < cz && c2 < cy) {
+          if (m > 0) acc0 += v[c][0];
+          if (!last) {
+            acc0 += v[c][1];
+            acc1 += v[c][2];
+          }
         }
       }
     if constexpr (OUT == 0) {
@@ -419,14 +438,15 @@ __global__ void __launch_bounds__(256)
         const double acc = (double)(h ? acc1 : acc0);
         const double bn = c.b[nn];
         if constexpr (OUT == 1) {
-          const double d = inv_theta * bn / c.diag[nn];
+          const double d = __dmul_rn(inv_theta * bn, c.diag[nn]);
           const double y = fx ? d : acc;
           c.r[nn] = bn - y;
           c.x[nn] = d;
         } else {
           const double xn = c.x[nn];
           const double y = fx ? xn : acc;
-          c.x[nn] = xn + inv_theta * (bn - y) / c.diag[nn];
+          // the update rounded on its own before the add, as the step-by-step smoother
+          c.x[nn] = xn + __dmul_rn(inv_theta * (bn - y), c.diag[nn]);
         }
       }
     }
@@ -559,29 +579,30 @@ static int launch_apply_t(const Lattice& L, void* jac, const uint8_t* ess, const
 
 // One Chebyshev-Jacobi smoothing step of degree 1 on the lattice operator (FP64, every
 // vector zero on the Dirichlet nodes), the operator pass and the vector update fused:
-//   from zero:  x = d = b / (theta diag),  r = b - A d          (pre-smoothing)
-//   from x:     x += (b - A x) / (theta diag)                   (post-smoothing)
+//   from zero:  x = d = b idiag / theta,  r = b - A d          (pre-smoothing)
+//   from x:     x += (b - A x) idiag / theta                   (post-smoothing)
+// (idiag: the reciprocal of the Jacobi diagonal)
 // the same arithmetic as the start / step / finish kernels of the multigrid smoother.
 int hm_launch_cheb1_from_zero(const Lattice& L, void* jac, const uint8_t* ess, const double* b,
-                              const double* diag, const double* cheb, double* x, double* r,
+                              const double* idiag, const double* cheb, double* x, double* r,
                               void* stream) {
   double* Dq = static_cast<double*>(jac);
   double* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
   k_elem_apply<double, double, false, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(
-      L, Dq, ess, b, Ye, diag, cheb);
-  ChebOut c{b, diag, cheb, r, x};
+      L, Dq, ess, b, Ye, idiag, cheb);
+  ChebOut c{b, idiag, cheb, r, x};
   k_node_gather<double, double, 1><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
 int hm_launch_cheb1_from_x(const Lattice& L, void* jac, const uint8_t* ess, const double* b,
-                           const double* diag, const double* cheb, double* x, void* stream) {
+                           const double* idiag, const double* cheb, double* x, void* stream) {
   double* Dq = static_cast<double*>(jac);
   double* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
   k_elem_apply<double, double, false><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
-  ChebOut c{b, diag, cheb, nullptr, x};
+  ChebOut c{b, idiag, cheb, nullptr, x};
   k_node_gather<double, double, 2><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;

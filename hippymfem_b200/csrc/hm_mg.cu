@@ -33,6 +33,7 @@ struct MGLevel {
   int64_t nodes, elems;
   double* coef;          // per element (levels >= 1)
   double* diag;          // Jacobi diagonal (level 0: the caller's)
+  double* idiag;         // its reciprocal, by which the smoothers multiply
   double *x, *b, *r, *d, *t;
   double* cheb;          // Chebyshev on the device: [0] theta (d0 = r / (theta diag)),
                          // [1 + k] c1_k, [1 + kChebMax + k] c2_k (d = c1 d + c2 r / diag)
@@ -121,15 +122,17 @@ __device__ __forceinline__ double q1_apply_at(const MGLevel& lv, const double* _
 }
 // A Chebyshev-Jacobi step of degree 1 of a Q1 level with its operator pass (the same
 // arithmetic as k_cheb_start / k_cheb_step / k_cheb_finish around k_q1_apply):
-//   from zero (pre-smoothing):  x = d = b / (theta diag),  r = b - A d
-//   from xin (post-smoothing):  xout = xin + (b - A xin) / (theta diag)   (xout != xin)
+//   from zero (pre-smoothing):  x = d = b idiag / theta,  r = b - A d
+//   from xin (post-smoothing):  xout = xin + (b - A xin) idiag / theta   (xout != xin)
 __global__ void __launch_bounds__(256) k_q1_cheb1_from_zero(MGLevel lv, const double* __restrict__ b) {
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= lv.nodes) return;
   const double inv_theta = 1.0 / lv.cheb[0];
-  const double* __restrict__ diag = lv.diag;
-  const double t = q1_apply_with(lv, n, [&](int64_t m) { return inv_theta * b[m] / diag[m]; });
-  lv.x[n] = inv_theta * b[n] / diag[n];
+  const double* __restrict__ idiag = lv.idiag;
+  // the products rounded on their own (__dmul_rn), as the step-by-step kernels store them,
+  // so that no multiply-add contraction changes a bit
+  const double t = q1_apply_with(lv, n, [&](int64_t m) { return __dmul_rn(inv_theta * b[m], idiag[m]); });
+  lv.x[n] = __dmul_rn(inv_theta * b[n], idiag[n]);
   lv.r[n] = b[n] - t;
 }
 __global__ void __launch_bounds__(256) k_q1_cheb1_from_x(MGLevel lv, const double* __restrict__ b,
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(256) k_q1_cheb1_from_x(MGLevel lv, const doubl
   if (n >= lv.nodes) return;
   const double inv_theta = 1.0 / lv.cheb[0];
   const double t = q1_apply_at(lv, xin, n);
-  xout[n] = xin[n] + inv_theta * (b[n] - t) / lv.diag[n];
+  xout[n] = xin[n] + __dmul_rn(inv_theta * (b[n] - t), lv.idiag[n]);
 }
 __global__ void __launch_bounds__(256) k_q1_apply(MGLevel lv, const double* __restrict__ x,
                                                   double* __restrict__ y) {
@@ -174,6 +177,11 @@ __global__ void k_coef_from_q2(int64_t ne, const double* __restrict__ Dq, double
 #pragma unroll
   for (int q = 0; q < 27; ++q) s += Dq[(int64_t)q * ne + e];
   coef[e] = s * inv_vol;
+}
+
+__global__ void k_recip(int64_t n, const double* __restrict__ a, double* __restrict__ ia) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) ia[i] = 1.0 / a[i];
 }
 
 // a coarse element's coefficient: the mean of its 8 children
@@ -243,24 +251,24 @@ __global__ void k_prolong_add(MGLevel f, MGLevel c, const double* __restrict__ x
   if (n < f.nodes) prolong_add_at(f, c, xc, xf, n);
 }
 
-// Chebyshev-Jacobi: start (r = b - t, or r = b with t == nullptr; d = r / (theta diag);
-// x = 0 when zero_x), step (x += d; r -= t; d = c1 d + c2 r / diag unless last), finish
-// (x += d)
+// Chebyshev-Jacobi (idiag: the reciprocal of the Jacobi diagonal): start (r = b - t, or
+// r = b with t == nullptr; d = r idiag / theta; x = 0 when zero_x), step (x += d; r -= t;
+// d = c1 d + c2 r idiag unless last), finish (x += d)
 __global__ void k_cheb_start(int64_t n, const double* __restrict__ b, const double* __restrict__ t,
-                             const double* __restrict__ diag, const double* __restrict__ cheb,
+                             const double* __restrict__ idiag, const double* __restrict__ cheb,
                              int zero_x, double* __restrict__ x, double* __restrict__ r,
                              double* __restrict__ d) {
   const double inv_theta = 1.0 / cheb[0];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double ri = t ? b[i] - t[i] : b[i];
     r[i] = ri;
-    d[i] = inv_theta * ri / diag[i];
+    d[i] = inv_theta * ri * idiag[i];
     if (zero_x) x[i] = 0.0;
   }
 }
 __global__ void k_cheb_step(int64_t n, double* __restrict__ x, double* __restrict__ d,
                             double* __restrict__ r, const double* __restrict__ t,
-                            const double* __restrict__ diag, const double* __restrict__ cheb,
+                            const double* __restrict__ idiag, const double* __restrict__ cheb,
                             int k, int last) {
   const double c1 = cheb[1 + k], c2 = cheb[1 + kChebMax + k];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -268,7 +276,7 @@ __global__ void k_cheb_step(int64_t n, double* __restrict__ x, double* __restric
     x[i] += di;
     const double ri = r[i] - t[i];
     r[i] = ri;
-    if (!last) d[i] = fma(c1, di, c2 * ri / diag[i]);
+    if (!last) d[i] = fma(c1, di, c2 * ri * idiag[i]);
   }
 }
 __global__ void k_cheb_finish(int64_t n, double* __restrict__ x, const double* __restrict__ d) {
@@ -359,7 +367,7 @@ __device__ void tail_smooth(const MGLevel& lv, bool zero_x, bool want_r, int deg
   double* __restrict__ r = lv.r;
   double* __restrict__ d = lv.d;
   double* __restrict__ t = lv.t;
-  const double* __restrict__ diag = lv.diag;
+  const double* __restrict__ idiag = lv.idiag;
   const double inv_theta = 1.0 / lv.cheb[0];
   if (!zero_x) {
     for (int64_t i = tid; i < n; i += nt) t[i] = q1_apply_at(lv, x, i);
@@ -368,7 +376,7 @@ __device__ void tail_smooth(const MGLevel& lv, bool zero_x, bool want_r, int deg
   for (int64_t i = tid; i < n; i += nt) {
     const double ri = zero_x ? b[i] : b[i] - t[i];
     r[i] = ri;
-    d[i] = inv_theta * ri / diag[i];
+    d[i] = inv_theta * ri * idiag[i];
     if (zero_x) x[i] = 0.0;
   }
   __syncthreads();
@@ -387,7 +395,7 @@ __device__ void tail_smooth(const MGLevel& lv, bool zero_x, bool want_r, int deg
       x[i] += di;
       const double ri = r[i] - t[i];
       r[i] = ri;
-      if (!last) d[i] = fma(c1, di, c2 * ri / diag[i]);
+      if (!last) d[i] = fma(c1, di, c2 * ri * idiag[i]);
     }
     __syncthreads();
   }
@@ -528,10 +536,10 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
   int rc;
   const int g = kMGBlocks;
   if (zero_x) {
-    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, nullptr, lv.diag, lv.cheb, 1, x, lv.r, lv.d);
+    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, nullptr, lv.idiag, lv.cheb, 1, x, lv.r, lv.d);
   } else {
     if ((rc = apply_level(mg, l, x, lv.t, clean, s))) return rc;
-    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, lv.t, lv.diag, lv.cheb, 0, x, lv.r, lv.d);
+    k_cheb_start<<<g, 256, 0, s>>>(lv.nodes, b, lv.t, lv.idiag, lv.cheb, 0, x, lv.r, lv.d);
   }
   for (int k = 1; k <= degree; ++k) {
     const bool last = k == degree;
@@ -540,7 +548,7 @@ int smooth(hm_mg* mg, int l, const double* b, double* x, bool zero_x, bool want_
       break;
     }
     if ((rc = apply_level(mg, l, lv.d, lv.t, clean, s))) return rc;
-    k_cheb_step<<<g, 256, 0, s>>>(lv.nodes, x, lv.d, lv.r, lv.t, lv.diag, lv.cheb, k, last ? 1 : 0);
+    k_cheb_step<<<g, 256, 0, s>>>(lv.nodes, x, lv.d, lv.r, lv.t, lv.idiag, lv.cheb, k, last ? 1 : 0);
   }
   return HM_OK;
 }
@@ -572,7 +580,7 @@ int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_
   const bool fuse = mg->fused && mg->degree == 1 &&
                     (l == 0 ? clean : (b == lv.b && x == lv.x));
   if (fuse && l == 0) {
-    if ((rc = hm_launch_cheb1_from_zero(mg->L, mg->jac, mg->ess, b, lv.diag, lv.cheb, x, lv.r,
+    if ((rc = hm_launch_cheb1_from_zero(mg->L, mg->jac, mg->ess, b, lv.idiag, lv.cheb, x, lv.r,
                                         (void*)s)))
       return rc;
   } else if (fuse) {
@@ -585,7 +593,7 @@ int vcycle(hm_mg* mg, int l, const double* b, double* x, bool clean, cudaStream_
   if ((rc = vcycle(mg, l + 1, cv.b, cv.x, clean, s, &xc))) return rc;
   k_prolong_add<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, cv, xc, x);
   if (fuse && l == 0)
-    return hm_launch_cheb1_from_x(mg->L, mg->jac, mg->ess, b, lv.diag, lv.cheb, x, (void*)s);
+    return hm_launch_cheb1_from_x(mg->L, mg->jac, mg->ess, b, lv.idiag, lv.cheb, x, (void*)s);
   if (fuse) {
     k_q1_cheb1_from_x<<<blocks_for(lv.nodes), 256, 0, s>>>(lv, b, x, lv.t);
     *out = lv.t;
@@ -656,9 +664,9 @@ extern "C" int64_t hm_mg_workspace_bytes(const hm_lattice* h) {
   if (!L) return 0;
   MGLevel lv[16];
   const int nl = plan_levels(*L, lv, 16);
-  int64_t doubles = 3 * L->ndof + 3 * kMGBlocks + 64 + nl * (2 * kChebMax + 8) +
+  int64_t doubles = 4 * L->ndof + 3 * kMGBlocks + 64 + nl * (2 * kChebMax + 8) +
                     kCoarseDirectMax * kCoarseDirectMax + 8;
-  for (int l = 1; l < nl; ++l) doubles += lv[l].elems + 6 * lv[l].nodes + 8;
+  for (int l = 1; l < nl; ++l) doubles += lv[l].elems + 7 * lv[l].nodes + 8;
   return doubles * (int64_t)sizeof(double);
 }
 
@@ -682,12 +690,13 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
   mg->checked_ess = nullptr;
   for (int l = 0; l < mg->nlev; ++l) mg->lv[l].cheb = take(2 * kChebMax + 8);
   MGLevel& z = mg->lv[0];
-  z.r = take(L->ndof); z.d = take(L->ndof); z.t = take(L->ndof);
+  z.r = take(L->ndof); z.d = take(L->ndof); z.t = take(L->ndof); z.idiag = take(L->ndof);
   z.x = z.b = nullptr; z.coef = nullptr; z.diag = nullptr;
   for (int l = 1; l < mg->nlev; ++l) {
     MGLevel& lv = mg->lv[l];
     lv.coef = take(lv.elems);
     lv.diag = take(lv.nodes);
+    lv.idiag = take(lv.nodes);
     lv.x = take(lv.nodes); lv.b = take(lv.nodes); lv.r = take(lv.nodes);
     lv.d = take(lv.nodes); lv.t = take(lv.nodes);
     lv.cinv = nullptr;
@@ -737,6 +746,9 @@ extern "C" int hm_mg_setup(hm_mg* mg, void* jac, const uint8_t* ess, const doubl
     for (int l = 1; l < mg->nlev; ++l)
       k_q1_diag<<<blocks_for(mg->lv[l].nodes), 256, 0, s>>>(mg->lv[l], mg->lv[l].diag);
   }
+  for (int l = 0; l < mg->nlev; ++l)
+    k_recip<<<blocks_for(mg->lv[l].nodes), 256, 0, s>>>(mg->lv[l].nodes, mg->lv[l].diag,
+                                                        mg->lv[l].idiag);
   // largest eigenvalue of D^{-1} A per level, on the device: power iteration with the
   // Rayleigh quotient v.Av / v.Dv (10 steps from a fixed start); smoothing interval
   // [hi/4, hi], the coarsest level's solve on [hi/64, hi]
