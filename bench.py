@@ -258,40 +258,54 @@ def _capacity(srv, sizes, poisson_trace, n=240):
 
 def run_serving(nreq, dev, sizes=(8, 12, 16, 24, 32, 48), slots=4, plain_sample=200):
     """The serving configuration: requests on n^3 meshes, n uniform over ``sizes``, 70%
-    forward solves (Jacobi-PCG to rtol 1e-8) / 30% Hessian actions, Poisson arrivals at
-    80% of the measured capacity, through the request loop (4 slots, FP32 operator and
-    recurrence with FP64 reliable updates, graph-captured iteration batches); beside it
-    the plain FP64 per-request path on a sample of the same trace, one request at a time."""
+    forward solves / 30% Hessian actions (solves to rtol 1e-8), Poisson arrivals at 80% of
+    the measured capacity, through the request loop: 4 slots, FP64 solves preconditioned
+    by the lattice multigrid V-cycle, same-size requests batched into solve groups (one
+    CUDA graph per iteration batch for the whole group; group size and graph batch length
+    per size from the autotuner).  Beside it the same mix with the FP32-recurrence solves
+    (FP64 reliable updates; not groupable) and the plain FP64 per-request path on a
+    sample of the same trace, one request at a time."""
     import torch
 
     from hippymfem_b200.serving import Server, latency_stats, plain_fp64, poisson_trace
 
-    srv = Server(slots=slots, precision="mixed", rel_tolerance=1e-8, device=dev,
-                 keep_results=False)
-    tuned = srv.autotune(sizes, candidates=(8, 16, 32), reps=2)
-    capacity = _capacity(srv, sizes, poisson_trace)
-    trace = poisson_trace(nreq, 0.8 * capacity, sizes, seed=12)
-    srv.run(trace)
-    st = latency_stats(trace)
-    st.update({"capacity_requests_per_s": capacity, "arrival_rate": 0.8 * capacity,
-               "slots": slots, "peak_workspace_bytes": srv.peak_resident,
-               "graph_batch_by_n": {str(k): v for k, v in tuned.items()},
-               "solves_per_s": sum(len(r.iterations) for r in trace) / (
-                   max(r.t_done for r in trace) - min(r.arrival for r in trace))})
-    srv.close()
-    # the same mix served with FP64 multigrid-preconditioned solves
+    def serve(srv, what, capacity=None):
+        if capacity is None:
+            capacity = _capacity(srv, sizes, poisson_trace)
+        trace = poisson_trace(nreq, 0.8 * capacity, sizes, seed=12)
+        srv.run(trace)
+        st = latency_stats(trace)
+        st.update({"capacity_requests_per_s": capacity, "arrival_rate": 0.8 * capacity,
+                   "slots": slots, "peak_workspace_bytes": srv.peak_resident, "what": what,
+                   "solves_per_s": sum(len(r.iterations) for r in trace) / (
+                       max(r.t_done for r in trace) - min(r.arrival for r in trace))})
+        return st, trace
+
     srv = Server(slots=slots, precision="fp64", multigrid=True, rel_tolerance=1e-8, device=dev,
                  keep_results=False)
-    tuned_mg = srv.autotune(sizes, candidates=(4, 8, 16), reps=2)
-    cap_mg = _capacity(srv, sizes, poisson_trace)
-    trace_mg = poisson_trace(nreq, 0.8 * cap_mg, sizes, seed=12)
-    srv.run(trace_mg)
-    st_mg = latency_stats(trace_mg)
-    st_mg.update({"capacity_requests_per_s": cap_mg, "arrival_rate": 0.8 * cap_mg,
-                  "graph_batch_by_n": {str(k): v for k, v in tuned_mg.items()},
-                  "what": "the same request mix (same sizes, seeds) at 80% of this server's "
-                          "capacity, FP64 solves with the lattice multigrid V-cycle"})
-    st["multigrid_fp64"] = st_mg
+    tuned = srv.autotune(sizes, candidates=(4, 8, 16), reps=2, group_candidates=(1, 2, 4))
+    st, trace = serve(srv, "FP64 solves with the lattice multigrid V-cycle, same-size requests "
+                           "in solve groups")
+    st["graph_batch_by_n"] = {str(k): v for k, v in tuned.items()}
+    st["group_size_by_n"] = {str(k): v for k, v in srv.group_by_n.items()}
+    srv.close()
+    # the same server without groups, on the same trace (same arrival times)
+    srv = Server(slots=slots, precision="fp64", multigrid=True, rel_tolerance=1e-8, device=dev,
+                 keep_results=False)
+    srv.autotune(sizes, candidates=(4, 8, 16), reps=2)
+    st_ng, _ = serve(srv, "the same trace, the same server without solve groups (one "
+                          "request per slot)", capacity=st["capacity_requests_per_s"])
+    st["no_groups"] = {k: st_ng[k] for k in ("p50_ms", "p99_ms", "mean_ms", "requests_per_s",
+                                              "arrival_rate", "what")}
+    srv.close()
+    srv = Server(slots=slots, precision="mixed", rel_tolerance=1e-8, device=dev,
+                 keep_results=False)
+    tuned_mx = srv.autotune(sizes, candidates=(8, 16, 32), reps=2)
+    st_mx, _ = serve(srv, "the same request mix (same sizes, seeds) at 80% of this server's "
+                          "capacity: Jacobi-PCG with the FP32 recurrence and FP64 reliable "
+                          "updates, one request per slot")
+    st_mx["graph_batch_by_n"] = {str(k): v for k, v in tuned_mx.items()}
+    st["mixed_fp32"] = st_mx
     srv.close()
     # the plain FP64 path, request by request (no overlap, no resident workspace)
     cache = {}
@@ -312,8 +326,8 @@ def run_serving(nreq, dev, sizes=(8, 12, 16, 24, 32, 48), slots=4, plain_sample=
                         "sample": len(lat),
                         "what": "service time of each request alone (no queueing), FP64, "
                                 "fresh problem objects, default stream"}
-    st["what"] = ("%d-request Poisson trace at 80%% of capacity, n in %s, 70%% forward / 30%% "
-                  "Hessian actions, rtol 1e-8; latency = completion - arrival" % (nreq, list(sizes)))
+    st["trace"] = ("%d-request Poisson trace at 80%% of capacity, n in %s, 70%% forward / 30%% "
+                   "Hessian actions, rtol 1e-8; latency = completion - arrival" % (nreq, list(sizes)))
     return st
 
 
@@ -646,6 +660,8 @@ def run_precision(a, n=128, nactions=20):
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     sp = stream_ptr()
     blocks = {}
+    cwork = torch.empty(lib.hm_lattice_consistent_workspace_bytes(mesh.handle) // 8 + 1,
+                        dtype=torch.float64, device=dev)
     for name in ("A", "C", "Wum", "Wmm"):
         vals, ms = {}, {}
         for prec in (_lib.HM_FP64, _lib.HM_FP32):
@@ -662,14 +678,44 @@ def run_precision(a, n=128, nactions=20):
             e1.record()
             torch.cuda.synchronize()
             vals[prec], ms[prec] = v, e0.elapsed_time(e1)
+            if prec == _lib.HM_FP64:
+                # the constant-exact single-precision block (consistent_block) from the
+                # same FP64 pointwise data
+                c = pat.new_values()
+                e0.record()
+                check(lib.hm_lattice_assemble_consistent(
+                    mesh.handle, ptr(quad), ptr(bc.marker),
+                    *(ptr(c) if name == b else None for b in ("A", "C", "Wum", "Wmm")),
+                    ptr(cwork), sp), "hm_lattice_assemble_consistent")
+                e1.record()
+                torch.cuda.synchronize()
+                vals["consistent"], ms["consistent"] = c, e0.elapsed_time(e1)
             del quad
-        d = vals[_lib.HM_FP32] - vals[_lib.HM_FP64]
         ref = vals[_lib.HM_FP64]
+        # products with the constants (row sums): what the consistent correction fixes
+        ones = torch.ones(mesh.ndof, dtype=torch.float64, device=dev)
+        rows = {}
+        for key in (_lib.HM_FP64, _lib.HM_FP32, "consistent"):
+            rows[key] = V.vector()
+            hm.CSRBlock(pat, vals[key]).mult(ones, rows[key])
+        scale = float(ref.abs().max())
+        row_defect_fp32 = float((rows[_lib.HM_FP32] - rows[_lib.HM_FP64]).abs().max()) / scale
+        row_defect_cons = float((rows["consistent"] - rows[_lib.HM_FP64]).abs().max()) / scale
+        del rows, ones
+        d = vals[_lib.HM_FP32] - ref
+        dc = vals["consistent"] - ref
         blocks[name] = {"rel_err_max": float(d.abs().max() / ref.abs().max()),
                         "rel_err_fro": float(d.norm() / ref.norm()),
-                        "ms_fp64": ms[_lib.HM_FP64], "ms_fp32": ms[_lib.HM_FP32]}
-        del vals, d, ref
+                        "consistent_rel_err_max": float(dc.abs().max() / ref.abs().max()),
+                        "consistent_rel_err_fro": float(dc.norm() / ref.norm()),
+                        "row_sum_defect_fp32": row_defect_fp32,
+                        "row_sum_defect_consistent": row_defect_cons,
+                        "ms_fp64": ms[_lib.HM_FP64], "ms_fp32": ms[_lib.HM_FP32],
+                        "ms_consistent": ms["consistent"]}
+        del vals, d, dc, ref
         torch.cuda.empty_cache()
+    del cwork
+    torch.cuda.empty_cache()
     # Hessian actions: FP64 (multigrid) against mixed-precision solves
     model.setPointForHessianEvaluations(x)
     H64 = hm.ReducedHessian(model)

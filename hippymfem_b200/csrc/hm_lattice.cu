@@ -720,3 +720,140 @@ extern "C" int hm_lattice_residual_noalloc(const hm_lattice* h, const double* d_
                             nullptr, d_vec_state, d_vec_param, d_vec_adjoint, zero_ess_vectors,
                             stream);
 }
+
+// ================================================== assembled vectors from the fields
+// dR/dp (ADJOINT, with the source -f w|J| phi), dR/du (STATE) and dR/dm (PARAMETER) of the
+// point (u, m, p) -- or, with mhat, the second-order products along mhat (D = w|J| e^m
+// mhat, f = 0) -- without the pointwise-data intermediate: one pass evaluates the
+// fields at the element's 27 points and contracts the element vectors (written in the
+// SoA layout Ye[a][e] of the operator), the node gather sums them per node in the fixed
+// order.  The vector counterpart of k_quad + the vector phases of the tile assembly.
+namespace hm {
+template <int NV>
+struct VecOut { double* ye[3]; };   // element results: ADJOINT, STATE, PARAMETER (NULL: skip)
+
+__global__ void __launch_bounds__(216) k_elem_vectors(Lattice L, const double* __restrict__ u,
+                                                      const double* __restrict__ m,
+                                                      const double* __restrict__ p,
+                                                      const double* __restrict__ mhat, double f,
+                                                      VecOut<3> o, uint32_t* __restrict__ status) {
+  __shared__ double tn[27][28];          // N(q, a)
+  __shared__ double tg[3][27][28];       // physical gradients G_k(q, a)
+  __shared__ double sv[8][4][27];        // node values of the 8 elements
+  __shared__ double sp[8][8][28];        // per element and point: E(3), F(3), W, source weight
+  const int tid = threadIdx.x, le = tid / 27, q = tid % 27;
+  const double ih[3] = {1.0 / L.hx, 1.0 / L.hy, 1.0 / L.hz};
+  for (int t = tid; t < 729; t += blockDim.x) {
+    const int qq = t / 27, a = t % 27;
+    const int q1 = qq % 3, q2 = (qq / 3) % 3, q3 = qq / 9;
+    const int a1 = a % 3, a2 = (a / 3) % 3, a3 = a / 9;
+    const double b1 = bq(q1, a1), b2 = bq(q2, a2), b3 = bq(q3, a3);
+    tn[qq][a] = b1 * b2 * b3;
+    tg[0][qq][a] = dbq(q1, a1) * b2 * b3 * ih[0];
+    tg[1][qq][a] = b1 * dbq(q2, a2) * b3 * ih[1];
+    tg[2][qq][a] = b1 * b2 * dbq(q3, a3) * ih[2];
+  }
+  const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
+  const double wdet = wq(q1) * wq(q2) * wq(q3) * L.hx * L.hy * L.hz;
+  for (int64_t g0 = blockIdx.x * 8LL; g0 < L.ne; g0 += (int64_t)gridDim.x * 8) {
+    const int64_t e = g0 + le;
+    const bool live = le < 8 && e < L.ne;
+    __syncthreads();                      // the previous group's smem is consumed
+    if (live) {
+      const int ex = (int)(e % L.nx), ey = (int)((e / L.nx) % L.ny), ez = (int)(e / ((int64_t)L.nx * L.ny));
+      const int a = q;
+      const int64_t node = (2 * ex + a % 3) + (int64_t)L.Nx * ((2 * ey + (a / 3) % 3) + (int64_t)L.Ny * (2 * ez + a / 9));
+      sv[le][0][a] = u[node];
+      sv[le][1][a] = m[node];
+      sv[le][2][a] = p[node];
+      sv[le][3][a] = mhat ? mhat[node] : 0.0;
+    }
+    __syncthreads();
+    if (live) {
+      // values and physical gradients at point q from the tables
+      double val[4] = {0, 0, 0, 0}, gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll 3
+      for (int a = 0; a < 27; ++a) {
+        const double na = tn[q][a], gx = tg[0][q][a], gy = tg[1][q][a], gz = tg[2][q][a];
+#pragma unroll
+        for (int fld = 0; fld < 4; ++fld) val[fld] = fma(na, sv[le][fld][a], val[fld]);
+#pragma unroll
+        for (int fld = 0; fld < 3; ++fld) {
+          if (fld == 1) continue;
+          const int k = fld == 0 ? 0 : 2;
+          gr[k][0] = fma(gx, sv[le][fld][a], gr[k][0]);
+          gr[k][1] = fma(gy, sv[le][fld][a], gr[k][1]);
+          gr[k][2] = fma(gz, sv[le][fld][a], gr[k][2]);
+        }
+      }
+      double D = wdet * exp(val[1]);
+      if (mhat) D *= val[3];
+      const double E0 = D * gr[0][0], E1 = D * gr[0][1], E2 = D * gr[0][2];
+      const double F0 = D * gr[2][0], F1 = D * gr[2][1], F2 = D * gr[2][2];
+      const double W = D * (gr[0][0] * gr[2][0] + gr[0][1] * gr[2][1] + gr[0][2] * gr[2][2]);
+      sp[le][0][q] = E0; sp[le][1][q] = E1; sp[le][2][q] = E2;
+      sp[le][3][q] = F0; sp[le][4][q] = F1; sp[le][5][q] = F2;
+      sp[le][6][q] = W;
+      sp[le][7][q] = mhat ? 0.0 : -f * wdet;
+      if (!(isfinite(E0) && isfinite(E1) && isfinite(E2) && isfinite(F0) && isfinite(F1) &&
+            isfinite(F2) && isfinite(W)))
+        atomicOr(status, HM_STATUS_NONFINITE);
+    }
+    __syncthreads();
+    if (live) {
+      // element vector entry a = q: sums over the 27 points, fixed order
+      const int a = q;
+      double ra = 0.0, rs = 0.0, rp = 0.0;
+#pragma unroll 3
+      for (int qq = 0; qq < 27; ++qq) {
+        const double gx = tg[0][qq][a], gy = tg[1][qq][a], gz = tg[2][qq][a], na = tn[qq][a];
+        ra = fma(sp[le][0][qq], gx, fma(sp[le][1][qq], gy, fma(sp[le][2][qq], gz, fma(sp[le][7][qq], na, ra))));
+        rs = fma(sp[le][3][qq], gx, fma(sp[le][4][qq], gy, fma(sp[le][5][qq], gz, rs)));
+        rp = fma(sp[le][6][qq], na, rp);
+      }
+      if (o.ye[0]) o.ye[0][(int64_t)a * L.ne + e] = ra;
+      if (o.ye[1]) o.ye[1][(int64_t)a * L.ne + e] = rs;
+      if (o.ye[2]) o.ye[2][(int64_t)a * L.ne + e] = rp;
+    }
+  }
+}
+
+__global__ void k_zero_marked(int64_t n, const uint8_t* __restrict__ ess, double* __restrict__ v) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n && ess[i]) v[i] = 0.0;
+}
+}  // namespace hm
+
+extern "C" int64_t hm_lattice_vectors_workspace_bytes(const hm_lattice* h, int nvectors) {
+  if (!h || nvectors < 1 || nvectors > 3) return 0;
+  return 8 * 27 * hm_lattice_geometry(h)->ne * (int64_t)nvectors;
+}
+
+extern "C" int hm_lattice_vectors(const hm_lattice* h, const double* d_u, const double* d_m,
+                                  const double* d_p, const double* d_mhat, double f,
+                                  const uint8_t* d_ess, double* d_vec_state, double* d_vec_param,
+                                  double* d_vec_adjoint, int zero_ess_vectors, void* d_work,
+                                  uint32_t* d_status, void* stream) {
+  if (!h || !d_u || !d_m || !d_p || !d_work || !d_status) return HM_ERR_ARG;
+  if (!d_vec_state && !d_vec_param && !d_vec_adjoint) return HM_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_work) & 7u) != 0) return HM_ERR_ARG;
+  const Lattice& L = *hm_lattice_geometry(h);
+  cudaStream_t s = S_(stream);
+  double* w = static_cast<double*>(d_work);
+  VecOut<3> o{};
+  double* outs[3] = {d_vec_adjoint, d_vec_state, d_vec_param};
+  int k = 0;
+  for (int i = 0; i < 3; ++i)
+    if (outs[i]) o.ye[i] = w + (int64_t)(k++) * 27 * L.ne;
+  const int64_t groups = (L.ne + 7) / 8;
+  const int grid = (int)(groups < 148 * 16 ? groups : 148 * 16);
+  k_elem_vectors<<<grid, 216, 0, s>>>(L, d_u, d_m, d_p, d_mhat, f, o, d_status);
+  for (int i = 0; i < 3; ++i) {
+    if (!outs[i]) continue;
+    k_node_gather<double, double, 0><<<gather_blocks(L), 256, 0, s>>>(
+        L, o.ye[i], nullptr, nullptr, outs[i], nullptr, nullptr, nullptr, nullptr);
+    if (zero_ess_vectors && d_ess && i != 2)
+      k_zero_marked<<<grid1(L.ndof, 256), 256, 0, s>>>(L.ndof, d_ess, outs[i]);
+  }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}

@@ -168,6 +168,28 @@ class PDEVariationalProblem:
                   "hm_lattice_quadrature_dir")
         return buf
 
+    def _direct_vectors(self, x, slots, f=None, mhat=None, zero_ess=False):
+        """The assembled vectors of ``slots`` at ``x`` (``hm_lattice_vectors``: straight
+        from the fields, no pointwise-data workspace); with ``mhat`` the second-order
+        products along it (no source)."""
+        u, m, p = self._locals(x)
+        n = len(slots)
+        need = lib.hm_lattice_vectors_workspace_bytes(self.mesh.handle, n)
+        buf = self._quad.get("vectors")
+        if buf is None or buf.numel() * 8 < need:
+            buf = self._quad["vectors"] = torch.empty((need + 7) // 8, dtype=torch.float64,
+                                                      device=self.mesh.device)
+        vecs = {s_: self.Vh[s_].vector() for s_ in slots}
+        if self.check_finite:
+            self._status.zero_()
+        check(lib.hm_lattice_vectors(
+            self.mesh.handle, ptr(u), ptr(m), ptr(p), ptr(mhat),
+            0.0 if mhat is not None else (self.f if f is None else float(f)),
+            ptr(self.bc0.marker), ptr(vecs.get(STATE)), ptr(vecs.get(PARAMETER)),
+            ptr(vecs.get(ADJOINT)), int(bool(zero_ess)), ptr(buf), ptr(self._status),
+            stream_ptr()), "hm_lattice_vectors")
+        return vecs
+
     def _require_finite(self, what):
         if self.check_finite and int(self._status.item()) & _lib.HM_STATUS_NONFINITE:
             raise RuntimeError("non-finite values in %s" % what)
@@ -191,8 +213,7 @@ class PDEVariationalProblem:
     def _residual(self, x, var=ADJOINT, ess=None):
         """``dR/d(var)`` at ``x`` (modeling/PDEVariationalProblem.py:423), essential
         entries of ``ess`` zeroed."""
-        quad = self._quadrature(x, "residual")
-        _, vecs = self._assemble(quad, vectors=(var,))
+        vecs = self._direct_vectors(x, (var,))
         self._require_finite("the residual")
         out = vecs[var]
         if ess is not None and len(ess):
@@ -363,18 +384,15 @@ class PDEVariationalProblem:
         return out
 
     def _dir_products(self, x, mhat):
-        """``C mhat``, ``W_um mhat`` and ``W_mm mhat`` at ``x`` from one pass of the
-        directional quadrature data (f = 0), with the row eliminations of C and W_um;
-        kept for the next products along the same ``mhat`` at the same point."""
+        """``C mhat``, ``W_um mhat`` and ``W_mm mhat`` at ``x`` from one pass over the
+        fields (``hm_lattice_vectors`` with ``mhat``, no source), with the row
+        eliminations of C and W_um; kept for the next products along the same ``mhat``
+        at the same point."""
         c = self._dir_cache
         if c is not None and all(a.matches(v) for a, v in zip(c[0], list(x) + [mhat])):
             return c[1]
-        quad = self._quadrature(x, "dir", mhat=mhat)
-        _, vecs = self._assemble(quad, vectors=(ADJOINT, STATE, PARAMETER), f=0.0)
+        vecs = self._direct_vectors(x, (ADJOINT, STATE, PARAMETER), mhat=mhat, zero_ess=True)
         self._require_finite("the second-order products")
-        mask = self.bc0.mask
-        vecs[ADJOINT].masked_fill_(mask, 0.0)
-        vecs[STATE].masked_fill_(mask, 0.0)
         self._dir_cache = (tuple(_Snapshot(v) for v in list(x) + [mhat]), vecs)
         return vecs
 
@@ -402,8 +420,7 @@ class PDEVariationalProblem:
             raise ValueError("no block (%d, %d)" % (i, j))
         d = dir.masked_fill(self.bc0.mask, 0.0)
         y = [x[STATE], x[PARAMETER], d] if j == ADJOINT else [d, x[PARAMETER], x[ADJOINT]]
-        quad = self._quadrature(y, "transpose")
-        _, vecs = self._assemble(quad, vectors=(PARAMETER,))
+        vecs = self._direct_vectors(y, (PARAMETER,))
         self._require_finite("the second-order products")
         out.copy_(vecs[PARAMETER])
         return out

@@ -147,6 +147,25 @@ int hm_lattice_assemble(const hm_lattice* h, const void* d_quad, int precision,
                         double* d_vals_Wmm, double* d_vec_state, double* d_vec_param,
                         double* d_vec_adjoint, int zero_ess_vectors, void* stream);
 
+/* The assembled vectors straight from the fields, without the pointwise-data
+ * workspace: dR/du (STATE), dR/dm (PARAMETER), dR/dp (ADJOINT, with the source f) at
+ * (u, m, p), or with d_mhat != NULL the second-order products along mhat (D = w|J| e^m
+ * mhat, no source: ADJOINT C mhat, STATE W_um mhat, PARAMETER W_mm mhat, rows not
+ * eliminated) -- the vectors hm_lattice_quadrature(_dir) + hm_lattice_assemble give,
+ * summed in another fixed order (equal to rounding; deterministic).  One pass evaluates
+ * the fields at each element's 27 points and contracts its element vectors, a node
+ * gather sums them; the replacement of element_vectors + assemble_vector
+ * (hippymfem/fem/kernel.py:2070-2078, fem/pattern.py:1186-1233) and of the directional
+ * products of apply_ij_at (modeling/PDEVariationalProblem.py:1672).  With
+ * zero_ess_vectors the STATE and ADJOINT vectors are zeroed on d_ess.  d_work:
+ * hm_lattice_vectors_workspace_bytes(h, number of vectors asked for).  Non-finite
+ * pointwise values set HM_STATUS_NONFINITE in *d_status. */
+int64_t hm_lattice_vectors_workspace_bytes(const hm_lattice* h, int nvectors);
+int hm_lattice_vectors(const hm_lattice* h, const double* d_u, const double* d_m,
+                       const double* d_p, const double* d_mhat, double f, const uint8_t* d_ess,
+                       double* d_vec_state, double* d_vec_param, double* d_vec_adjoint,
+                       int zero_ess_vectors, void* d_work, uint32_t* d_status, void* stream);
+
 /* Matrix-free Q2 operator y = A(D) x with the Jacobian's elimination (x zeroed on
  * d_ess, y = x there): the product apply_ij_at gives for (ADJOINT, STATE)
  * (modeling/PDEVariationalProblem.py:1672).  Its data d_jac (hm_lattice_jacobian_bytes)

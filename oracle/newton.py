@@ -14,8 +14,12 @@ What it follows (paths relative to the hIPPyMFEM tree):
   operator and preconditioner left at their own (``cg_incremental_tolerance = 0``,
   ``cg_preconditioner_tolerance = 0``: here every solve is direct);
 * :func:`steihaug_cg` -- ``CGSolverSteihaug._solve``
-  (``hippymfem/algorithms/cgsolverSteihaug.py:218-344``), without a trust region, with
-  the explicit reorthogonalization against the earlier residuals;
+  (``hippymfem/algorithms/cgsolverSteihaug.py:218-344``) with the explicit
+  reorthogonalization against the earlier residuals, and with or without the trust
+  region of ``set_TR`` / ``update_x_with_TR`` / ``_tau_to_boundary`` /
+  ``_negative_curvature`` (``:117-197``);
+* :func:`newton_cg_tr` -- ``ReducedSpaceNewtonCG._solve_tr`` (``NewtonCG.py:377-510``):
+  the radius from the first step, the ratio test with ``eta``, the radius updates;
 * :func:`armijo` -- ``armijo_backtrack`` (``hippymfem/algorithms/linesearch.py:12-62``);
 * :class:`InverseProblem` -- the model the algorithm drives, for the Q2 log-conductivity
   problem on the lattice: the forward and adjoint solves
@@ -127,10 +131,27 @@ class InverseProblem:
 
 
 def steihaug_cg(A, Binv, b, rel_tolerance, abs_tolerance=1e-12, max_iter=1000,
-                reorthogonalize=True):
-    """Returns ``(x, iterations, actions, reason)``; ``actions`` counts ``A`` products."""
+                reorthogonalize=True, tr=None):
+    """Returns ``(x, iterations, actions, reason)``; ``actions`` counts ``A`` products.
+    ``tr = (radius, B)``: the steps stay in ``x^T B x <= radius^2``."""
     actions = 0
     x = np.zeros_like(b)
+    if tr is not None:
+        R2, Bop = tr[0] ** 2, tr[1]
+
+    def bdot(u, v):
+        return float(Bop(u) @ v)
+
+    def to_boundary(x, d, rd, dAd):
+        a, b_half = bdot(d, d), bdot(d, x)
+        c = bdot(x, x) - R2
+        disc = np.sqrt(max(b_half * b_half - a * c, 0.0))
+        best = None
+        for tau in ((-b_half + disc) / a, (-b_half - disc) / a):
+            mv = -tau * rd + 0.5 * tau * tau * dAd
+            if best is None or mv < best[0]:
+                best = (mv, tau)
+        return best[1]
     r = b.copy()
     z = Binv(r)
     d = z.copy()
@@ -143,11 +164,19 @@ def steihaug_cg(A, Binv, b, rel_tolerance, abs_tolerance=1e-12, max_iter=1000,
     actions += 1
     den = float(Ad @ d)
     if den <= 0.0:
-        return x + d, 0, actions, 2
+        tau = to_boundary(x, d, float(r @ d), den) if tr is not None else 1.0
+        return x + tau * d, 0, actions, 2
     it = 1
     while True:
         alpha = nom / den
-        x = x + alpha * d
+        xn = x + alpha * d
+        if tr is not None and bdot(xn, xn) >= R2:
+            a_tau = alpha * alpha * bdot(d, d)
+            b_half = alpha * bdot(d, x)
+            c_tau = bdot(x, x) - R2
+            tau = (-b_half + np.sqrt(max(b_half * b_half - a_tau * c_tau, 0.0))) / a_tau
+            return x + (tau * alpha) * d, it, actions, 3
+        x = xn
         r = r - alpha * Ad
         if basis is not None:
             for rj, zj, rho in basis:
@@ -166,6 +195,8 @@ def steihaug_cg(A, Binv, b, rel_tolerance, abs_tolerance=1e-12, max_iter=1000,
         actions += 1
         den = float(d @ Ad)
         if den <= 0.0:
+            if tr is not None:
+                x = x + to_boundary(x, d, float(r @ d), den) * d
             return x, it, actions, 2
         nom = betanom
     del nom0
@@ -225,5 +256,55 @@ def newton_cg_ls(prob, m0, rel_tolerance=1e-6, abs_tolerance=1e-12, gdm_toleranc
             break
         if -mg_mhat <= gdm_tolerance:
             converged, reason = True, 3
+            break
+    return m, history, reason, converged
+
+
+def newton_cg_tr(prob, m0, rel_tolerance=1e-6, abs_tolerance=1e-12, max_iter=20, GN_iter=5,
+                 cg_coarse_tolerance=0.5, cg_max_iter=100, cg_reorthogonalize=True, eta=0.05):
+    """Returns ``(m, history, reason, converged)``."""
+    m = np.array(m0, dtype=np.float64)
+    u = prob.solve_fwd(m)
+    it, converged, reason = 0, False, 0
+    cost_old = cost_new = prob.cost(u, m)[0]
+    delta = None
+    gradnorm_ini = float("nan")
+    tol = abs_tolerance
+    history = []
+    while it < max_iter and not converged:
+        p = prob.solve_adj(u, m)
+        prob.set_point(u, m, p, gauss_newton=it < GN_iter)
+        g, gradnorm = prob.gradient(u, m, p)
+        if it == 0:
+            gradnorm_ini = gradnorm
+            tol = max(abs_tolerance, gradnorm_ini * rel_tolerance)
+        if gradnorm < tol and it > 0:
+            converged, reason = True, 1
+            break
+        it += 1
+        tolcg = min(cg_coarse_tolerance, np.sqrt(gradnorm / max(gradnorm_ini, 1e-300)))
+        mhat, _, actions, _ = steihaug_cg(prob.hessian, prob.Rinv, -g, tolcg, max_iter=cg_max_iter,
+                                          reorthogonalize=cg_reorthogonalize,
+                                          tr=None if delta is None else (delta, prob.R))
+        if delta is None:
+            delta = max(np.sqrt(max(float(prob.R(mhat) @ mhat), 0.0)) * 5.0, 1.0)
+        m_star = m + mhat
+        u_star = prob.solve_fwd(m_star)
+        cost_star = prob.cost(u_star, m_star)
+        pred = -(float(g @ mhat) + 0.5 * float(prob.hessian(mhat) @ mhat))
+        rho = (cost_old - cost_star[0]) / pred if pred != 0.0 else 0.0
+        mhat_R = np.sqrt(max(float(prob.R(mhat) @ mhat), 0.0))
+        accept = rho > eta
+        if accept:
+            m, u = m_star, u_star
+            cost_old = cost_new = cost_star[0]
+        if rho < 0.25:
+            delta *= 0.5
+        elif rho > 0.75 and mhat_R >= 0.99 * delta:
+            delta *= 2.0
+        history.append({"it": it, "cg_it": actions, "cost": cost_new, "gradnorm": gradnorm,
+                        "radius": delta, "rho": rho, "accepted": accept, "tolcg": tolcg})
+        if delta < 1e-12:
+            converged, reason = False, 2
             break
     return m, history, reason, converged

@@ -198,3 +198,63 @@ def test_nonfinite_parameter_is_reported(cuda):
     m[5] = float("nan")
     with pytest.raises(RuntimeError):
         prob._residual([None, m, None], PARAMETER)
+
+
+@pytest.mark.parametrize("with_mhat", [False, True])
+def test_direct_vectors_match_the_oracle_and_the_tile_path(cuda, with_mhat):
+    """hm_lattice_vectors (fields -> element vectors -> node gather, no pointwise data)
+    against the oracle's assembled vectors and against the tile kernel's vector phases:
+    the point's dR/du, dR/dm, dR/dp with the source, or the directional products C mhat,
+    W_um mhat, W_mm mhat along mhat; zeroing on the Dirichlet nodes as asked."""
+    from hippymfem_b200 import BoxMesh, DirichletBC, Q2Space
+    from hippymfem_b200 import _lib
+    from hippymfem_b200._lib import check, lib, ptr, stream_ptr
+
+    n, L = (5, 6, 4), (1.0, 0.9, 0.7)
+    mesh = BoxMesh(n, L)
+    mo = q2.Lattice(n, L)
+    u, m, p = _point(mesh.ndof, 9)
+    mh = np.random.default_rng(10).standard_normal(mesh.ndof)
+    marker = DirichletBC(Q2Space(mesh)).marker
+    U, M, P, MH = (torch.as_tensor(v, device=cuda) for v in (u, m, p, mh))
+    f = 0.0 if with_mhat else 1.3
+    work = torch.empty(lib.hm_lattice_vectors_workspace_bytes(mesh.handle, 3) // 8,
+                       dtype=torch.float64, device=cuda)
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    out = [torch.full((mesh.ndof,), float("nan"), dtype=torch.float64, device=cuda)
+           for _ in range(3)]
+    check(lib.hm_lattice_vectors(mesh.handle, ptr(U), ptr(M), ptr(P), ptr(MH) if with_mhat else None,
+                                 f, ptr(marker), ptr(out[0]), ptr(out[1]), ptr(out[2]), 1,
+                                 ptr(work), ptr(status), stream_ptr()), "hm_lattice_vectors")
+    quad = torch.empty(mesh.quad_bytes() // 8, dtype=torch.float64, device=cuda)
+    if with_mhat:
+        check(lib.hm_lattice_quadrature_dir(mesh.handle, ptr(U), ptr(M), ptr(P), ptr(MH),
+                                            _lib.HM_FP64, ptr(quad), ptr(status), stream_ptr()))
+    else:
+        check(lib.hm_lattice_quadrature(mesh.handle, ptr(U), ptr(M), ptr(P), _lib.HM_FP64,
+                                        ptr(quad), ptr(status), stream_ptr()))
+    tile = [torch.empty(mesh.ndof, dtype=torch.float64, device=cuda) for _ in range(3)]
+    check(lib.hm_lattice_assemble(mesh.handle, ptr(quad), _lib.HM_FP64, None, ptr(marker), f,
+                                  None, None, None, None, ptr(tile[0]), ptr(tile[1]),
+                                  ptr(tile[2]), 1, stream_ptr()))
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    ess = mo.boundary_dofs()
+    E = mo.edofs()
+    if with_mhat:
+        blk = q2.element_blocks(mo, E, u, m, p)
+        pat = q2.build_tables(E, E, mo.ndof, mo.ndof, True)
+        ref = {}
+        for s, name in ((0, "Wum"), (1, "Wmm"), (2, "C")):
+            M_ = q2.csr(pat, q2.scatter(pat[2], blk[name], pat[3]), (mo.ndof, mo.ndof))
+            ref[s] = M_ @ mh
+    else:
+        ev = q2.element_vectors(mo, E, u, m, p, f)
+        ref = {s: q2.assemble_vector(E, ev[s], mo.ndof) for s in range(3)}
+    for s in range(3):
+        r = ref[s].copy()
+        if s != 1:
+            r[ess] = 0.0
+        got = out[s].cpu().numpy()
+        assert _rel(got, r) <= TOL, (s, _rel(got, r))
+        assert _rel(got, tile[s].cpu().numpy()) <= 1e-13, s

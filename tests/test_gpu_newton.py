@@ -153,3 +153,34 @@ def test_newton_cg_iterates_match_the_oracle_restatement(cuda):
             assert abs(a[k] - b[k]) <= 1e-8 * abs(b[k]), (k, a, b)
         assert abs(a["gdm"] - b["gdm"]) <= 1e-8 * abs(b["gdm"]) + 1e-14, (a, b)
     assert np.linalg.norm(x[1].cpu().numpy() - m) <= 1e-7 * np.linalg.norm(m)
+
+
+def test_trust_region_newton_cg_matches_the_oracle_restatement(cuda):
+    """The trust-region globalization (NewtonCG.py:377-510, Steihaug CG inside the region
+    of the prior's precision) against the oracle's restatement: the same CG counts,
+    acceptances and termination; cost, |g| and radius to 1e-8, the reduction ratio to
+    1e-5 (a difference of nearly equal costs)."""
+    from hippymfem_b200.newton import ReducedSpaceNewtonCG, ReducedSpaceNewtonCG_ParameterList
+    from hippymfem_b200.synthetic import interior_points
+
+    from oracle import newton as on
+
+    n = 8
+    mesh, V, prob, model = _inverse_problem(n)
+    prm = ReducedSpaceNewtonCG_ParameterList()
+    prm.update({"print_level": -1, "rel_tolerance": 1e-6, "max_iter": 25, "globalization": "TR"})
+    solver = ReducedSpaceNewtonCG(model, prm)
+    x = [V.vector(), V.vector(), V.vector()]
+    solver.solve(x)
+    ref = on.InverseProblem(n, interior_points(64, seed=2), model.misfit.d.cpu().numpy(),
+                            model.misfit.noise_variance, gamma=0.05, delta=0.5)
+    m, hist, reason, converged = on.newton_cg_tr(ref, np.zeros(ref.nd), rel_tolerance=1e-6,
+                                                 max_iter=25)
+    assert (solver.reason, solver.converged) == (reason, converged)
+    assert len(solver.history) == len(hist) >= 3
+    for a, b in zip(solver.history, hist):
+        assert a["cg_it"] == b["cg_it"] and a["accepted"] == b["accepted"], (a, b)
+        for k in ("cost", "gradnorm", "radius"):
+            assert abs(a[k] - b[k]) <= 1e-8 * abs(b[k]), (k, a, b)
+        assert abs(a["rho"] - b["rho"]) <= 1e-5, (a, b)
+    assert np.linalg.norm(x[1].cpu().numpy() - m) <= 1e-7 * np.linalg.norm(m)
