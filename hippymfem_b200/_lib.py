@@ -97,6 +97,7 @@ SIGNATURES = {
     "hm_pcg_group_create": (_i32, [_p, _i32, _p]),
     "hm_pcg_group_solve": (_i32, [_p, _d, _i32, _p, _p, _p]),
     "hm_pcg_group_destroy": (_i32, [_p]),
+    "hm_lattice_add_boundary_mass": (_i32, [_p, _d, _p, _p]),
     "hm_lattice_vectors_workspace_bytes": (_i64, [_p, _i32]),
     "hm_lattice_vectors": (_i32, [_p, _p, _p, _p, _p, _d, _p, _p, _p, _p, _i32, _p, _p, _p]),
     "hm_dot_workspace_bytes": (_i64, [_i64]),

@@ -732,88 +732,152 @@ namespace hm {
 template <int NV>
 struct VecOut { double* ye[3]; };   // element results: ADJOINT, STATE, PARAMETER (NULL: skip)
 
-__global__ void __launch_bounds__(216) k_elem_vectors(Lattice L, const double* __restrict__ u,
+// Sum factorisation on the element's 3 x 3 x 3 nodes and points: nodes -> points one
+// axis at a time (x, y, z), the pointwise data at the 27 points, then points -> nodes
+// (z, y, x) for the three element vectors.  One CTA holds 8 elements, a thread per
+// (element, index); every stage reads the previous one's arrays in shared memory.
+//   evaluation   X: B u, B' u, B p, B' p, B m, B mhat        (index q1 + 3 a2 + 9 a3)
+//                Y: u: BB, BB', B'B;  p: the same;  m, mhat: BB  (q1 + 3 q2 + 9 a3)
+//                Z: grad u, grad p, m, mhat at the point      (q1 + 3 q2 + 9 q3)
+//   integration  Z: E_x B, E_y B, E_z B' + s B | F_x B, F_y B, F_z B' | W B
+//                Y: (.) B, (.) B' + (.) B per vector        (q1 + 3 a2 + 9 a3)
+//                X: B' (.) + B (.)                          (a1 + 3 a2 + 9 a3)
+// with the 1/h of each derivative folded in at its z sums.
+__device__ __forceinline__ double b1d(int q, int a) { return bq(q, a); }
+__device__ __forceinline__ double d1d(int q, int a) { return dbq(q, a); }
+
+__global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double* __restrict__ u,
                                                       const double* __restrict__ m,
                                                       const double* __restrict__ p,
                                                       const double* __restrict__ mhat, double f,
                                                       VecOut<3> o, uint32_t* __restrict__ status) {
-  __shared__ double tn[27][28];          // N(q, a)
-  __shared__ double tg[3][27][28];       // physical gradients G_k(q, a)
-  __shared__ double sv[8][4][27];        // node values of the 8 elements
-  __shared__ double sp[8][8][28];        // per element and point: E(3), F(3), W, source weight
-  const int tid = threadIdx.x, le = tid / 27, q = tid % 27;
-  const double ih[3] = {1.0 / L.hx, 1.0 / L.hy, 1.0 / L.hz};
-  for (int t = tid; t < 729; t += blockDim.x) {
-    const int qq = t / 27, a = t % 27;
-    const int q1 = qq % 3, q2 = (qq / 3) % 3, q3 = qq / 9;
-    const int a1 = a % 3, a2 = (a / 3) % 3, a3 = a / 9;
-    const double b1 = bq(q1, a1), b2 = bq(q2, a2), b3 = bq(q3, a3);
-    tn[qq][a] = b1 * b2 * b3;
-    tg[0][qq][a] = dbq(q1, a1) * b2 * b3 * ih[0];
-    tg[1][qq][a] = b1 * dbq(q2, a2) * b3 * ih[1];
-    tg[2][qq][a] = b1 * b2 * dbq(q3, a3) * ih[2];
-  }
-  const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
-  const double wdet = wq(q1) * wq(q2) * wq(q3) * L.hx * L.hy * L.hz;
+  __shared__ double sv[8][4][27];        // node values u, m, p, mhat
+  __shared__ double s1[8][7][27];        // evaluation X / integration Z
+  __shared__ double s2[8][8][27];        // evaluation Y / integration Y
+  __shared__ double sp[8][8][27];        // E(3), F(3), W, source weight at the points
+  const int tid = threadIdx.x, le = tid / 27, i = tid % 27;
+  const int c1 = i % 3, c2 = (i / 3) % 3, c3 = i / 9;   // the thread's three indices
+  const double ihx = 1.0 / L.hx, ihy = 1.0 / L.hy, ihz = 1.0 / L.hz;
+  const double wdet = wq(c1) * wq(c2) * wq(c3) * L.hx * L.hy * L.hz;
   for (int64_t g0 = blockIdx.x * 8LL; g0 < L.ne; g0 += (int64_t)gridDim.x * 8) {
     const int64_t e = g0 + le;
     const bool live = le < 8 && e < L.ne;
-    __syncthreads();                      // the previous group's smem is consumed
+    __syncthreads();                      // the previous group's arrays are consumed
     if (live) {
       const int ex = (int)(e % L.nx), ey = (int)((e / L.nx) % L.ny), ez = (int)(e / ((int64_t)L.nx * L.ny));
-      const int a = q;
-      const int64_t node = (2 * ex + a % 3) + (int64_t)L.Nx * ((2 * ey + (a / 3) % 3) + (int64_t)L.Ny * (2 * ez + a / 9));
-      sv[le][0][a] = u[node];
-      sv[le][1][a] = m[node];
-      sv[le][2][a] = p[node];
-      sv[le][3][a] = mhat ? mhat[node] : 0.0;
+      const int64_t node = (2 * ex + c1) + (int64_t)L.Nx * ((2 * ey + c2) + (int64_t)L.Ny * (2 * ez + c3));
+      sv[le][0][i] = u[node];
+      sv[le][1][i] = m[node];
+      sv[le][2][i] = p[node];
+      sv[le][3][i] = mhat ? mhat[node] : 0.0;
     }
     __syncthreads();
-    if (live) {
-      // values and physical gradients at point q from the tables
-      double val[4] = {0, 0, 0, 0}, gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll 3
-      for (int a = 0; a < 27; ++a) {
-        const double na = tn[q][a], gx = tg[0][q][a], gy = tg[1][q][a], gz = tg[2][q][a];
+    if (live) {   // X: index (q1 = c1, a2 = c2, a3 = c3), sums over a1
+      double r[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-        for (int fld = 0; fld < 4; ++fld) val[fld] = fma(na, sv[le][fld][a], val[fld]);
-#pragma unroll
-        for (int fld = 0; fld < 3; ++fld) {
-          if (fld == 1) continue;
-          const int k = fld == 0 ? 0 : 2;
-          gr[k][0] = fma(gx, sv[le][fld][a], gr[k][0]);
-          gr[k][1] = fma(gy, sv[le][fld][a], gr[k][1]);
-          gr[k][2] = fma(gz, sv[le][fld][a], gr[k][2]);
-        }
+      for (int a1 = 0; a1 < 3; ++a1) {
+        const int j = a1 + 3 * c2 + 9 * c3;
+        const double b = b1d(c1, a1), d = d1d(c1, a1);
+        const double vu = sv[le][0][j], vm = sv[le][1][j], vp = sv[le][2][j], vh = sv[le][3][j];
+        r[0] = fma(b, vu, r[0]); r[1] = fma(d, vu, r[1]);
+        r[2] = fma(b, vp, r[2]); r[3] = fma(d, vp, r[3]);
+        r[4] = fma(b, vm, r[4]); r[5] = fma(b, vh, r[5]);
       }
-      double D = wdet * exp(val[1]);
-      if (mhat) D *= val[3];
-      const double E0 = D * gr[0][0], E1 = D * gr[0][1], E2 = D * gr[0][2];
-      const double F0 = D * gr[2][0], F1 = D * gr[2][1], F2 = D * gr[2][2];
-      const double W = D * (gr[0][0] * gr[2][0] + gr[0][1] * gr[2][1] + gr[0][2] * gr[2][2]);
-      sp[le][0][q] = E0; sp[le][1][q] = E1; sp[le][2][q] = E2;
-      sp[le][3][q] = F0; sp[le][4][q] = F1; sp[le][5][q] = F2;
-      sp[le][6][q] = W;
-      sp[le][7][q] = mhat ? 0.0 : -f * wdet;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) s1[le][k][i] = r[k];
+    }
+    __syncthreads();
+    if (live) {   // Y: index (q1 = c1, q2 = c2, a3 = c3), sums over a2
+      double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int a2 = 0; a2 < 3; ++a2) {
+        const int j = c1 + 3 * a2 + 9 * c3;
+        const double b = b1d(c2, a2), d = d1d(c2, a2);
+        const double x0 = s1[le][0][j], x1 = s1[le][1][j], x2 = s1[le][2][j], x3 = s1[le][3][j];
+        r[0] = fma(b, x0, r[0]); r[1] = fma(b, x1, r[1]); r[2] = fma(d, x0, r[2]);
+        r[3] = fma(b, x2, r[3]); r[4] = fma(b, x3, r[4]); r[5] = fma(d, x2, r[5]);
+        r[6] = fma(b, s1[le][4][j], r[6]); r[7] = fma(b, s1[le][5][j], r[7]);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s2[le][k][i] = r[k];
+    }
+    __syncthreads();
+    if (live) {   // Z: the point (c1, c2, c3), sums over a3; then the pointwise data
+      double gu[3] = {0, 0, 0}, gp[3] = {0, 0, 0}, mv = 0.0, mh = 0.0;
+#pragma unroll
+      for (int a3 = 0; a3 < 3; ++a3) {
+        const int j = c1 + 3 * c2 + 9 * a3;
+        const double b = b1d(c3, a3), d = d1d(c3, a3);
+        gu[0] = fma(b, s2[le][1][j], gu[0]); gu[1] = fma(b, s2[le][2][j], gu[1]);
+        gu[2] = fma(d, s2[le][0][j], gu[2]);
+        gp[0] = fma(b, s2[le][4][j], gp[0]); gp[1] = fma(b, s2[le][5][j], gp[1]);
+        gp[2] = fma(d, s2[le][3][j], gp[2]);
+        mv = fma(b, s2[le][6][j], mv); mh = fma(b, s2[le][7][j], mh);
+      }
+      gu[0] *= ihx; gu[1] *= ihy; gu[2] *= ihz;
+      gp[0] *= ihx; gp[1] *= ihy; gp[2] *= ihz;
+      double D = wdet * exp(mv);
+      if (mhat) D *= mh;
+      const double E0 = D * gu[0], E1 = D * gu[1], E2 = D * gu[2];
+      const double F0 = D * gp[0], F1 = D * gp[1], F2 = D * gp[2];
+      const double W = D * (gu[0] * gp[0] + gu[1] * gp[1] + gu[2] * gp[2]);
+      sp[le][0][i] = E0; sp[le][1][i] = E1; sp[le][2][i] = E2;
+      sp[le][3][i] = F0; sp[le][4][i] = F1; sp[le][5][i] = F2;
+      sp[le][6][i] = W;
+      sp[le][7][i] = mhat ? 0.0 : -f * wdet;
       if (!(isfinite(E0) && isfinite(E1) && isfinite(E2) && isfinite(F0) && isfinite(F1) &&
             isfinite(F2) && isfinite(W)))
         atomicOr(status, HM_STATUS_NONFINITE);
     }
     __syncthreads();
-    if (live) {
-      // element vector entry a = q: sums over the 27 points, fixed order
-      const int a = q;
-      double ra = 0.0, rs = 0.0, rp = 0.0;
-#pragma unroll 3
-      for (int qq = 0; qq < 27; ++qq) {
-        const double gx = tg[0][qq][a], gy = tg[1][qq][a], gz = tg[2][qq][a], na = tn[qq][a];
-        ra = fma(sp[le][0][qq], gx, fma(sp[le][1][qq], gy, fma(sp[le][2][qq], gz, fma(sp[le][7][qq], na, ra))));
-        rs = fma(sp[le][3][qq], gx, fma(sp[le][4][qq], gy, fma(sp[le][5][qq], gz, rs)));
-        rp = fma(sp[le][6][qq], na, rp);
+    if (live) {   // integration Z: index (q1 = c1, q2 = c2, a3 = c3), sums over q3
+      double r[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int q3 = 0; q3 < 3; ++q3) {
+        const int j = c1 + 3 * c2 + 9 * q3;
+        const double b = b1d(q3, c3), d = d1d(q3, c3);
+        r[0] = fma(b, sp[le][0][j], r[0]);
+        r[1] = fma(b, sp[le][1][j], r[1]);
+        r[2] = fma(d * ihz, sp[le][2][j], fma(b, sp[le][7][j], r[2]));
+        r[3] = fma(b, sp[le][3][j], r[3]);
+        r[4] = fma(b, sp[le][4][j], r[4]);
+        r[5] = fma(d, sp[le][5][j], r[5]);
+        r[6] = fma(b, sp[le][6][j], r[6]);
       }
-      if (o.ye[0]) o.ye[0][(int64_t)a * L.ne + e] = ra;
-      if (o.ye[1]) o.ye[1][(int64_t)a * L.ne + e] = rs;
-      if (o.ye[2]) o.ye[2][(int64_t)a * L.ne + e] = rp;
+      s1[le][0][i] = r[0] * ihx; s1[le][1][i] = r[1] * ihy; s1[le][2][i] = r[2];
+      s1[le][3][i] = r[3] * ihx; s1[le][4][i] = r[4] * ihy; s1[le][5][i] = r[5] * ihz;
+      s1[le][6][i] = r[6];
+    }
+    __syncthreads();
+    if (live) {   // integration Y: index (q1 = c1, a2 = c2, a3 = c3), sums over q2
+      double r[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+      for (int q2 = 0; q2 < 3; ++q2) {
+        const int j = c1 + 3 * q2 + 9 * c3;
+        const double b = b1d(q2, c2), d = d1d(q2, c2);
+        r[0] = fma(b, s1[le][0][j], r[0]);
+        r[1] = fma(d, s1[le][1][j], fma(b, s1[le][2][j], r[1]));
+        r[2] = fma(b, s1[le][3][j], r[2]);
+        r[3] = fma(d, s1[le][4][j], fma(b, s1[le][5][j], r[3]));
+        r[4] = fma(b, s1[le][6][j], r[4]);
+      }
+#pragma unroll
+      for (int k = 0; k < 5; ++k) s2[le][k][i] = r[k];
+    }
+    __syncthreads();
+    if (live) {   // integration X: the node (a1 = c1, a2 = c2, a3 = c3), sums over q1
+      double ra = 0.0, rs = 0.0, rp = 0.0;
+#pragma unroll
+      for (int q1 = 0; q1 < 3; ++q1) {
+        const int j = q1 + 3 * c2 + 9 * c3;
+        const double b = b1d(q1, c1), d = d1d(q1, c1);
+        ra = fma(d, s2[le][0][j], fma(b, s2[le][1][j], ra));
+        rs = fma(d, s2[le][2][j], fma(b, s2[le][3][j], rs));
+        rp = fma(b, s2[le][4][j], rp);
+      }
+      if (o.ye[0]) o.ye[0][(int64_t)i * L.ne + e] = ra;
+      if (o.ye[1]) o.ye[1][(int64_t)i * L.ne + e] = rs;
+      if (o.ye[2]) o.ye[2][(int64_t)i * L.ne + e] = rp;
     }
   }
 }
@@ -855,5 +919,67 @@ extern "C" int hm_lattice_vectors(const hm_lattice* h, const double* d_u, const 
     if (zero_ess_vectors && d_ess && i != 2)
       k_zero_marked<<<grid1(L.ndof, 256), 256, 0, s>>>(L.ndof, d_ess, outs[i]);
   }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+// ======================================================== boundary mass (Robin term)
+// beta * int_{boundary} phi_n phi_c ds added to a block's values in the lattice pattern:
+// the boundary-integrator term of the prior's operator (modeling/prior.py:941-944).  On
+// the box's face x = 0 the integrand is phi_i(0) phi_ci(0) (= 1 for i = ci = 0) times the
+// y and z 1D factors, so each entry gains, per face holding both nodes, the product of
+// the two in-face 1D assembled mass entries.  One warp per boundary row.
+namespace hm {
+// 1D assembled Q2 mass entry between nodes i and c on an axis of n elements of size h
+// (3-point Gauss, exact for the products): sum over the elements holding both
+__device__ __forceinline__ double mass_1d(int i, int c, int n, double h) {
+  const int hi = i > c ? i : c, lo = i < c ? i : c;
+  if (hi - lo > 2) return 0.0;
+  double s = 0.0;
+  for (int e = (hi - 1) / 2 < 0 ? 0 : (hi - 1) / 2; e <= lo / 2 && e < n; ++e) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) t += wq(q) * bq(q, i - 2 * e) * bq(q, c - 2 * e);
+    s += h * t;
+  }
+  return s;
+}
+
+__global__ void k_boundary_mass(Lattice L, double beta, double* __restrict__ vals) {
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= L.ndof) return;
+  const int i = (int)(row % L.Nx), j = (int)((row / L.Nx) % L.Ny), k = (int)(row / ((int64_t)L.Nx * L.Ny));
+  const bool on[3] = {i == 0 || i == L.Nx - 1, j == 0 || j == L.Ny - 1, k == 0 || k == L.Nz - 1};
+  if (!on[0] && !on[1] && !on[2]) return;
+  const int n1 = stencil_n(i, L.Nx), n2 = stencil_n(j, L.Ny), n3 = stencil_n(k, L.Nz);
+  const int lo1 = stencil_lo(i), lo2 = stencil_lo(j), lo3 = stencil_lo(k);
+  const int kd = ((k - lo3) * n2 + (j - lo2)) * n1 + (i - lo1);
+  const int len = n1 * n2 * n3;
+  const int64_t base = row_start(L, i, j, k);
+  for (int pos = lane; pos < len; pos += 32) {
+    const int rank = pos == 0 ? kd : (pos <= kd ? pos - 1 : pos);
+    const int k1 = rank % n1, t = rank / n1, k2 = t % n2, k3 = t / n2;
+    const int c[3] = {lo1 + k1, lo2 + k2, lo3 + k3};
+    const int r[3] = {i, j, k};
+    double add = 0.0;
+    // the faces normal to axis d: the row and the column on the same face
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (!on[d] || c[d] != r[d]) continue;
+      const int a = (d + 1) % 3, b = (d + 2) % 3;
+      const int na[3] = {L.nx, L.ny, L.nz};
+      const double ha[3] = {L.hx, L.hy, L.hz};
+      add += mass_1d(r[a], c[a], na[a], ha[a]) * mass_1d(r[b], c[b], na[b], ha[b]);
+    }
+    if (add != 0.0) vals[base + pos] += beta * add;
+  }
+}
+}  // namespace hm
+
+extern "C" int hm_lattice_add_boundary_mass(const hm_lattice* h, double beta, double* d_vals,
+                                            void* stream) {
+  if (!h || !d_vals) return HM_ERR_ARG;
+  const Lattice& L = *hm_lattice_geometry(h);
+  k_boundary_mass<<<grid1(L.ndof * 32, 256), 256, 0, S_(stream)>>>(L, beta, d_vals);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }

@@ -555,18 +555,29 @@ __global__ void __launch_bounds__(256, 2)
       S.runstart[run] = a0 + ((want - a0) & 1);
       S.runlen[run] = run_sel(run, true);
     } else {
-      int off = 0;
-      for (int q = 0; q <= run; ++q) {
-        const int wq_ = kBulk ? (S.rowptr[q] & 1) : 0;
-        off += (wq_ - off) & 1;
-        int len = 0;
-        for (int r1 = 0; r1 < 4; ++r1) {
-          if (q == run) S.rowoff[run * 4 + r1] = off + len;
-          len += S.nst[0][r1] * S.nst[1][q & 3] * S.nst[2][q >> 2];
-        }
-        if (q == run) { S.runstart[run] = off; S.runlen[run] = len; }
-        off += len;
+      // this run's length and its rows' offsets in it; then the runs in order, each at
+      // the first slot after the previous one with its parity: a scan over the 16
+      // (length, parity) pairs, which every lane runs on shuffled copies
+      const int n23 = S.nst[1][run & 3] * S.nst[2][run >> 2];
+      int part[4], len = 0;
+#pragma unroll
+      for (int r1 = 0; r1 < 4; ++r1) {
+        part[r1] = len;
+        len += S.nst[0][r1] * n23;
       }
+      int off = 0, mine = 0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int lq = __shfl_sync(0xffffu, len, q);
+        const int wq_ = __shfl_sync(0xffffu, want, q);
+        off += (wq_ - off) & 1;
+        if (q == run) mine = off;
+        off += lq;
+      }
+      S.runstart[run] = mine;
+      S.runlen[run] = len;
+#pragma unroll
+      for (int r1 = 0; r1 < 4; ++r1) S.rowoff[run * 4 + r1] = mine + part[r1];
     }
   }
   __syncthreads();

@@ -237,59 +237,116 @@ class _BilaplacianRsolver:
 
 class BiLaplacianPrior:
     """Matern-class Gaussian prior with precision ``R = A M^{-1} A``,
-    ``A = gamma K + delta M`` (isotropic, natural boundary conditions):
-    BiLaplacianPrior of modeling/prior.py:894-952 (no ``Theta``, no Robin term, no
-    lumped mass).
+    ``A = gamma div(Theta grad) + delta M`` with natural boundary conditions, plus with
+    ``robin_bc`` the boundary term ``beta M_boundary``, ``beta = sqrt(gamma delta) /
+    1.42``: BiLaplacianPrior of modeling/prior.py:894-952.  ``Theta``: ``None``
+    (isotropic), a scalar, or a constant diagonal tensor (a 3-vector or a diagonal 3 x 3
+    array); a tensor with off-diagonal entries or a spatially varying one, and the lumped
+    mass, are not part of this prior.
 
     The operators come from the fused assembly kernel on the lattice's pattern: ``gamma
     K`` is the Jacobian block ``A`` at the constant field ``m = log gamma``, and
     ``delta M`` the block ``W_mm`` at ``u = p = x`` (so that ``grad u . grad p = 1``) and
-    ``m = log delta``; no Dirichlet elimination.  Solves with ``A`` and ``M`` are
-    Jacobi-PCG to ``rel_tol``."""
+    ``m = log delta``; no Dirichlet elimination.  A diagonal ``Theta`` scales the
+    element sizes of the stiffness lattice to ``h / sqrt(theta)`` (the derivative terms
+    take ``theta / h^2``) with ``m = log gamma + log(theta_x theta_y theta_z) / 2``
+    restoring ``|J|``; the Robin term is added by ``hm_lattice_add_boundary_mass``.
+    Solves with ``A`` and ``M`` are Jacobi-PCG to ``rel_tol``."""
 
-    def __init__(self, Vh, gamma, delta, mean=None, rel_tol=1e-12, max_iter=1000,
-                 robin_bc=False):
+    def __init__(self, Vh, gamma, delta, Theta=None, mean=None, rel_tol=1e-12, max_iter=1000,
+                 robin_bc=False, lumped_mass=False):
+        import math
+
+        import numpy as np
+
+        from .mesh import BoxMesh
         from .pattern import LatticePattern
-        from .problem import PDEVariationalProblem
         from .sparse import CSRBlock
 
-        if robin_bc:
-            raise NotImplementedError("the Robin boundary term is not part of this prior")
+        if lumped_mass:
+            raise NotImplementedError("the lumped mass is not part of this prior")
         if not (gamma > 0 and delta > 0):
             raise ValueError("gamma and delta must be positive")
+        theta = self._theta(Theta)
         self.Vh = Vh
         mesh = Vh.mesh
-        self.gamma, self.delta, self.robin_bc = float(gamma), float(delta), False
+        self.gamma, self.delta, self.robin_bc = float(gamma), float(delta), bool(robin_bc)
+        self.Theta = theta
         pat = LatticePattern(mesh)
-        prob = PDEVariationalProblem([Vh, Vh, Vh], f=0.0, check_finite=True)
-        prob._pattern = pat
-        x = torch.as_tensor(mesh.node_coords()[:, 0], device=mesh.device).contiguous()
-        zero = Vh.vector()
-        const = Vh.vector()
 
-        def block(name, u, logc, p):
+        status = torch.zeros(1, dtype=torch.int32, device=mesh.device)
+        quad = torch.empty((mesh.quad_bytes() + 7) // 8, dtype=torch.float64, device=mesh.device)
+
+        def block(msh, name, u, logc, p):
+            # msh: the lattice of the prior's mesh, or its rescaled copy (same pattern)
+            const = Vh.vector()
             const.fill_(float(logc))
-            quad = prob._quadrature([u, const, p], "prior")
+            check(lib.hm_lattice_quadrature(msh.handle, ptr(u), ptr(const), ptr(p), _lib.HM_FP64,
+                                            ptr(quad), ptr(status), stream_ptr()),
+                  "hm_lattice_quadrature")
             vals = pat.new_values()
             check(lib.hm_lattice_assemble(
-                mesh.handle, ptr(quad), _lib.HM_FP64, ptr(pat.indptr), None, 0.0,
+                msh.handle, ptr(quad), _lib.HM_FP64, ptr(pat.indptr), None, 0.0,
                 ptr(vals) if name == "A" else None, None, None,
                 ptr(vals) if name == "Wmm" else None, None, None, None, 0, stream_ptr()),
                 "hm_lattice_assemble")
-            prob._require_finite("the prior's operators")
+            if int(status.item()) & _lib.HM_STATUS_NONFINITE:
+                raise RuntimeError("non-finite values in the prior's operators")
             return vals
 
-        import math
-        K = block("A", zero, math.log(self.gamma), zero)
-        Md = block("Wmm", x, math.log(self.delta), x)
-        M1 = block("Wmm", x, 0.0, x)
-        self.A = CSRBlock(pat, K.add_(Md))
+        x = torch.as_tensor(mesh.node_coords()[:, 0], device=mesh.device).contiguous()
+        zero = Vh.vector()
+        logg = math.log(self.gamma)
+        stiff = mesh
+        if theta is not None and np.all(theta == theta[0]):
+            logg += math.log(theta[0])                      # isotropic: gamma theta
+        elif theta is not None:
+            logg += 0.5 * float(np.sum(np.log(theta)))
+            stiff = BoxMesh(mesh.n, tuple(Ld / math.sqrt(t) for Ld, t in zip(mesh.L, theta)),
+                            device=mesh.device)
+        K = block(stiff, "A", zero, logg, zero)
+        Md = block(mesh, "Wmm", x, math.log(self.delta), x)
+        M1 = block(mesh, "Wmm", x, 0.0, x)
+        K.add_(Md)
+        if self.robin_bc:
+            beta = math.sqrt(self.gamma * self.delta) / 1.42
+            check(lib.hm_lattice_add_boundary_mass(mesh.handle, beta, ptr(K), stream_ptr()),
+                  "hm_lattice_add_boundary_mass")
+        self.A = CSRBlock(pat, K)
         self.M = CSRBlock(pat, M1)
         self.Msolver = _BlockSolver(self.M, rel_tol, max_iter)
         self.Asolver = _BlockSolver(self.A, rel_tol, max_iter)
         self.R = _BilaplacianR(self.A, self.Msolver)
         self.Rsolver = _BilaplacianRsolver(self.Asolver, self.M)
         self.mean = mean.clone() if mean is not None else Vh.vector()
+
+    @staticmethod
+    def _theta(Theta):
+        """``None`` or the three diagonal entries of a constant ``Theta``."""
+        import numbers
+
+        import numpy as np
+
+        if Theta is None:
+            return None
+        if isinstance(Theta, numbers.Number):
+            t = np.full(3, float(Theta))
+        else:
+            a = np.asarray(Theta, dtype=float)
+            if a.shape == (3,):
+                t = a.copy()
+            elif a.shape == (3, 3):
+                if np.any(a - np.diag(np.diag(a))):
+                    raise NotImplementedError("Theta with off-diagonal entries is not part of "
+                                              "this prior (the lattice kernels assemble "
+                                              "axis-aligned diffusion)")
+                t = np.diag(a).copy()
+            else:
+                raise NotImplementedError("Theta must be a scalar, a 3-vector or a constant "
+                                          "diagonal 3 x 3 array")
+        if not np.all(t > 0):
+            raise ValueError("Theta must be positive definite")
+        return t
 
     def init_vector(self, x=None, dim=0):
         return self.Vh.vector()

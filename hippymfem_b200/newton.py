@@ -282,7 +282,7 @@ class ReducedSpaceNewtonCG:
         raise ValueError("unknown globalization %r" % (g,))
 
     def _solve_tr(self, x):
-        """Trust-region globalization (NewtonCG.py:377-510): the Newton step from
+        """Trust-region globalization (NewtonCG.py:377-493): the Newton step from
         Steihaug CG inside the region ``mhat^T R mhat <= delta^2`` of the prior's
         precision (the first step unrestricted, setting ``delta = max(5 |mhat|_R, 1)``),
         accepted when the actual over the predicted reduction exceeds ``eta``; the radius

@@ -147,6 +147,12 @@ int hm_lattice_assemble(const hm_lattice* h, const void* d_quad, int precision,
                         double* d_vals_Wmm, double* d_vec_state, double* d_vec_param,
                         double* d_vec_adjoint, int zero_ess_vectors, void* stream);
 
+/* beta * (boundary mass) added in place to a block's values in the lattice pattern
+ * (d_vals, nnz of hm_lattice_sizes): beta int_{boundary} phi_n phi_c ds over the whole
+ * box boundary, the Robin term the reference's BiLaplacianPrior adds with robin_bc=True
+ * (beta = sqrt(gamma delta) / 1.42, modeling/prior.py:941-944). */
+int hm_lattice_add_boundary_mass(const hm_lattice* h, double beta, double* d_vals, void* stream);
+
 /* The assembled vectors straight from the fields, without the pointwise-data
  * workspace: dR/du (STATE), dR/dm (PARAMETER), dR/dp (ADJOINT, with the source f) at
  * (u, m, p), or with d_mhat != NULL the second-order products along mhat (D = w|J| e^m

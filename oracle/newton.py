@@ -18,7 +18,7 @@ What it follows (paths relative to the hIPPyMFEM tree):
   reorthogonalization against the earlier residuals, and with or without the trust
   region of ``set_TR`` / ``update_x_with_TR`` / ``_tau_to_boundary`` /
   ``_negative_curvature`` (``:117-197``);
-* :func:`newton_cg_tr` -- ``ReducedSpaceNewtonCG._solve_tr`` (``NewtonCG.py:377-510``):
+* :func:`newton_cg_tr` -- ``ReducedSpaceNewtonCG._solve_tr`` (``NewtonCG.py:377-493``):
   the radius from the first step, the ratio test with ``eta``, the radius updates;
 * :func:`armijo` -- ``armijo_backtrack`` (``hippymfem/algorithms/linesearch.py:12-62``);
 * :class:`InverseProblem` -- the model the algorithm drives, for the Q2 log-conductivity

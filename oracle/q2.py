@@ -41,6 +41,9 @@ What each function follows in the reference (paths relative to the hIPPyMFEM tre
   (``TrueHessian``) and ``modeling/PDEVariationalProblem.py:1583-1609``
   (``solveIncremental``: right-hand side zeroed on the essential dofs), with a
   Jacobi-PCG standing in for hypre BoomerAMG-PCG (unavailable here).
+* :func:`boundary_mass` — the boundary integrator the reference's ``BiLaplacianPrior``
+  adds with ``robin_bc=True`` (``modeling/prior.py:941-944``: ``MassIntegrator`` over the
+  boundary elements), integrated face element by face element with the 3x3 Gauss rule.
 * :func:`observation_matrix` — ``modeling/pointwiseObservation.py:36-224`` (rows of basis
   values at the points) and ``modeling/misfit.py:102-110`` (``W_uu = B^T B / sigma^2``).
 """
@@ -401,6 +404,39 @@ def assembled_rows(mesh, u, m, p, rows, ess_mask=None, f=1.0, which=("A", "C", "
 
 
 # ------------------------------------------------------------------- observations
+def boundary_mass(mesh):
+    """``int_{boundary} phi_n phi_c ds`` over the six faces of the box (scipy CSR,
+    ``ndof x ndof``): each face is a grid of Q2 quadrilaterals, each integrated with the
+    3x3 Gauss rule (exact for the products) and scattered by its 9 nodes."""
+    x, w = gauss3()
+    B, _ = lagrange3(x)                        # B[q, a]
+    N = mesh.N
+    rows, cols, vals = [], [], []
+    for d in range(3):
+        a, b = (d + 1) % 3, (d + 2) % 3
+        na, nb = mesh.n[a], mesh.n[b]
+        jac = mesh.h[a] * mesh.h[b]
+        # face-element mass [i1 + 3 i2, j1 + 3 j2] on the reference square
+        Wq = w[:, None] * w[None, :]           # [qa, qb]
+        M = np.einsum("xy,xi,yj,xk,yl->ijkl", Wq, B, B, B, B) * jac   # (ia, ib, ja, jb)
+        M = M.transpose(1, 0, 3, 2).reshape(9, 9)   # [ia + 3 ib, ja + 3 jb]
+        ea, eb = np.meshgrid(np.arange(na), np.arange(nb), indexing="ij")
+        ea, eb = ea.reshape(-1), eb.reshape(-1)
+        loc = np.arange(9)
+        ia = 2 * ea[:, None] + (loc % 3)[None]
+        ib = 2 * eb[:, None] + (loc // 3)[None]
+        for side in (0, N[d] - 1):
+            idx = [None, None, None]
+            idx[d] = np.full_like(ia, side)
+            idx[a], idx[b] = ia, ib
+            nodes = idx[0] + N[0] * (idx[1] + N[1] * idx[2])      # (nface, 9)
+            rows.append(np.repeat(nodes, 9, axis=1).reshape(-1))
+            cols.append(np.tile(nodes, (1, 9)).reshape(-1))
+            vals.append(np.broadcast_to(M.reshape(1, 81), (nodes.shape[0], 81)).reshape(-1))
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                         shape=(mesh.ndof, mesh.ndof))
+
+
 def observation_matrix(mesh, points):
     """Pointwise observation operator ``B``: row ``o`` holds the Q2 basis values at
     ``points[o]`` (``pointwiseObservation.py:36-224``)."""

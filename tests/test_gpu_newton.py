@@ -57,6 +57,61 @@ def test_prior_operators_match_the_oracle_and_known_answers(cuda):
     assert float((back - v).norm()) <= TOL_SOLVE * float(v.norm())
 
 
+def _pattern_values(pat, mat):
+    """The entries of a scipy matrix at the positions of a CSR pattern."""
+    ip, ind = pat[0].astype(np.int64), pat[1].astype(np.int64)
+    rows = np.repeat(np.arange(len(ip) - 1), np.diff(ip))
+    return np.asarray(mat[rows, ind]).ravel()
+
+
+def test_prior_robin_term_and_diagonal_theta(cuda):
+    """robin_bc adds beta times the boundary mass (beta = sqrt(gamma delta) / 1.42; the
+    oracle integrates it face element by face element); a diagonal Theta scales each
+    direction's stiffness (against the oracle on the rescaled lattice and the known
+    answers int gamma theta_d (d_d x_d)^2 = gamma theta_d |Omega|); a scalar Theta is
+    gamma Theta; an off-diagonal Theta is refused."""
+    from hippymfem_b200 import BiLaplacianPrior, BoxMesh, Q2Space
+
+    n, L, gamma, delta = (4, 3, 5), (1.0, 0.7, 1.3), 0.1, 2.0
+    mesh = BoxMesh(n, L)
+    V = Q2Space(mesh)
+    mo = q2.Lattice(n, L)
+    E = mo.edofs()
+    pat = q2.build_tables(E, E, mo.ndof, mo.ndof, True)
+    zero = np.zeros(mo.ndof)
+    x = mesh.node_coords()
+    Md = q2.scatter(pat[2], q2.element_blocks(mo, E, x[:, 0], np.full(mo.ndof, math.log(delta)),
+                                               x[:, 0])["Wmm"], pat[3])
+    base = BiLaplacianPrior(V, gamma, delta).A.values.cpu().numpy()
+    rob = BiLaplacianPrior(V, gamma, delta, robin_bc=True).A.values.cpu().numpy()
+    beta = math.sqrt(gamma * delta) / 1.42
+    want = base + beta * _pattern_values(pat, q2.boundary_mass(mo))
+    assert np.abs(rob - want).max() <= TOL * np.abs(want).max()
+    area = 2 * (L[0] * L[1] + L[1] * L[2] + L[0] * L[2])
+    assert abs(np.sum(rob - base) - beta * area) <= 1e-12 * beta * area      # 1^T B 1 = |dOmega|
+
+    theta = np.array([2.0, 0.5, 3.0])
+    an = BiLaplacianPrior(V, gamma, delta, Theta=np.diag(theta)).A.values.cpu().numpy()
+    K = an - Md
+    ms = q2.Lattice(n, tuple(Ld / math.sqrt(t) for Ld, t in zip(L, theta)))
+    Kref = q2.scatter(pat[2], q2.element_blocks(
+        ms, E, zero, np.full(mo.ndof, math.log(gamma) + 0.5 * np.log(theta).sum()), zero)["A"],
+        pat[3])
+    assert np.abs(K - Kref).max() <= TOL * np.abs(Kref).max()
+    Km = q2.csr(pat, K, (mo.ndof, mo.ndof))
+    vol = L[0] * L[1] * L[2]
+    for d in range(3):
+        got = x[:, d] @ (Km @ x[:, d])
+        assert abs(got - gamma * theta[d] * vol) <= 1e-12 * gamma * theta[d] * vol, d
+    assert abs(x[:, 0] @ (Km @ x[:, 1])) <= 1e-12 * gamma * vol
+    assert np.array_equal(an, BiLaplacianPrior(V, gamma, delta, Theta=theta).A.values.cpu().numpy())
+    iso = BiLaplacianPrior(V, gamma, delta, Theta=2.0).A.values.cpu().numpy()
+    g2 = BiLaplacianPrior(V, 2.0 * gamma, delta).A.values.cpu().numpy()
+    assert np.abs(iso - g2).max() <= TOL * np.abs(g2).max()
+    with pytest.raises(NotImplementedError):
+        BiLaplacianPrior(V, gamma, delta, Theta=np.array([[1.0, 0.2, 0], [0.2, 1, 0], [0, 0, 1]]))
+
+
 def _inverse_problem(n=10, nobs=64, seed=0):
     from hippymfem_b200 import (DirichletBC, Model, PDEVariationalProblem,
                                 PointwiseStateObservation)

@@ -227,3 +227,16 @@ def test_assembled_rows_equal_the_whole_mesh_assembly():
         assert np.array_equal(got_b[name][1], full[sel][order]), name
     for s in range(3):
         assert np.array_equal(got_v[s], q2.assemble_vector(E, ev[s], nd)[rows]), s
+
+
+def test_boundary_mass_known_answers():
+    """The oracle's boundary mass: symmetric, int 1 ds = |boundary|, int x^2 ds by faces."""
+    mo = q2.Lattice((3, 2, 4), (1.0, 0.7, 1.3))
+    B = q2.boundary_mass(mo)
+    assert abs(B - B.T).max() <= 1e-16
+    one = np.ones(mo.ndof)
+    area = 2 * (1.0 * 0.7 + 0.7 * 1.3 + 1.0 * 1.3)
+    assert abs(one @ (B @ one) - area) <= 1e-13 * area
+    x = mo.node_coords()[:, 0]
+    want = 0.7 * 1.3 + 2 * 1.3 / 3 + 2 * 0.7 / 3       # x = 1 face, then the y and z faces
+    assert abs(x @ (B @ x) - want) <= 1e-13 * want
