@@ -496,8 +496,8 @@ __global__ void __launch_bounds__(256, 2)
     clipped |= tt[d] == 0 || 4 * tt[d] + 4 > Nn[d] - 1;
   }
   // the Dirichlet markers of the halo'd nodes [s3][s2][s1] (343, two per thread at most):
-  // loaded now, stored to shared memory once the first phase's fields have landed, so
-  // that the two latencies overlap
+  // loaded now, stored to shared memory at the end of the first phase's z stage, so that
+  // their latency hides behind the first field copy and that stage
   uint8_t em[2] = {0, 0};
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -509,9 +509,10 @@ __global__ void __launch_bounds__(256, 2)
       em[h] = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
   }
   // CSR offsets of the rows (0, r2, r3): the lattice pattern's, computed rather than
-  // loaded.  The caller's indptr is loaded at the same rows and compared once the first
-  // fields have landed (the load's latency hidden behind theirs): a pattern other than
-  // the lattice's is rejected (HM_STATUS_RANGE, nothing written by this tile).
+  // loaded.  The caller's indptr is loaded at the same rows and compared at the end of
+  // the first phase's y stage, before this tile writes anything to global memory (the
+  // load's latency hidden behind the first field copy and two stages): a pattern other
+  // than the lattice's is rejected (HM_STATUS_RANGE, nothing written by this tile).
   int32_t given = 0, expect = 0;
   if (tid < 16) {
     const int r2 = tid & 3, r3 = tid >> 2;
@@ -671,21 +672,11 @@ __global__ void __launch_bounds__(256, 2)
     if (!((pm >> ph) & 1u)) continue;
     const int buf = k & 1;
     const bool ok = mbar_wait(&S.mbar[buf], (uint32_t)(k >> 1) & 1u);
-    if (k == 0) {
-      // the markers: to shared memory, then this thread's elimination masks
-      uint8_t* const es = &S.ess[0][0][0];
-      es[tid] = em[0];
-      if (tid + 256 < 343) es[tid + 256] = em[1];
-      has_ess = __syncthreads_or(em[0] | em[1]) != 0;
-      if (has_ess) ess_masks();
-    }
     // the previous phase's image copies must have left the image before it is rewritten
     if (kBulk && tid < 16) bulk_wait_read();
-    const bool foreign = k == 0 && given != expect;
-    if (__syncthreads_or(!ok || foreign)) {
-      const bool pattern_bad = __syncthreads_or(foreign) != 0;
+    if (__syncthreads_or(!ok)) {
       if (tid == 0) {
-        atomicOr(&g_device_status, pattern_bad ? HM_STATUS_RANGE : HM_STATUS_TIMEOUT);
+        atomicOr(&g_device_status, HM_STATUS_TIMEOUT);
         // the other buffer's copy, if one is in flight, before the CTA leaves
         const int nx = next_phase(ph);
         if (nx >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
@@ -698,6 +689,36 @@ __global__ void __launch_bounds__(256, 2)
     double* const vec = ph == 0 ? nullptr : ph == 1 ? o.vec_adj : ph == 2 ? o.vec_state : o.vec_param;
     const int after = next_phase(ph);
     const int after2 = after >= 0 ? next_phase(after) : -1;
+    // the barrier after the z stage; in the first phase it also takes the markers to
+    // shared memory and then forms this thread's elimination masks
+    auto z_barrier = [&]() {
+      if (k != 0) {
+        __syncthreads();
+        return;
+      }
+      uint8_t* const es = &S.ess[0][0][0];
+      es[tid] = em[0];
+      if (tid + 256 < 343) es[tid + 256] = em[1];
+      has_ess = __syncthreads_or(em[0] | em[1]) != 0;
+      if (has_ess) ess_masks();
+    };
+    // the barrier after the y stage; in the first phase it also compares the row
+    // pointers: false (every thread) when the tile must leave, its copies in flight
+    // (the next phase's, and the one after it, issued into this buffer after the z
+    // stage) waited for
+    auto y_barrier = [&]() -> bool {
+      if (k != 0 || !__syncthreads_or(given != expect)) {
+        if (k != 0) __syncthreads();
+        return true;
+      }
+      if (tid == 0) {
+        atomicOr(&g_device_status, HM_STATUS_RANGE);
+        if (after >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
+        if (after2 >= 0) (void)mbar_wait(&S.mbar[buf], (uint32_t)((k + 2) >> 1) & 1u);
+      }
+      if (kBulk && tid < 16) bulk_wait_all();
+      return false;
+    };
     // with its block, a phase's vector is the block's row sums (summed in the x stage)
     const bool rows = vals != nullptr && vec != nullptr;
     real rs[4] = {0, 0, 0, 0};
@@ -714,7 +735,7 @@ __global__ void __launch_bounds__(256, 2)
         else if (tid < 162) z_task<TM, BI>(W + 27 + zbase, &S.T1[1][zt1]);
         else if (tid < 243) z_task<TR, BI>(W + 54 + zbase, &S.T1[2][zt1]);
       }
-      __syncthreads();
+      z_barrier();
       if ((vec == nullptr || rows) && tid == 0 && after2 >= 0) {
         fence_proxy_async();
         issue_fields(&tmap, S, buf, after2, e1, e2, e3);
@@ -739,7 +760,7 @@ __global__ void __launch_bounds__(256, 2)
           y_task<TM>(&S.T1[0][q3 * kT1P + h1], &S.T2[0][q3 * kT2P + h1], ph == PH_A ? ihx * ihx : ihx);
         }
       }
-      __syncthreads();
+      if (!y_barrier()) return;
       // x: the tile image
       {
         const int r = xp3 * kT2P + xp2 * 9;
@@ -805,7 +826,7 @@ __global__ void __launch_bounds__(256, 2)
       if (ph == PH_C) vec_z<PH_C, BI>(W, U1, tid);
       else if (ph == PH_WUM) vec_z<PH_WUM, BI>(W, U1, tid);
       else vec_z<PH_WMM, BI>(W, U1, tid);
-      __syncthreads();
+      z_barrier();
       if (tid == 0 && after2 >= 0) {
         fence_proxy_async();
         issue_fields(&tmap, S, buf, after2, e1, e2, e3);
@@ -813,7 +834,7 @@ __global__ void __launch_bounds__(256, 2)
       if (ph == PH_C) vec_y<PH_C>(U1, U2, tid);
       else if (ph == PH_WUM) vec_y<PH_WUM>(U1, U2, tid);
       else vec_y<PH_WMM>(U1, U2, tid);
-      __syncthreads();
+      if (!y_barrier()) return;
       if (tid < 64) {
         real y = ph == PH_C ? vec_x<PH_C>(U2, vr1, vr2, vr3, ihx, ihy, ihz)
                : ph == PH_WUM ? vec_x<PH_WUM>(U2, vr1, vr2, vr3, ihx, ihy, ihz)

@@ -128,10 +128,15 @@ def test_assembly_rejects_a_foreign_row_pointer_array(cuda):
     assert st[0] == 0
     wrong = pat.indptr.clone()
     wrong[1:] += 1
+    vals.fill_(float("nan"))
+    vec = torch.full((mesh.ndof,), float("nan"), dtype=torch.float64, device=cuda)
     check(lib.hm_lattice_assemble(mesh.handle, ptr(quad), _lib.HM_FP64, ptr(wrong), None, 1.0,
-                                  ptr(vals), None, None, None, None, None, None, 0, stream_ptr()))
+                                  ptr(vals), None, None, None, ptr(vec), None, None, 0,
+                                  stream_ptr()))
     check(lib.hm_device_status(st.ctypes.data, 1))
     assert st[0] & _lib.HM_STATUS_RANGE
+    # every tile sees a row pointer that is not the lattice's: nothing is written
+    assert bool(torch.isnan(vals).all()) and bool(torch.isnan(vec).all())
 
 
 def test_element_matrices_match_the_oracle(cuda):
