@@ -497,10 +497,19 @@ __global__ void k_diag_A(Lattice L, const real* __restrict__ quad, const uint8_t
         const int e1 = el0[0] + c1, e2 = el0[1] + c2, e3 = el0[2] + c3;
         const int a1 = i - 2 * e1, a2 = j - 2 * e2, a3 = k - 2 * e3;
         const real* Dq = quad + (e1 + (int64_t)L.nx * (e2 + (int64_t)L.ny * e3)) * 216;
+        // the node's 1D values and derivatives at the three points of each axis, once
+        // per element (the products below keep their order)
+        double b[3][3], d[3][3];
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+          b[0][t] = bq(t, a1); b[1][t] = bq(t, a2); b[2][t] = bq(t, a3);
+          d[0][t] = dbq(t, a1); d[1][t] = dbq(t, a2); d[2][t] = dbq(t, a3);
+        }
+#pragma unroll
         for (int q = 0; q < 27; ++q) {
           const int q1 = q % 3, q2 = (q / 3) % 3, q3 = q / 9;
-          const double b1 = bq(q1, a1), b2 = bq(q2, a2), b3 = bq(q3, a3);
-          const double d1 = dbq(q1, a1), d2 = dbq(q2, a2), d3 = dbq(q3, a3);
+          const double b1 = b[0][q1], b2 = b[1][q2], b3 = b[2][q3];
+          const double d1 = d[0][q1], d2 = d[1][q2], d3 = d[2][q3];
           const double s = d1 * d1 * b2 * b2 * b3 * b3 * h2[0] + b1 * b1 * d2 * d2 * b3 * b3 * h2[1] +
                            b1 * b1 * b2 * b2 * d3 * d3 * h2[2];
           acc += (double)Dq[q] * s;

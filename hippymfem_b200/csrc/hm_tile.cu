@@ -496,8 +496,9 @@ __global__ void __launch_bounds__(256, 2)
     clipped |= tt[d] == 0 || 4 * tt[d] + 4 > Nn[d] - 1;
   }
   // the Dirichlet markers of the halo'd nodes [s3][s2][s1] (343, two per thread at most):
-  // loaded now, stored to shared memory at the end of the first phase's z stage, so that
-  // their latency hides behind the first field copy and that stage
+  // loaded now, stored to shared memory at the end of the first phase's y stage (of its
+  // z stage for a vector alone), so that their latency hides behind the first field
+  // copy and those stages
   uint8_t em[2] = {0, 0};
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -509,10 +510,11 @@ __global__ void __launch_bounds__(256, 2)
       em[h] = ess[gx + (int64_t)L.Nx * (gy + (int64_t)L.Ny * gz)];
   }
   // CSR offsets of the rows (0, r2, r3): the lattice pattern's, computed rather than
-  // loaded.  The caller's indptr is loaded at the same rows and compared at the end of
-  // the first phase's y stage, before this tile writes anything to global memory (the
-  // load's latency hidden behind the first field copy and two stages): a pattern other
-  // than the lattice's is rejected (HM_STATUS_RANGE, nothing written by this tile).
+  // loaded.  The caller's indptr is loaded at the same rows and compared at the last
+  // barrier before this tile's first global write (the end of the first phase's x stage,
+  // or of its y stage for a vector alone), the load's latency hidden behind the first
+  // field copy and the stages: a pattern other than the lattice's is rejected
+  // (HM_STATUS_RANGE, nothing written by this tile).
   int32_t given = 0, expect = 0;
   if (tid < 16) {
     const int r2 = tid & 3, r3 = tid >> 2;
@@ -689,9 +691,10 @@ __global__ void __launch_bounds__(256, 2)
     double* const vec = ph == 0 ? nullptr : ph == 1 ? o.vec_adj : ph == 2 ? o.vec_state : o.vec_param;
     const int after = next_phase(ph);
     const int after2 = after >= 0 ? next_phase(after) : -1;
-    // the barrier after the z stage; in the first phase it also takes the markers to
-    // shared memory and then forms this thread's elimination masks
-    auto z_barrier = [&]() {
+    // a barrier that, in the first phase, also takes the markers to shared memory and
+    // then forms this thread's elimination masks (the last barrier before the x stage,
+    // or before a vector's y stage)
+    auto marker_barrier = [&]() {
       if (k != 0) {
         __syncthreads();
         return;
@@ -702,15 +705,16 @@ __global__ void __launch_bounds__(256, 2)
       has_ess = __syncthreads_or(em[0] | em[1]) != 0;
       if (has_ess) ess_masks();
     };
-    // the barrier after the y stage; in the first phase it also compares the row
-    // pointers: false (every thread) when the tile must leave, its copies in flight
-    // (the next phase's, and the one after it, issued into this buffer after the z
-    // stage) waited for
-    auto y_barrier = [&]() -> bool {
-      if (k != 0 || !__syncthreads_or(given != expect)) {
-        if (k != 0) __syncthreads();
+    // a barrier that, in the first phase and with `check`, also compares the row
+    // pointers (the last barrier before the tile's first global write): false (every
+    // thread) when the tile must leave, its copies in flight (the next phase's, and the
+    // one after it, issued into this buffer after the z stage) waited for
+    auto checked_barrier = [&](bool check) -> bool {
+      if (k != 0 || !check) {
+        __syncthreads();
         return true;
       }
+      if (!__syncthreads_or(given != expect)) return true;
       if (tid == 0) {
         atomicOr(&g_device_status, HM_STATUS_RANGE);
         if (after >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
@@ -735,7 +739,7 @@ __global__ void __launch_bounds__(256, 2)
         else if (tid < 162) z_task<TM, BI>(W + 27 + zbase, &S.T1[1][zt1]);
         else if (tid < 243) z_task<TR, BI>(W + 54 + zbase, &S.T1[2][zt1]);
       }
-      z_barrier();
+      __syncthreads();
       if ((vec == nullptr || rows) && tid == 0 && after2 >= 0) {
         fence_proxy_async();
         issue_fields(&tmap, S, buf, after2, e1, e2, e3);
@@ -760,7 +764,7 @@ __global__ void __launch_bounds__(256, 2)
           y_task<TM>(&S.T1[0][q3 * kT1P + h1], &S.T2[0][q3 * kT2P + h1], ph == PH_A ? ihx * ihx : ihx);
         }
       }
-      if (!y_barrier()) return;
+      marker_barrier();
       // x: the tile image
       {
         const int r = xp3 * kT2P + xp2 * 9;
@@ -789,7 +793,7 @@ __global__ void __launch_bounds__(256, 2)
         }
       }
       if (kBulk) fence_proxy_async();   // the image stores, before the async copies read them
-      __syncthreads();
+      if (!checked_barrier(true)) return;
       // the leaders' sums [r1][p3][r2] into the y buffer (free after the x stage); the sums
       // over p3 finish at the end of the phase
       if (rows && (xp2 == 0 || xp2 == 5 || xp2 == 8 || xp2 == 13)) {
@@ -826,7 +830,7 @@ __global__ void __launch_bounds__(256, 2)
       if (ph == PH_C) vec_z<PH_C, BI>(W, U1, tid);
       else if (ph == PH_WUM) vec_z<PH_WUM, BI>(W, U1, tid);
       else vec_z<PH_WMM, BI>(W, U1, tid);
-      z_barrier();
+      marker_barrier();
       if (tid == 0 && after2 >= 0) {
         fence_proxy_async();
         issue_fields(&tmap, S, buf, after2, e1, e2, e3);
@@ -834,7 +838,7 @@ __global__ void __launch_bounds__(256, 2)
       if (ph == PH_C) vec_y<PH_C>(U1, U2, tid);
       else if (ph == PH_WUM) vec_y<PH_WUM>(U1, U2, tid);
       else vec_y<PH_WMM>(U1, U2, tid);
-      if (!y_barrier()) return;
+      if (!checked_barrier(true)) return;
       if (tid < 64) {
         real y = ph == PH_C ? vec_x<PH_C>(U2, vr1, vr2, vr3, ihx, ihy, ihz)
                : ph == PH_WUM ? vec_x<PH_WUM>(U2, vr1, vr2, vr3, ihx, ihy, ihz)

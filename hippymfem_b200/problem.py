@@ -113,6 +113,7 @@ class PDEVariationalProblem:
         self._jac_cache = None
         self.A = self.At = self.C = self.Wuu = self.Wum = self.Wmm = self.Ct = self.Wmu = None
         self._lin_point = None
+        self._lin_vectors = None
         self.gauss_newton_approx = False
         self.solver = self.solver_fwd_inc = self.solver_adj_inc = None
         self.n_calls = {"forward": 0, "adjoint": 0, "incremental_forward": 0,
@@ -213,12 +214,28 @@ class PDEVariationalProblem:
     def _residual(self, x, var=ADJOINT, ess=None):
         """``dR/d(var)`` at ``x`` (modeling/PDEVariationalProblem.py:423), essential
         entries of ``ess`` zeroed."""
-        vecs = self._direct_vectors(x, (var,))
-        self._require_finite("the residual")
-        out = vecs[var]
+        cached = self._lin_vectors.get(var) if self._lin_vectors else None
+        if cached is not None and self._at_linearization_point(x):
+            out = cached.clone()
+        else:
+            vecs = self._direct_vectors(x, (var,))
+            self._require_finite("the residual")
+            out = vecs[var]
         if ess is not None and len(ess):
             out.masked_fill_(self.mesh.ess_marker(ess).bool(), 0.0)
         return out
+
+    def _at_linearization_point(self, x):
+        """``x`` holds the values of the current linearization point (compared on the
+        device, value for value)."""
+        if self._lin_point is None:
+            return False
+        for a, b in zip(self._locals(x), self._lin_point):
+            if (a is None) != (b is None):
+                return False
+            if a is not None and not (a.shape == b.shape and bool(torch.equal(a, b))):
+                return False
+        return True
 
     def _block(self, i, j, x):
         """Block ``(i, j)`` at ``x`` with its elimination policy (``_block``, :448)."""
@@ -301,6 +318,7 @@ class PDEVariationalProblem:
         ``matrix_free`` only the quadrature data is kept and every product is taken
         from it (``apply_ij_at``)."""
         self._lin_point = [v.clone() if v is not None else None for v in self._locals(x)]
+        self._lin_vectors = None
         self.C = self.Wuu = self.Wum = self.Wmm = self.Ct = self.Wmu = None
         self.gauss_newton_approx = bool(gauss_newton_approx)
         self._mf = bool(matrix_free)
@@ -314,8 +332,15 @@ class PDEVariationalProblem:
             names.append("C")
             if not gauss_newton_approx:
                 names += ["Wum", "Wmm"]
-        blocks, _ = self._assemble(quad, blocks=tuple(names)) if names else ({}, {})
+        # the vectors of the assembled blocks come with them (their row sums, summed in
+        # the same pass): dR/dp with C, dR/du with W_um, dR/dm with W_mm, kept for a
+        # residual or gradient asked for at this same point
+        vnames = tuple(v for v, b in ((ADJOINT, "C"), (STATE, "Wum"), (PARAMETER, "Wmm"))
+                       if b in names) if self.precision == _lib.HM_FP64 else ()
+        blocks, vecs = (self._assemble(quad, blocks=tuple(names), vectors=vnames) if names
+                        else ({}, {}))
         self._require_finite("linearization point")
+        self._lin_vectors = vecs
         if need_A:
             A = blocks["A"] if "A" in blocks else self._make_jacobian(quad)
             self._jac_cache = (_Snapshot(m), A, quad)
