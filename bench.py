@@ -2,6 +2,7 @@
 """Benchmark of the Q2 log-conductivity assembly + Hessian-action path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 64]
+                    [--config main|precision|differentiation|solve] [--shard]
 
 Workload (one step): the linearization point of the 64^3 Q2 configuration in FP64 --
 pointwise data of (u, m, p) and one fused assembly of the full block set (A = K, its
@@ -54,6 +55,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", type=int, default=2000,
                     help="requests of the serving trace (0: skip)")
+    ap.add_argument("--shard", action="store_true",
+                    help="the Hessian action sharded over z-slabs of the 64^3 lattice across "
+                         "the ranks (one per GPU; halo exchange by point-to-point messages, "
+                         "plane-ordered dot products; Jacobi-PCG), H-applies/s, strong scaling")
     ap.add_argument("--config", choices=("main", "precision", "differentiation", "solve"),
                     default="main",
                     help="precision: 128^3, FP32 contractions and mixed-precision Hessian "
@@ -874,8 +879,84 @@ def run_solve(a):
     print(json.dumps(line), flush=True)
 
 
+def run_shard(a):
+    """The sharded Hessian action (``shard.ShardedHessian`` with the CUDA slab operators)
+    at the benchmark's m on the 64^3 lattice, seeded u and p, 4096 observations, split
+    into z-slabs, one per rank; every
+    operator of the action is an assembly on the rank's slab after one halo exchange of
+    its input, every inner product a plane-ordered sum of all ranks' plane partials, so
+    the action is bit for bit the same on any number of ranks.  Timed like the main line
+    (CUDA events, barrier on both sides, maximum over the ranks)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from hippymfem_b200 import synthetic
+    from hippymfem_b200.shard import DeviceSlabOps, ShardedHessian, SlabPartition
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    n = (a.n, a.n, a.n)
+    L = (1.0, 1.0, 1.0)
+    part = SlabPartition(n, L, world)
+    N = part.N
+    nd = N[0] * N[1] * N[2]
+    x = np.stack(np.meshgrid(*(np.linspace(0.0, Lv, Nv) for Lv, Nv in zip(L, N)),
+                             indexing="ij"), -1).transpose(2, 1, 0, 3).reshape(-1, 3)
+    m = synthetic.log_conductivity(x, seed=0)
+    rng = np.random.default_rng(0)
+    u, p, d = rng.standard_normal(nd), rng.standard_normal(nd), rng.standard_normal(nd)
+    i = np.arange(nd)
+    ix, iy, iz = i % N[0], (i // N[0]) % N[1], i // (N[0] * N[1])
+    ess = ((ix == 0) | (ix == N[0] - 1) | (iy == 0) | (iy == N[1] - 1) | (iz == 0) |
+           (iz == N[2] - 1)).astype(np.int32)
+    k0, k1 = part.owned_planes(rank)
+    own = [torch.as_tensor(v.reshape(N[2], -1)[k0:k1].copy(), device=dev)
+           for v in (u, m, p, ess, d)]
+    pts = synthetic.interior_points(4096, seed=2)
+    ops = DeviceSlabOps(part, rank, pts, 1e-4, dev)
+    H = ShardedHessian(part, rank, ops, *own[:4], rtol=1e-12)
+    for _ in range(max(1, min(a.warmup, 2))):
+        H.mult(own[4])
+    k = max(1, min(a.steps, 3))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(k):
+        H.mult(own[4])
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    (ms,) = max_over_ranks([e0.elapsed_time(e1)], world, dev)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "sharded Hessian action at %d^3 (z-slabs, Jacobi-PCG rtol 1e-12)" % a.n,
+            "value": k / (ms / 1000.0), "unit": "H-applies/s", "n_gpus": world, "steps": k,
+            "warmup": max(1, min(a.warmup, 2)), "ms_per_step": ms / k,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "pcg_iterations": H.iterations[-2:],
+            "config": {"workload": "TrueHessian action, 4096 pointwise observations, %d^3 Q2 "
+                                   "split into %d z-slabs" % (a.n, world),
+                       "parallelism": "z-slabs x%d" % world}}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
+    if a.shard and a.impl != "reference":
+        run_shard(a)
+        return
     if a.impl == "reference":
         run_reference(a)
     elif a.config == "precision":

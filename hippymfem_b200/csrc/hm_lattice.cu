@@ -760,10 +760,13 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
                                                       const double* __restrict__ p,
                                                       const double* __restrict__ mhat, double f,
                                                       VecOut<3> o, uint32_t* __restrict__ status) {
-  __shared__ double sv[8][4][27];        // node values u, m, p, mhat
-  __shared__ double s1[8][7][27];        // evaluation X / integration Z
-  __shared__ double s2[8][8][27];        // evaluation Y / integration Y
-  __shared__ double sp[8][8][27];        // E(3), F(3), W, source weight at the points
+  // per element: arrays of 27, the element's block padded to 11 (mod 16) doubles, so
+  // that the two elements a warp spans fall on different banks
+  constexpr int kV = 4 * 27 + 15, kA = 7 * 27 + 14, kB = 8 * 27 + 3;
+  __shared__ double sv[8][kV];           // node values u, m, p, mhat
+  __shared__ double s1[8][kA];           // evaluation X / integration Z
+  __shared__ double s2[8][kB];           // evaluation Y / integration Y
+  __shared__ double sp[8][kB];           // E(3), F(3), W, source weight at the points
   const int tid = threadIdx.x, le = tid / 27, i = tid % 27;
   const int c1 = i % 3, c2 = (i / 3) % 3, c3 = i / 9;   // the thread's three indices
   const double ihx = 1.0 / L.hx, ihy = 1.0 / L.hy, ihz = 1.0 / L.hz;
@@ -775,10 +778,10 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
     if (live) {
       const int ex = (int)(e % L.nx), ey = (int)((e / L.nx) % L.ny), ez = (int)(e / ((int64_t)L.nx * L.ny));
       const int64_t node = (2 * ex + c1) + (int64_t)L.Nx * ((2 * ey + c2) + (int64_t)L.Ny * (2 * ez + c3));
-      sv[le][0][i] = u[node];
-      sv[le][1][i] = m[node];
-      sv[le][2][i] = p[node];
-      sv[le][3][i] = mhat ? mhat[node] : 0.0;
+      sv[le][(0) * 27 + i] = u[node];
+      sv[le][(1) * 27 + i] = m[node];
+      sv[le][(2) * 27 + i] = p[node];
+      sv[le][(3) * 27 + i] = mhat ? mhat[node] : 0.0;
     }
     __syncthreads();
     if (live) {   // X: index (q1 = c1, a2 = c2, a3 = c3), sums over a1
@@ -787,13 +790,13 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       for (int a1 = 0; a1 < 3; ++a1) {
         const int j = a1 + 3 * c2 + 9 * c3;
         const double b = b1d(c1, a1), d = d1d(c1, a1);
-        const double vu = sv[le][0][j], vm = sv[le][1][j], vp = sv[le][2][j], vh = sv[le][3][j];
+        const double vu = sv[le][(0) * 27 + j], vm = sv[le][(1) * 27 + j], vp = sv[le][(2) * 27 + j], vh = sv[le][(3) * 27 + j];
         r[0] = fma(b, vu, r[0]); r[1] = fma(d, vu, r[1]);
         r[2] = fma(b, vp, r[2]); r[3] = fma(d, vp, r[3]);
         r[4] = fma(b, vm, r[4]); r[5] = fma(b, vh, r[5]);
       }
 #pragma unroll
-      for (int k = 0; k < 6; ++k) s1[le][k][i] = r[k];
+      for (int k = 0; k < 6; ++k) s1[le][(k) * 27 + i] = r[k];
     }
     __syncthreads();
     if (live) {   // Y: index (q1 = c1, q2 = c2, a3 = c3), sums over a2
@@ -802,13 +805,13 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       for (int a2 = 0; a2 < 3; ++a2) {
         const int j = c1 + 3 * a2 + 9 * c3;
         const double b = b1d(c2, a2), d = d1d(c2, a2);
-        const double x0 = s1[le][0][j], x1 = s1[le][1][j], x2 = s1[le][2][j], x3 = s1[le][3][j];
+        const double x0 = s1[le][(0) * 27 + j], x1 = s1[le][(1) * 27 + j], x2 = s1[le][(2) * 27 + j], x3 = s1[le][(3) * 27 + j];
         r[0] = fma(b, x0, r[0]); r[1] = fma(b, x1, r[1]); r[2] = fma(d, x0, r[2]);
         r[3] = fma(b, x2, r[3]); r[4] = fma(b, x3, r[4]); r[5] = fma(d, x2, r[5]);
-        r[6] = fma(b, s1[le][4][j], r[6]); r[7] = fma(b, s1[le][5][j], r[7]);
+        r[6] = fma(b, s1[le][(4) * 27 + j], r[6]); r[7] = fma(b, s1[le][(5) * 27 + j], r[7]);
       }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) s2[le][k][i] = r[k];
+      for (int k = 0; k < 8; ++k) s2[le][(k) * 27 + i] = r[k];
     }
     __syncthreads();
     if (live) {   // Z: the point (c1, c2, c3), sums over a3; then the pointwise data
@@ -817,11 +820,11 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       for (int a3 = 0; a3 < 3; ++a3) {
         const int j = c1 + 3 * c2 + 9 * a3;
         const double b = b1d(c3, a3), d = d1d(c3, a3);
-        gu[0] = fma(b, s2[le][1][j], gu[0]); gu[1] = fma(b, s2[le][2][j], gu[1]);
-        gu[2] = fma(d, s2[le][0][j], gu[2]);
-        gp[0] = fma(b, s2[le][4][j], gp[0]); gp[1] = fma(b, s2[le][5][j], gp[1]);
-        gp[2] = fma(d, s2[le][3][j], gp[2]);
-        mv = fma(b, s2[le][6][j], mv); mh = fma(b, s2[le][7][j], mh);
+        gu[0] = fma(b, s2[le][(1) * 27 + j], gu[0]); gu[1] = fma(b, s2[le][(2) * 27 + j], gu[1]);
+        gu[2] = fma(d, s2[le][(0) * 27 + j], gu[2]);
+        gp[0] = fma(b, s2[le][(4) * 27 + j], gp[0]); gp[1] = fma(b, s2[le][(5) * 27 + j], gp[1]);
+        gp[2] = fma(d, s2[le][(3) * 27 + j], gp[2]);
+        mv = fma(b, s2[le][(6) * 27 + j], mv); mh = fma(b, s2[le][(7) * 27 + j], mh);
       }
       gu[0] *= ihx; gu[1] *= ihy; gu[2] *= ihz;
       gp[0] *= ihx; gp[1] *= ihy; gp[2] *= ihz;
@@ -830,10 +833,10 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       const double E0 = D * gu[0], E1 = D * gu[1], E2 = D * gu[2];
       const double F0 = D * gp[0], F1 = D * gp[1], F2 = D * gp[2];
       const double W = D * (gu[0] * gp[0] + gu[1] * gp[1] + gu[2] * gp[2]);
-      sp[le][0][i] = E0; sp[le][1][i] = E1; sp[le][2][i] = E2;
-      sp[le][3][i] = F0; sp[le][4][i] = F1; sp[le][5][i] = F2;
-      sp[le][6][i] = W;
-      sp[le][7][i] = mhat ? 0.0 : -f * wdet;
+      sp[le][(0) * 27 + i] = E0; sp[le][(1) * 27 + i] = E1; sp[le][(2) * 27 + i] = E2;
+      sp[le][(3) * 27 + i] = F0; sp[le][(4) * 27 + i] = F1; sp[le][(5) * 27 + i] = F2;
+      sp[le][(6) * 27 + i] = W;
+      sp[le][(7) * 27 + i] = mhat ? 0.0 : -f * wdet;
       if (!(isfinite(E0) && isfinite(E1) && isfinite(E2) && isfinite(F0) && isfinite(F1) &&
             isfinite(F2) && isfinite(W)))
         atomicOr(status, HM_STATUS_NONFINITE);
@@ -845,17 +848,17 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       for (int q3 = 0; q3 < 3; ++q3) {
         const int j = c1 + 3 * c2 + 9 * q3;
         const double b = b1d(q3, c3), d = d1d(q3, c3);
-        r[0] = fma(b, sp[le][0][j], r[0]);
-        r[1] = fma(b, sp[le][1][j], r[1]);
-        r[2] = fma(d * ihz, sp[le][2][j], fma(b, sp[le][7][j], r[2]));
-        r[3] = fma(b, sp[le][3][j], r[3]);
-        r[4] = fma(b, sp[le][4][j], r[4]);
-        r[5] = fma(d, sp[le][5][j], r[5]);
-        r[6] = fma(b, sp[le][6][j], r[6]);
+        r[0] = fma(b, sp[le][(0) * 27 + j], r[0]);
+        r[1] = fma(b, sp[le][(1) * 27 + j], r[1]);
+        r[2] = fma(d * ihz, sp[le][(2) * 27 + j], fma(b, sp[le][(7) * 27 + j], r[2]));
+        r[3] = fma(b, sp[le][(3) * 27 + j], r[3]);
+        r[4] = fma(b, sp[le][(4) * 27 + j], r[4]);
+        r[5] = fma(d, sp[le][(5) * 27 + j], r[5]);
+        r[6] = fma(b, sp[le][(6) * 27 + j], r[6]);
       }
-      s1[le][0][i] = r[0] * ihx; s1[le][1][i] = r[1] * ihy; s1[le][2][i] = r[2];
-      s1[le][3][i] = r[3] * ihx; s1[le][4][i] = r[4] * ihy; s1[le][5][i] = r[5] * ihz;
-      s1[le][6][i] = r[6];
+      s1[le][(0) * 27 + i] = r[0] * ihx; s1[le][(1) * 27 + i] = r[1] * ihy; s1[le][(2) * 27 + i] = r[2];
+      s1[le][(3) * 27 + i] = r[3] * ihx; s1[le][(4) * 27 + i] = r[4] * ihy; s1[le][(5) * 27 + i] = r[5] * ihz;
+      s1[le][(6) * 27 + i] = r[6];
     }
     __syncthreads();
     if (live) {   // integration Y: index (q1 = c1, a2 = c2, a3 = c3), sums over q2
@@ -864,14 +867,14 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       for (int q2 = 0; q2 < 3; ++q2) {
         const int j = c1 + 3 * q2 + 9 * c3;
         const double b = b1d(q2, c2), d = d1d(q2, c2);
-        r[0] = fma(b, s1[le][0][j], r[0]);
-        r[1] = fma(d, s1[le][1][j], fma(b, s1[le][2][j], r[1]));
-        r[2] = fma(b, s1[le][3][j], r[2]);
-        r[3] = fma(d, s1[le][4][j], fma(b, s1[le][5][j], r[3]));
-        r[4] = fma(b, s1[le][6][j], r[4]);
+        r[0] = fma(b, s1[le][(0) * 27 + j], r[0]);
+        r[1] = fma(d, s1[le][(1) * 27 + j], fma(b, s1[le][(2) * 27 + j], r[1]));
+        r[2] = fma(b, s1[le][(3) * 27 + j], r[2]);
+        r[3] = fma(d, s1[le][(4) * 27 + j], fma(b, s1[le][(5) * 27 + j], r[3]));
+        r[4] = fma(b, s1[le][(6) * 27 + j], r[4]);
       }
 #pragma unroll
-      for (int k = 0; k < 5; ++k) s2[le][k][i] = r[k];
+      for (int k = 0; k < 5; ++k) s2[le][(k) * 27 + i] = r[k];
     }
     __syncthreads();
     if (live) {   // integration X: the node (a1 = c1, a2 = c2, a3 = c3), sums over q1
@@ -880,9 +883,9 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
       for (int q1 = 0; q1 < 3; ++q1) {
         const int j = q1 + 3 * c2 + 9 * c3;
         const double b = b1d(q1, c1), d = d1d(q1, c1);
-        ra = fma(d, s2[le][0][j], fma(b, s2[le][1][j], ra));
-        rs = fma(d, s2[le][2][j], fma(b, s2[le][3][j], rs));
-        rp = fma(b, s2[le][4][j], rp);
+        ra = fma(d, s2[le][(0) * 27 + j], fma(b, s2[le][(1) * 27 + j], ra));
+        rs = fma(d, s2[le][(2) * 27 + j], fma(b, s2[le][(3) * 27 + j], rs));
+        rp = fma(b, s2[le][(4) * 27 + j], rp);
       }
       if (o.ye[0]) o.ye[0][(int64_t)i * L.ne + e] = ra;
       if (o.ye[1]) o.ye[1][(int64_t)i * L.ne + e] = rs;
