@@ -249,18 +249,24 @@ def plane_partials(a, b):
     return (a * b).sum(dim=1)
 
 
-def sharded_dot(part, a, b, group=None):
-    """a . b over all ranks' owned planes, summed plane by plane in order."""
+def sharded_dot_t(part, a, b, group=None):
+    """a . b over all ranks' owned planes, summed plane by plane in order, as a 0-d
+    tensor on the vectors' device (no host synchronisation)."""
     pp = plane_partials(a, b)
     if part.world == 1:
-        return float(pp.sum())
+        return pp.sum()
     sizes = [part.owned_planes(r)[1] - part.owned_planes(r)[0] for r in range(part.world)]
     width = max(sizes)
     mine = torch.zeros(width, dtype=pp.dtype, device=pp.device)
     mine[:pp.numel()] = pp
     bufs = [torch.empty(width, dtype=pp.dtype, device=pp.device) for _ in sizes]
     dist.all_gather(bufs, mine, group=group)
-    return float(torch.cat([b[:s] for b, s in zip(bufs, sizes)]).sum())
+    return torch.cat([b[:s] for b, s in zip(bufs, sizes)]).sum()
+
+
+def sharded_dot(part, a, b, group=None):
+    """a . b over all ranks' owned planes, summed plane by plane in order."""
+    return float(sharded_dot_t(part, a, b, group))
 
 
 class ShardedHessian:
@@ -276,8 +282,9 @@ class ShardedHessian:
     local lattice (vectors of its local planes, flattened)."""
 
     def __init__(self, part, rank, ops, u, m, p, ess, rtol=1e-12, max_iter=20000,
-                 gauss_newton=False, group=None):
+                 gauss_newton=False, group=None, check_every=8):
         self.part, self.rank, self.ops, self.group = part, rank, ops, group
+        self.check_every = max(1, int(check_every))
         self.rtol, self.max_iter, self.gauss_newton = float(rtol), int(max_iter), gauss_newton
         self.shape = tuple(u.shape)
         self.ess = ess.to(torch.bool)
@@ -301,33 +308,47 @@ class ShardedHessian:
     def dot(self, a, b):
         return sharded_dot(self.part, a, b, self.group)
 
+    def dot_t(self, a, b):
+        return sharded_dot_t(self.part, a, b, self.group)
+
     def solve(self, b):
         """A x = b (b zero on the Dirichlet nodes) by Jacobi-PCG from zero to ||r|| <=
-        rtol ||b||; the iteration count is kept."""
+        rtol ||b||; the iteration count is kept.  The scalars stay on the vectors'
+        device; convergence is read every ``check_every`` iterations and frozen on the
+        device when reached (the step length is zero from then on), so the result and
+        the count are those of a check after every iteration."""
         x = torch.zeros_like(b)
-        bb = self.dot(b, b)
-        if bb == 0.0:
+        bb = self.dot_t(b, b)
+        if float(bb) == 0.0:
             self.iterations.append(0)
             return x
         r = b.clone()
         z = r / self.diag
         d = z.clone()
-        rz = self.dot(r, z)
-        tol2 = self.rtol * self.rtol * bb
+        rz = self.dot_t(r, z)
+        tol2 = (self.rtol * self.rtol) * bb
+        zero = torch.zeros((), dtype=b.dtype, device=b.device)
+        done = torch.zeros((), dtype=torch.bool, device=b.device)
+        conv = torch.zeros((), dtype=torch.int64, device=b.device)
         for it in range(1, self.max_iter + 1):
             q = self.apply_A(d)
-            alpha = rz / self.dot(d, q)
-            x.add_(d, alpha=alpha)
-            r.add_(q, alpha=-alpha)
-            if self.dot(r, r) <= tol2:
-                self.iterations.append(it)
-                return x
+            alpha = torch.where(done, zero, rz / self.dot_t(d, q))
+            x.add_(alpha * d)
+            r.sub_(alpha * q)
+            newly = (~done) & (self.dot_t(r, r) <= tol2)
+            conv = torch.where(newly, torch.full_like(conv, it), conv)
+            done = done | newly
+            if it % self.check_every == 0 and bool(done):
+                break
             z = r / self.diag
-            rz_new = self.dot(r, z)
-            d.mul_(rz_new / rz).add_(z)
-            rz = rz_new
-        raise RuntimeError("sharded PCG did not reach rtol %g in %d iterations"
-                           % (self.rtol, self.max_iter))
+            rz_new = self.dot_t(r, z)
+            d = z + torch.where(done, zero, rz_new / rz) * d
+            rz = torch.where(done, rz, rz_new)
+        if not bool(done):
+            raise RuntimeError("sharded PCG did not reach rtol %g in %d iterations"
+                               % (self.rtol, self.max_iter))
+        self.iterations.append(int(conv))
+        return x
 
     def mult(self, x):
         """y = H x on rank's owned planes (collective: every rank calls it)."""
@@ -361,8 +382,8 @@ def local_points(part, rank, points):
 
 class DeviceSlabOps:
     """``ShardedHessian``'s local operators on the GPU: rank's lattice as a ``BoxMesh``
-    and the library's kernels (matrix-free Jacobian, directional quadrature data and the
-    fused vector assembly, the device observation operator)."""
+    and the library's kernels (the matrix-free Jacobian from the point's quadrature data,
+    the assembled vectors straight from the fields, the device observation operator)."""
 
     def __init__(self, part, rank, points, noise_variance, device):
         from .mesh import BoxMesh
@@ -376,6 +397,7 @@ class DeviceSlabOps:
         self.inv_noise = 1.0 / float(noise_variance)
         self.quad = torch.empty(self.mesh.quad_bytes() // 8, dtype=torch.float64, device=device)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self.work = None
 
     def _quadrature(self, u, m, p, mhat=None):
         from . import _lib
@@ -387,17 +409,6 @@ class DeviceSlabOps:
             check(lib.hm_lattice_quadrature_dir(self.mesh.handle, ptr(u), ptr(m), ptr(p), ptr(mhat),
                                                 _lib.HM_FP64, ptr(self.quad), ptr(self.status),
                                                 stream_ptr()))
-
-    def _vectors(self, slots, f=0.0):
-        from . import _lib
-        from ._lib import check, lib, ptr, stream_ptr
-        out = {s: torch.empty(self.mesh.ndof, dtype=torch.float64, device=self.quad.device)
-               for s in slots}
-        check(lib.hm_lattice_assemble(self.mesh.handle, ptr(self.quad), _lib.HM_FP64, None,
-                                      ptr(self.marker), float(f), None, None, None, None,
-                                      ptr(out.get(0)), ptr(out.get(1)), ptr(out.get(2)), 0,
-                                      stream_ptr()))
-        return out
 
     def set_point(self, u, m, p, ess):
         from .sparse import MatrixFreeJacobian
@@ -414,14 +425,27 @@ class DeviceSlabOps:
     def diag_A(self):
         return self.A.diagonal()
 
+    def _direct(self, u, m, p, mhat, slots):
+        """The vectors of ``slots`` straight from the fields (``hm_lattice_vectors``, no
+        source term): STATE 0, PARAMETER 1, ADJOINT 2."""
+        from ._lib import check, lib, ptr, stream_ptr
+        if self.work is None:
+            self.work = torch.empty(lib.hm_lattice_vectors_workspace_bytes(self.mesh.handle, 3) // 8,
+                                    dtype=torch.float64, device=self.quad.device)
+        out = {s: torch.empty(self.mesh.ndof, dtype=torch.float64, device=self.quad.device)
+               for s in slots}
+        check(lib.hm_lattice_vectors(self.mesh.handle, ptr(u), ptr(m), ptr(p), ptr(mhat), 0.0,
+                                     None, ptr(out.get(0)), ptr(out.get(1)), ptr(out.get(2)), 0,
+                                     ptr(self.work), ptr(self.status), stream_ptr()),
+              "hm_lattice_vectors")
+        return out
+
     def dir_products(self, mhat):
-        self._quadrature(self.u, self.m, self.p, mhat.contiguous())
-        v = self._vectors((0, 1, 2))
+        v = self._direct(self.u, self.m, self.p, mhat.contiguous(), (0, 1, 2))
         return (v[2].masked_fill(self.mask, 0.0), v[0].masked_fill(self.mask, 0.0), v[1])
 
     def grad_m(self, u, p):
-        self._quadrature(u.contiguous(), self.m, p.contiguous())
-        return self._vectors((1,))[1]
+        return self._direct(u.contiguous(), self.m, p.contiguous(), None, (1,))[1]
 
     def wuu(self, x):
         if not self.nobs:

@@ -45,8 +45,8 @@ def test_slab_stretches_equal_the_global_assembly(cuda):
 
 
 def test_device_slab_operators_give_the_hessian_action(cuda):
-    """ShardedHessian with the CUDA slab operators (matrix-free Jacobian, directional
-    quadrature data, fused vector assembly, device observation operator) on one rank:
+    """ShardedHessian with the CUDA slab operators (matrix-free Jacobian, the vectors
+    straight from the fields, device observation operator) on one rank:
     the oracle's TrueHessian restatement to the solve tolerance.  The decomposition over
     several ranks is tested with gloo on the CPU (bit for bit against one rank)."""
     from hippymfem_b200.shard import DeviceSlabOps, ShardedHessian, SlabPartition
