@@ -454,6 +454,8 @@ __global__ void __launch_bounds__(256, 2)
   const int t1 = blockIdx.x, t2 = blockIdx.y, t3 = blockIdx.z;
   const int e1 = 2 * t1 - 1, e2 = 2 * t2 - 1, e3 = 2 * t3 - 1;   // first halo'd element
   const int xp2 = tid & 15, xp3 = tid >> 4;    // this thread's x task (p2, p3)
+  // the copy-out of run xp3 is issued by lane 0 or 16 of a warp (two runs per warp)
+  const bool issuer = xp2 == 0;
   // its image offsets in an interior tile, loaded before the set-up's other global reads
   // are waited for (one round trip to memory instead of two)
   const uint4* const tab = reinterpret_cast<const uint4*>(&kTileTabs.inv[xp3][xp2][0]);
@@ -675,7 +677,7 @@ __global__ void __launch_bounds__(256, 2)
     const int buf = k & 1;
     const bool ok = mbar_wait(&S.mbar[buf], (uint32_t)(k >> 1) & 1u);
     // the previous phase's image copies must have left the image before it is rewritten
-    if (kBulk && tid < 16) bulk_wait_read();
+    if (kBulk && issuer) bulk_wait_read();
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicOr(&g_device_status, HM_STATUS_TIMEOUT);
@@ -683,7 +685,7 @@ __global__ void __launch_bounds__(256, 2)
         const int nx = next_phase(ph);
         if (nx >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
       }
-      if (kBulk && tid < 16) bulk_wait_all();
+      if (kBulk && issuer) bulk_wait_all();
       return;
     }
     const real* W = reinterpret_cast<const real*>(S.wbuf[buf]) + phase_off<real>(ph);
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(256, 2)
         if (after >= 0) (void)mbar_wait(&S.mbar[buf ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
         if (after2 >= 0) (void)mbar_wait(&S.mbar[buf], (uint32_t)((k + 2) >> 1) & 1u);
       }
-      if (kBulk && tid < 16) bulk_wait_all();
+      if (kBulk && issuer) bulk_wait_all();
       return false;
     };
     // with its block, a phase's vector is the block's row sums (summed in the x stage)
@@ -804,8 +806,8 @@ __global__ void __launch_bounds__(256, 2)
       // stream the image out, run by run (four consecutive rows, one stretch of CSR)
       const real* O = reinterpret_cast<const real*>(img);
       if constexpr (kBulk) {
-        if (tid < 16) {
-          const int run = tid, a0 = S.runstart[run], len = S.runlen[run];
+        if (issuer) {
+          const int run = xp3, a0 = S.runstart[run], len = S.runlen[run];
           if (len > 0) {
             double* dst = vals + (int64_t)S.rowptr[run];
             const int h = S.rowptr[run] & 1;   // the values are 16-byte aligned
@@ -857,7 +859,7 @@ __global__ void __launch_bounds__(256, 2)
     }
     ++k;
   }
-  if (kBulk && tid < 16) bulk_wait_all();
+  if (kBulk && issuer) bulk_wait_all();
 }
 
 // ------------------------------------------------------------ host side
