@@ -245,6 +245,7 @@ class Server:
         self.group_size = max(1, int(group_size))
         self.group_by_n = {}
         self._groups = {}
+        self._busy = 0           # slots serving a request now
         self._ws = {}            # (slot, n) -> _Workspace
         self._resident = 0
         self.peak_resident = 0
@@ -419,10 +420,13 @@ class Server:
                     return
                 req = pending.popleft()
                 # the oldest request, and (FP64) up to group_size - 1 more of its size and
-                # kind that are waiting, taken in arrival order
+                # kind that are waiting, taken in arrival order -- only from a backlog:
+                # while another slot is idle, a waiting request is served there, in
+                # parallel, rather than in this slot's group
                 group = [req]
                 kmax = self.group_size_for(req.n)
-                if kmax > 1:
+                idle_others = self.slots - 1 - self._busy
+                if kmax > 1 and len(pending) > idle_others:
                     for other in pending:
                         if len(group) >= kmax:
                             break
@@ -439,6 +443,7 @@ class Server:
                         group = group[:j]
                         break
                     got.append((ws, reserved))
+                self._busy += 1
             wss = []
             for j, (ws, reserved) in enumerate(got):
                 if ws is None:
@@ -468,6 +473,7 @@ class Server:
                 for ws in wss:
                     ws.in_use = False
                     ws.last_used = t_done
+                self._busy -= 1
                 self._lock.notify_all()
 
     def run(self, requests):
