@@ -418,9 +418,10 @@ def run_ours(a):
     # ------------------------------------------------------------ e2e (public API)
     # Every step copies its fields from pinned host memory, sets the linearization point
     # (all blocks and the vectors of the point in the fused pass) and the gradient dR/dm
-    # through the public API, and copies the gradient back.  The copies run on a copy
-    # stream with two buffer sets, so that step i + 1's inputs and step i - 1's result
-    # move while step i computes; every copy of a timed step is inside the timed region.
+    # through the public API, and copies the gradient back.  The copies run on two copy
+    # streams (host to device, device to host: the two directions of the link) with two
+    # buffer sets, so that step i + 1's inputs and step i - 1's result move while step i
+    # computes; every copy of a timed step is inside the timed region.
     pin = [torch.empty(nd, dtype=torch.float64).pin_memory() for _ in range(3)]
     for h, src in zip(pin, (u_h, m_h, p_h)):
         h.copy_(torch.as_tensor(src))
@@ -429,35 +430,43 @@ def run_ours(a):
     prob._pattern = pat
     ins = [[torch.empty(nd, dtype=torch.float64, device=dev) for _ in range(3)] for _ in range(2)]
     gs = [torch.empty(nd, dtype=torch.float64, device=dev) for _ in range(2)]
-    cstream = torch.cuda.Stream(device=dev)
+    cstream = torch.cuda.Stream(device=dev)            # host -> device
+    dstream = torch.cuda.Stream(device=dev)            # device -> host
     ready = [torch.cuda.Event() for _ in range(2)]     # buffer set b: inputs landed
     done = [torch.cuda.Event() for _ in range(2)]      # buffer set b: its step computed
+    taken = [torch.cuda.Event() for _ in range(2)]     # buffer set b: its gradient copied out
 
-    def h2d(b):
+    def h2d(b, after=None):
         with torch.cuda.stream(cstream):
+            if after is not None:                      # the step that read this set is done
+                cstream.wait_event(after)
             for dst, src in zip(ins[b], pin):
                 dst.copy_(src, non_blocking=True)
             ready[b].record(cstream)
 
     def e2e_run(nsteps, start=None):
-        with torch.cuda.stream(cstream):
+        for cs in (cstream, dstream):
             if start is not None:
-                cstream.wait_event(start)
+                cs.wait_event(start)
         for b in range(min(2, nsteps)):
             h2d(b)
         for i in range(nsteps):
             b = i % 2
             stream.wait_event(ready[b])
+            if i >= 2:                                 # gs[b] copied out two steps ago
+                stream.wait_event(taken[b])
             prob._jac_cache = None                     # a new point: the Jacobian too
             prob.setLinearizationPoint(ins[b])
             prob.evalGradientParameter(ins[b], gs[b])
             done[b].record(stream)
-            with torch.cuda.stream(cstream):
-                cstream.wait_event(done[b])
+            with torch.cuda.stream(dstream):
+                dstream.wait_event(done[b])
                 gpin[b].copy_(gs[b], non_blocking=True)
+                taken[b].record(dstream)
             if i + 2 < nsteps:
-                h2d(b)
+                h2d(b, after=done[b])
         stream.wait_stream(cstream)
+        stream.wait_stream(dstream)
 
     e2e_run(3)
     torch.cuda.synchronize()
@@ -630,8 +639,8 @@ def run_ours(a):
                     "steps": e_steps,
                     "what": "setLinearizationPoint + evalGradientParameter per step, fields "
                             "from pinned host memory and the gradient back; the copies on "
-                            "a copy stream with two buffer sets (step i+1's inputs and "
-                            "step i-1's result move during step i)"},
+                            "two copy streams (one per direction) with two buffer sets "
+                            "(step i+1's inputs and step i-1's result move during step i)"},
             "clocks": ck,
             "serving": serving,
             "gpu_launches": launches_per_step * a.steps,
