@@ -100,6 +100,8 @@ SIGNATURES = {
     "hm_lattice_add_boundary_mass": (_i32, [_p, _d, _p, _p]),
     "hm_lattice_vectors_workspace_bytes": (_i64, [_p, _i32]),
     "hm_lattice_vectors": (_i32, [_p, _p, _p, _p, _p, _d, _p, _p, _p, _p, _i32, _p, _p, _p]),
+    "hm_lattice_vectors_at": (_i32, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _d, _p, _p, _p, _p,
+                                     _p, _p, _p]),
     "hm_dot_workspace_bytes": (_i64, [_i64]),
     "hm_dot": (_i32, [_i64, _p, _p, _p, _p, _p]),
 }

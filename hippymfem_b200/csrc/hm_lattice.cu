@@ -371,7 +371,9 @@ __global__ void __launch_bounds__(256)
     k_node_gather(Lattice L, const real* __restrict__ Ye, const uint8_t* __restrict__ ess,
                   const vec* __restrict__ xin, vec* __restrict__ yout,
                   const vec* __restrict__ dotw, double* __restrict__ part,
-                  double* __restrict__ sc, unsigned* __restrict__ counter, ChebOut c = {}) {
+                  double* __restrict__ sc, unsigned* __restrict__ counter, ChebOut c = {},
+                  const uint32_t* __restrict__ skip = nullptr) {
+  if (skip != nullptr && *skip != 0u) return;    // the whole launch stands down
   const unsigned per_row = (unsigned)L.nx + 1u;                  // pairs + the last node
   const unsigned rows = (unsigned)L.Ny * (unsigned)L.Nz;
   const unsigned task = blockIdx.x * blockDim.x + threadIdx.x;
@@ -759,7 +761,9 @@ __global__ void __launch_bounds__(216, 4) k_elem_vectors(Lattice L, const double
                                                       const double* __restrict__ m,
                                                       const double* __restrict__ p,
                                                       const double* __restrict__ mhat, double f,
-                                                      VecOut<3> o, uint32_t* __restrict__ status) {
+                                                      VecOut<3> o, uint32_t* __restrict__ status,
+                                                      const uint32_t* __restrict__ skip = nullptr) {
+  if (skip != nullptr && *skip != 0u) return;    // the whole launch stands down
   // per element: arrays of 27, the element's block padded to 11 (mod 16) doubles, so
   // that the two elements a warp spans fall on different banks
   constexpr int kV = 4 * 27 + 15, kA = 7 * 27 + 14, kB = 8 * 27 + 3;
@@ -898,6 +902,27 @@ __global__ void k_zero_marked(int64_t n, const uint8_t* __restrict__ ess, double
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n && ess[i]) v[i] = 0.0;
 }
+
+// *same = 0 where (u, m, p) differs from (u0, m0, p0) in any entry (compared as values:
+// NaN differs from itself); *same was set nonzero before
+__global__ void k_points_compare(int64_t n, const double* __restrict__ u, const double* __restrict__ u0,
+                                 const double* __restrict__ m, const double* __restrict__ m0,
+                                 const double* __restrict__ p, const double* __restrict__ p0,
+                                 uint32_t* __restrict__ same) {
+  bool diff = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    diff |= !(u[i] == u0[i]) || !(m[i] == m0[i]) || !(p[i] == p0[i]);
+  if (__syncthreads_or(diff) && threadIdx.x == 0) *same = 0u;
+}
+// out = kept where *same (nonzero), left alone otherwise
+__global__ void k_copy_if_same(int64_t n, const uint32_t* __restrict__ same,
+                               const double* __restrict__ kept, double* __restrict__ out) {
+  if (*same == 0u) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = kept[i];
+}
 }  // namespace hm
 
 extern "C" int64_t hm_lattice_vectors_workspace_bytes(const hm_lattice* h, int nvectors) {
@@ -930,6 +955,44 @@ extern "C" int hm_lattice_vectors(const hm_lattice* h, const double* d_u, const 
         L, o.ye[i], nullptr, nullptr, outs[i], nullptr, nullptr, nullptr, nullptr);
     if (zero_ess_vectors && d_ess && i != 2)
       k_zero_marked<<<grid1(L.ndof, 256), 256, 0, s>>>(L.ndof, d_ess, outs[i]);
+  }
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+extern "C" int hm_lattice_vectors_at(const hm_lattice* h, const double* d_u, const double* d_m,
+                                     const double* d_p, const double* d_u0, const double* d_m0,
+                                     const double* d_p0, const double* d_kept_state,
+                                     const double* d_kept_param, const double* d_kept_adjoint,
+                                     double f, double* d_vec_state, double* d_vec_param,
+                                     double* d_vec_adjoint, void* d_work, uint32_t* d_same,
+                                     uint32_t* d_status, void* stream) {
+  if (!h || !d_u || !d_m || !d_p || !d_u0 || !d_m0 || !d_p0 || !d_work || !d_same || !d_status)
+    return HM_ERR_ARG;
+  double* outs[3] = {d_vec_adjoint, d_vec_state, d_vec_param};
+  const double* kept[3] = {d_kept_adjoint, d_kept_state, d_kept_param};
+  if (!outs[0] && !outs[1] && !outs[2]) return HM_ERR_ARG;
+  for (int i = 0; i < 3; ++i)
+    if (outs[i] && !kept[i]) return HM_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_work) & 7u) != 0) return HM_ERR_ARG;
+  const Lattice& L = *hm_lattice_geometry(h);
+  cudaStream_t s = S_(stream);
+  if (cudaMemsetAsync(d_same, 0xff, sizeof(uint32_t), s) != cudaSuccess) return HM_ERR_CUDA;
+  const int cgrid = (int)(grid1(L.ndof, 256) < 148 * 8 ? grid1(L.ndof, 256) : 148 * 8);
+  k_points_compare<<<cgrid, 256, 0, s>>>(L.ndof, d_u, d_u0, d_m, d_m0, d_p, d_p0, d_same);
+  // the vectors from the fields, every launch standing down when the point is the same
+  double* w = static_cast<double*>(d_work);
+  VecOut<3> o{};
+  int k = 0;
+  for (int i = 0; i < 3; ++i)
+    if (outs[i]) o.ye[i] = w + (int64_t)(k++) * 27 * L.ne;
+  const int64_t groups = (L.ne + 7) / 8;
+  const int grid = (int)(groups < 148 * 16 ? groups : 148 * 16);
+  k_elem_vectors<<<grid, 216, 0, s>>>(L, d_u, d_m, d_p, nullptr, f, o, d_status, d_same);
+  for (int i = 0; i < 3; ++i) {
+    if (!outs[i]) continue;
+    k_node_gather<double, double, 0><<<gather_blocks(L), 256, 0, s>>>(
+        L, o.ye[i], nullptr, nullptr, outs[i], nullptr, nullptr, nullptr, nullptr, ChebOut{}, d_same);
+    k_copy_if_same<<<cgrid, 256, 0, s>>>(L.ndof, d_same, kept[i], outs[i]);
   }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }

@@ -114,6 +114,7 @@ class PDEVariationalProblem:
         self.A = self.At = self.C = self.Wuu = self.Wum = self.Wmm = self.Ct = self.Wmu = None
         self._lin_point = None
         self._lin_vectors = None
+        self._same_word = None
         self.gauss_newton_approx = False
         self.solver = self.solver_fwd_inc = self.solver_adj_inc = None
         self.n_calls = {"forward": 0, "adjoint": 0, "incremental_forward": 0,
@@ -215,7 +216,11 @@ class PDEVariationalProblem:
         """``dR/d(var)`` at ``x`` (modeling/PDEVariationalProblem.py:423), essential
         entries of ``ess`` zeroed."""
         cached = self._lin_vectors.get(var) if self._lin_vectors else None
-        if cached is not None and self._at_linearization_point(x):
+        if cached is not None and not self.check_finite and self._point_complete(x):
+            # the point's vector where x is the point, else from the fields: decided on
+            # the device, without waiting for it
+            out = self._vectors_at(x, var, cached)
+        elif cached is not None and self._at_linearization_point(x):
             out = cached.clone()
         else:
             vecs = self._direct_vectors(x, (var,))
@@ -223,6 +228,36 @@ class PDEVariationalProblem:
             out = vecs[var]
         if ess is not None and len(ess):
             out.masked_fill_(self.mesh.ess_marker(ess).bool(), 0.0)
+        return out
+
+    def _point_complete(self, x):
+        loc = self._locals(x)
+        return (self._lin_point is not None and all(v is not None for v in loc)
+                and all(v is not None for v in self._lin_point)
+                and all(a.shape == b.shape for a, b in zip(loc, self._lin_point)))
+
+    def _vectors_at(self, x, var, kept):
+        """``hm_lattice_vectors_at``: the kept vector of slot ``var`` where ``x`` equals
+        the linearization point value for value, else the vector from the fields."""
+        u, m, p = self._locals(x)
+        u0, m0, p0 = self._lin_point
+        need = lib.hm_lattice_vectors_workspace_bytes(self.mesh.handle, 1)
+        buf = self._quad.get("vectors")
+        if buf is None or buf.numel() * 8 < need:
+            buf = self._quad["vectors"] = torch.empty((need + 7) // 8, dtype=torch.float64,
+                                                      device=self.mesh.device)
+        if self._same_word is None:
+            self._same_word = torch.zeros(1, dtype=torch.int32, device=self.mesh.device)
+        out = self.Vh[var].vector()
+        kept_s = kept if var == STATE else None
+        kept_m = kept if var == PARAMETER else None
+        kept_a = kept if var == ADJOINT else None
+        check(lib.hm_lattice_vectors_at(
+            self.mesh.handle, ptr(u), ptr(m), ptr(p), ptr(u0), ptr(m0), ptr(p0),
+            ptr(kept_s), ptr(kept_m), ptr(kept_a), float(self.f),
+            ptr(out) if var == STATE else None, ptr(out) if var == PARAMETER else None,
+            ptr(out) if var == ADJOINT else None, ptr(buf), ptr(self._same_word),
+            ptr(self._status), stream_ptr()), "hm_lattice_vectors_at")
         return out
 
     def _at_linearization_point(self, x):
@@ -349,8 +384,9 @@ class PDEVariationalProblem:
         self.C = blocks.get("C")
         self.Wum = blocks.get("Wum")
         self.Wmm = blocks.get("Wmm")
-        self.solver_fwd_inc = self._get_solver(self.A)
-        self.solver_adj_inc = self.solver_fwd_inc      # A^T = A: one solver serves both
+        # the incremental solvers are made at the first incremental solve of the point
+        # (a point whose gradient alone is asked for never pays for their set-up)
+        self.solver_fwd_inc = self.solver_adj_inc = None
         return self
 
     def solveIncremental(self, out, rhs, is_adj, rel_tolerance=None):
@@ -360,6 +396,9 @@ class PDEVariationalProblem:
         self.bc0.zero(r)
         out.zero_()
         self.n_calls["incremental_adjoint" if is_adj else "incremental_forward"] += 1
+        if self.solver_fwd_inc is None or self.solver_fwd_inc.op is not self.A:
+            self.solver_fwd_inc = self._get_solver(self.A)
+            self.solver_adj_inc = self.solver_fwd_inc      # A^T = A: one solver serves both
         solver = self.solver_adj_inc if is_adj else self.solver_fwd_inc
         prm = solver.parameters
         own = None

@@ -172,6 +172,20 @@ int hm_lattice_vectors(const hm_lattice* h, const double* d_u, const double* d_m
                        double* d_vec_state, double* d_vec_param, double* d_vec_adjoint,
                        int zero_ess_vectors, void* d_work, uint32_t* d_status, void* stream);
 
+/* The vectors of hm_lattice_vectors at (u, m, p) (no mhat, no elimination) for a caller
+ * that holds them already at a point (u0, m0, p0): the kept vectors d_kept_* (one for
+ * every vector asked for) where (u, m, p) equals (u0, m0, p0) entry for entry, else the
+ * vectors computed from the fields -- decided on the device (d_same: one uint32 of
+ * scratch, nonzero when the points were equal), so the call never waits for the GPU.
+ * The reference's residual and gradient at the linearization point
+ * (modeling/PDEVariationalProblem.py:423, :1365) with its shared pass. */
+int hm_lattice_vectors_at(const hm_lattice* h, const double* d_u, const double* d_m,
+                          const double* d_p, const double* d_u0, const double* d_m0,
+                          const double* d_p0, const double* d_kept_state,
+                          const double* d_kept_param, const double* d_kept_adjoint, double f,
+                          double* d_vec_state, double* d_vec_param, double* d_vec_adjoint,
+                          void* d_work, uint32_t* d_same, uint32_t* d_status, void* stream);
+
 /* Matrix-free Q2 operator y = A(D) x with the Jacobian's elimination (x zeroed on
  * d_ess, y = x there): the product apply_ij_at gives for (ADJOINT, STATE)
  * (modeling/PDEVariationalProblem.py:1672).  Its data d_jac (hm_lattice_jacobian_bytes)

@@ -182,3 +182,40 @@ def test_small_assembled_solves(cuda, n):
     r = V.vector()
     A.mult(x, r)
     assert float((r - b).norm()) <= 1e-10 * float(b.norm())
+
+
+def test_vectors_at_the_point_decided_on_the_device(cuda):
+    """Without finiteness checks the residual and gradient at the linearization point
+    come from hm_lattice_vectors_at, which compares the point on the device: the point's
+    own vectors (its fused pass) where x is the point, the vectors from the fields as
+    soon as one entry differs -- each bit for bit as the synchronous route gives them."""
+    from hippymfem_b200 import (ADJOINT, PARAMETER, STATE, BoxMesh, DirichletBC,
+                                PDEVariationalProblem, Q2Space)
+
+    mesh = BoxMesh((5, 4, 6))
+    V = Q2Space(mesh)
+    bc = DirichletBC(V)
+    sync = PDEVariationalProblem([V, V, V], f=1.0, bc=bc, check_finite=True)
+    fast = PDEVariationalProblem([V, V, V], f=1.0, bc=bc, check_finite=False)
+    rng = np.random.default_rng(21)
+    u, m, p = (torch.as_tensor(rng.standard_normal(mesh.ndof) * s, device=cuda)
+               for s in (1.0, 0.3, 1.0))
+    x = [u, m, p]
+    for prob in (sync, fast):
+        prob.setLinearizationPoint(x)
+    for var in (STATE, PARAMETER, ADJOINT):
+        a, b = sync._residual(x, var), fast._residual(x, var)
+        assert torch.equal(a, b)
+        assert torch.equal(b, fast._lin_vectors[var])        # the point's own vector
+    # one entry moved: every vector from the fields, as the synchronous route computes it
+    x2 = [u.clone(), m.clone(), p]
+    x2[PARAMETER][mesh.ndof // 2] += 1e-3
+    for var in (STATE, PARAMETER, ADJOINT):
+        a, b = sync._residual(x2, var), fast._residual(x2, var)
+        assert torch.equal(a, b)
+        assert not torch.equal(b, fast._lin_vectors[var])
+    # and back at the point
+    g1, g2 = V.vector(), V.vector()
+    sync.evalGradientParameter(x, g1)
+    fast.evalGradientParameter(x, g2)
+    assert torch.equal(g1, g2)
