@@ -508,28 +508,52 @@ class ReducedHessian:
         self.mult(x, Hx)
         return float(torch.dot(Hx, y))
 
+    def _applyCt(self, dp, out):
+        # C^T dp as dR/dm from the point's fields where the problem offers it
+        prob = self.model.problem
+        if hasattr(prob, "transposed_product"):
+            return prob.transposed_product(PARAMETER, ADJOINT, dp, out)
+        return self.model.applyCt(dp, out)
+
     def GNHessian(self, x, y):
         self.model.applyC(x, self.rhs_fwd)
         self._incremental(False, self.uhat, self.rhs_fwd)
         self.model.applyWuu(self.uhat, self.rhs_adj)
         self._incremental(True, self.phat, self.rhs_adj)
-        self.model.applyCt(self.phat, y)
+        self._applyCt(self.phat, y)
         if not self.misfit_only:
             self.model.applyR(x, self.yhelp)
             y.add_(self.yhelp)
         return y
 
     def TrueHessian(self, x, y):
-        self.model.applyC(x, self.rhs_fwd)
+        # C x, W_um x and W_mm x in one pass over the point's fields where the problem
+        # offers it (reducedHessian.py:102-131 takes them as three block products)
+        prob = self.model.problem
+        fwd = (prob.directional_products(x) if hasattr(prob, "directional_products")
+               and not self.model.gauss_newton_approx else None)
+        if fwd is not None:
+            self.rhs_fwd.copy_(fwd[ADJOINT])
+        else:
+            self.model.applyC(x, self.rhs_fwd)
         self._incremental(False, self.uhat, self.rhs_fwd)
         self.model.applyWuu(self.uhat, self.rhs_adj)
-        self.model.applyWum(x, self.rhs_adj2)
-        self.rhs_adj.sub_(self.rhs_adj2)
+        if fwd is not None:
+            self.rhs_adj.sub_(fwd[STATE])
+        else:
+            self.model.applyWum(x, self.rhs_adj2)
+            self.rhs_adj.sub_(self.rhs_adj2)
         self._incremental(True, self.phat, self.rhs_adj)
-        self.model.applyWmm(x, y)
-        self.model.applyCt(self.phat, self.yhelp)
+        if fwd is not None:
+            y.copy_(fwd[PARAMETER])
+        else:
+            self.model.applyWmm(x, y)
+        self._applyCt(self.phat, self.yhelp)
         y.add_(self.yhelp)
-        self.model.applyWmu(self.uhat, self.yhelp)
+        if fwd is not None and hasattr(prob, "transposed_product"):
+            prob.transposed_product(PARAMETER, STATE, self.uhat, self.yhelp)
+        else:
+            self.model.applyWmu(self.uhat, self.yhelp)
         y.sub_(self.yhelp)
         if not self.misfit_only:
             self.model.applyR(x, self.yhelp)

@@ -460,6 +460,28 @@ class PDEVariationalProblem:
         self._dir_cache = (tuple(_Snapshot(v) for v in list(x) + [mhat]), vecs)
         return vecs
 
+    def directional_products(self, mhat):
+        """``{ADJOINT: C mhat, STATE: W_um mhat, PARAMETER: W_mm mhat}`` at the
+        linearization point in one pass over its fields (the row eliminations of C and
+        W_um applied), or None where the point has no FP64 fields to take them from.  The
+        Hessian action's three products along its direction, faster than three products
+        of the assembled blocks, equal to rounding."""
+        if self._lin_point is None or any(v is None for v in self._lin_point):
+            return None
+        vecs = self._direct_vectors(self._lin_point, (ADJOINT, STATE, PARAMETER), mhat=mhat,
+                                    zero_ess=True)
+        self._require_finite("the second-order products")
+        return vecs
+
+    def transposed_product(self, i, j, dir, out):
+        """``C^T dir`` (i, j = PARAMETER, ADJOINT) or ``W_mu dir`` (PARAMETER, STATE) at
+        the linearization point as ``dR/dm`` with the direction in the adjoint or state
+        slot: faster than the transposed product of the assembled block, equal to
+        rounding; through ``apply_ij`` where the point has no FP64 fields."""
+        if self._lin_point is None or any(v is None for v in self._lin_point):
+            return self.apply_ij(i, j, dir, out)
+        return self.apply_ij_at(i, j, self._lin_point, dir, out)
+
     def apply_ij_at(self, i, j, x, dir, out):
         """The ``(i, j)`` block at ``x`` applied to ``dir`` without forming the block
         (:1672): the Jacobian pair through the matrix-free operator; the second-order
