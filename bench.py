@@ -553,40 +553,51 @@ def run_ours(a):
     del H, model, prob
     torch.cuda.empty_cache()
 
-    # the same actions with the lattice multigrid preconditioner (FP64), in a stream of
-    # their own, where the solver replays its iteration batches as CUDA graphs
+    # the same actions with the lattice multigrid preconditioner, in a stream of their
+    # own, where the solver replays its iteration batches as CUDA graphs: the FP64 CG with
+    # the V-cycle in FP64 ("fp64") and in FP32 ("mixed")
     hs = torch.cuda.Stream(device=dev)
-    torch.cuda.synchronize()
-    with torch.cuda.stream(hs):
-        prob = hm.PDEVariationalProblem([V, V, V], f=1.0, bc=bc, preconditioner="mg",
-                                        check_finite=False, solver_tolerance=1e-12)
-        prob._pattern = pat
-        model = hm.Model(prob, None, misfit)
-        model.setPointForHessianEvaluations(x)
-        H = hm.ReducedHessian(model)
-        H.mult(v, y)
-        hs.synchronize()
-        lat_mg = []
-        H.iterations.clear()
-        for _ in range(a.happly):
-            h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            h0.record(hs)
+
+    def mg_actions(solver_precision):
+        torch.cuda.synchronize()
+        with torch.cuda.stream(hs):
+            prob = hm.PDEVariationalProblem([V, V, V], f=1.0, bc=bc, preconditioner="mg",
+                                            check_finite=False, solver_tolerance=1e-12,
+                                            solver_precision=solver_precision)
+            prob._pattern = pat
+            model = hm.Model(prob, None, misfit)
+            model.setPointForHessianEvaluations(x)
+            H = hm.ReducedHessian(model)
             H.mult(v, y)
-            h1.record(hs)
             hs.synchronize()
-            lat_mg.append(h0.elapsed_time(h1))
-    torch.cuda.synchronize()
-    mg_err = float((y - y64).norm() / y64.norm())
-    iters_mg = list(H.iterations)
+            lats = []
+            H.iterations.clear()
+            for _ in range(a.happly):
+                h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                h0.record(hs)
+                H.mult(v, y)
+                h1.record(hs)
+                hs.synchronize()
+                lats.append(h0.elapsed_time(h1))
+        torch.cuda.synchronize()
+        its = list(H.iterations)
+        del H, model, prob
+        torch.cuda.empty_cache()
+        return lats, y.clone(), its
+
+    lat_mg, y_mg, iters_mg = mg_actions("fp64")
+    mg_err = float((y_mg - y64).norm() / y64.norm())
+    lat_mg32, y_mg32, iters_mg32 = mg_actions("mixed")
+    mg32_err = float((y_mg32 - y64).norm() / y64.norm())
+    mg32_vs_mg = float((y_mg32 - y_mg).norm() / y_mg.norm())
     ck = clocks.stop()
-    del H, model, prob
-    torch.cuda.empty_cache()
 
     # the latency figures of the three solvers: each the maximum over the ranks
     def lat_stats(ls):
         return [statistics.mean(ls), float(np.percentile(ls, 50)), float(np.percentile(ls, 99))]
 
-    hs_mg, hs_j, hs_32 = (max_over_ranks(lat_stats(ls), world, dev) for ls in (lat_mg, lat, lat32))
+    hs_mg, hs_j, hs_32, hs_mg32 = (max_over_ranks(lat_stats(ls), world, dev)
+                                   for ls in (lat_mg, lat, lat32, lat_mg32))
     mg_degree = default_smoothing_degree(mesh)
 
     serving = None
@@ -644,6 +655,16 @@ def run_ours(a):
                                   "(Q2 -> Q1 -> coarser Q1, Chebyshev-Jacobi degree %d, the coarsest "
                                   "level solved exactly when it has at most 64 interior "
                                   "nodes), rtol 1e-12" % mg_degree},
+            "multigrid_fp32_cycle": {
+                "h_applies_per_s": whole_job_rate(1, hs_mg32[0], world),
+                "latency_ms": {"p50": hs_mg32[1], "p99": hs_mg32[2]},
+                "rel_err_vs_jacobi": mg32_err, "rel_err_vs_fp64_cycle": mg32_vs_mg,
+                "speedup_vs_fp64_cycle": hs_mg[0] / hs_mg32[0],
+                "speedup_vs_fp64_jacobi": hs_j[0] / hs_mg32[0],
+                "pcg_iterations": iters_mg32,
+                "what": "the same FP64 PCG (recurrence, inner products and stopping test in "
+                        "FP64, rtol 1e-12) with the V-cycle run in FP32 on single-precision "
+                        "copies of the level data"},
             "e2e": {"value": e2e_value, "unit": "elements/s",
                     "h2d_bytes_per_step": 3 * 8 * nd, "d2h_bytes_per_step": 8 * nd,
                     "steps": e_steps,

@@ -80,6 +80,8 @@ SIGNATURES = {
     "hm_mg_levels": (_i32, [_p]),
     "hm_mg_set_tail_nodes": (_i32, [_p, _i64]),
     "hm_mg_set_fused": (_i32, [_p, _i32]),
+    "hm_mg_single_workspace_bytes": (_i64, [_p]),
+    "hm_mg_set_single": (_i32, [_p, _p, _p]),
     "hm_mg_destroy": (_i32, [_p]),
     "hm_pcg_mg": (_i32, [_p, _p, _p, _d, _i32, _i32, _p, _p, _p, _p]),
     "hm_pcg_plan_set_mg": (_i32, [_p, _p]),

@@ -52,3 +52,15 @@ int hm_launch_cheb1_from_zero(const hm::Lattice& L, void* jac, const uint8_t* es
                               void* stream);
 int hm_launch_cheb1_from_x(const hm::Lattice& L, void* jac, const uint8_t* ess, const double* b,
                            const double* idiag, const double* cheb, double* x, void* stream);
+// the FP32 operator (jac32: the points' D in FP32, then the FP32 element results) on
+// FP32 vectors; clean: x zero on the Dirichlet nodes
+int hm_launch_apply_A32(const hm::Lattice& L, void* jac32, const uint8_t* ess, const float* x,
+                        float* y, bool clean, void* stream);
+// the two fused smoothing steps above with the FP32 operator: from zero, b FP64 in, x and
+// r FP32 out; from x (FP32), the result z = x + (b - A x) idiag / theta written in FP64
+int hm_launch_cheb1_from_zero32(const hm::Lattice& L, void* jac32, const uint8_t* ess,
+                                const double* b, const double* idiag, const double* cheb,
+                                float* x, float* r, void* stream);
+int hm_launch_cheb1_from_x32(const hm::Lattice& L, void* jac32, const uint8_t* ess, const double* b,
+                             const double* idiag, const double* cheb, const float* x, double* z,
+                             void* stream);

@@ -357,21 +357,25 @@ __device__ __forceinline__ void axis_elems(int i, int nel, int& e0, int& a0, int
 //   0  yout = y
 //   1  the first smoothing step from zero (the input was d = b c.diag / theta):
 //      c.r = b - y, c.x = d
-//   2  one smoothing step from c.x (the input): c.x += (b - y) c.diag / theta, in place
-//      (this pass reads no x but the Dirichlet nodes' own)
-struct ChebOut {
+//   2  one smoothing step from c.x (the input): c.x += (b - y) c.diag / theta, in place,
+//      or into c.z (FP64) when given (this pass reads no x but the Dirichlet nodes' own)
+// c.r and c.x are in the vector type V (the updates are formed in FP64 and rounded once)
+template <typename V>
+struct ChebOutT {
   const double* b;
   const double* diag;
   const double* cheb;
-  double* r;
-  double* x;
+  V* r;
+  V* x;
+  double* z;
 };
+using ChebOut = ChebOutT<double>;
 template <typename real, typename vec, int OUT = 0>
 __global__ void __launch_bounds__(256)
     k_node_gather(Lattice L, const real* __restrict__ Ye, const uint8_t* __restrict__ ess,
                   const vec* __restrict__ xin, vec* __restrict__ yout,
                   const vec* __restrict__ dotw, double* __restrict__ part,
-                  double* __restrict__ sc, unsigned* __restrict__ counter, ChebOut c = {},
+                  double* __restrict__ sc, unsigned* __restrict__ counter, ChebOutT<vec> c = {},
                   const uint32_t* __restrict__ skip = nullptr) {
   if (skip != nullptr && *skip != 0u) return;    // the whole launch stands down
   const unsigned per_row = (unsigned)L.nx + 1u;                  // pairs + the last node
@@ -441,14 +445,16 @@ __global__ void __launch_bounds__(256)
         const double bn = c.b[nn];
         if constexpr (OUT == 1) {
           const double d = __dmul_rn(inv_theta * bn, c.diag[nn]);
-          const double y = fx ? d : acc;
-          c.r[nn] = bn - y;
-          c.x[nn] = d;
+          const double y = fx ? (double)(vec)d : acc;
+          c.r[nn] = (vec)(bn - y);
+          c.x[nn] = (vec)d;
         } else {
-          const double xn = c.x[nn];
+          const double xn = (double)c.x[nn];
           const double y = fx ? xn : acc;
           // the update rounded on its own before the add, as the step-by-step smoother
-          c.x[nn] = xn + __dmul_rn(inv_theta * (bn - y), c.diag[nn]);
+          const double xnew = xn + __dmul_rn(inv_theta * (bn - y), c.diag[nn]);
+          if (c.z != nullptr) c.z[nn] = xnew;
+          else c.x[nn] = (vec)xnew;
         }
       }
     }
@@ -602,7 +608,7 @@ int hm_launch_cheb1_from_zero(const Lattice& L, void* jac, const uint8_t* ess, c
   const int64_t warps = (L.ne + 9) / 10;
   k_elem_apply<double, double, false, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(
       L, Dq, ess, b, Ye, idiag, cheb);
-  ChebOut c{b, idiag, cheb, r, x};
+  ChebOut c{b, idiag, cheb, r, x, nullptr};
   k_node_gather<double, double, 1><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
@@ -613,10 +619,45 @@ int hm_launch_cheb1_from_x(const Lattice& L, void* jac, const uint8_t* ess, cons
   double* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
   k_elem_apply<double, double, false><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
-  ChebOut c{b, idiag, cheb, nullptr, x};
+  ChebOut c{b, idiag, cheb, nullptr, x, nullptr};
   k_node_gather<double, double, 2><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+
+// the same two steps with the FP32 operator and FP32 level vectors (the multigrid cycle in
+// single precision): the first direction d = b idiag / theta is formed in FP64 from the
+// FP64 right-hand side and rounded to FP32 on the fly; the post-smoothing result goes to
+// the FP64 z
+int hm_launch_cheb1_from_zero32(const Lattice& L, void* jac32, const uint8_t* ess, const double* b,
+                                const double* idiag, const double* cheb, float* x, float* r,
+                                void* stream) {
+  float* Dq = static_cast<float*>(jac32);
+  float* Ye = Dq + L.ne * 27;
+  const int64_t warps = (L.ne + 9) / 10;
+  k_elem_apply<float, double, false, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(
+      L, Dq, ess, b, Ye, idiag, cheb);
+  ChebOutT<float> c{b, idiag, cheb, r, x, nullptr};
+  k_node_gather<float, float, 1><<<gather_blocks(L), 256, 0, S_(stream)>>>(
+      L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+int hm_launch_cheb1_from_x32(const Lattice& L, void* jac32, const uint8_t* ess, const double* b,
+                             const double* idiag, const double* cheb, const float* x, double* z,
+                             void* stream) {
+  float* Dq = static_cast<float*>(jac32);
+  float* Ye = Dq + L.ne * 27;
+  const int64_t warps = (L.ne + 9) / 10;
+  k_elem_apply<float, float, false><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
+  ChebOutT<float> c{b, idiag, cheb, nullptr, const_cast<float*>(x), z};
+  k_node_gather<float, float, 2><<<gather_blocks(L), 256, 0, S_(stream)>>>(
+      L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
+  return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
+}
+int hm_launch_apply_A32(const Lattice& L, void* jac32, const uint8_t* ess, const float* x,
+                        float* y, bool clean, void* stream) {
+  return launch_apply_t<float, float>(L, jac32, ess, x, y, nullptr, nullptr, stream, nullptr,
+                                      nullptr, clean);
 }
 
 // number of partial sums k_node_gather writes when asked for the fused dot product

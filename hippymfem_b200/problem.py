@@ -70,10 +70,12 @@ class PDEVariationalProblem:
     preconditioner : ``"jacobi"`` or ``"mg"`` (the lattice's geometric multigrid V-cycle,
         in place of the reference's BoomerAMG; FP64 matrix-free solves, Dirichlet nodes
         on the whole boundary).
-    solver_precision : ``"fp64"``, or ``"mixed"``: Jacobi-PCG whose recurrence runs in
-        FP32 with the FP32 matrix-free operator, re-anchored to the FP64 true residual
-        each time it falls by ``reliable_delta``, to the same tolerance (in place of the
-        reference's ``_refined_solve``, :1220-1329); implies ``matrix_free_solves``.
+    solver_precision : ``"fp64"``, or ``"mixed"``: with ``"jacobi"``, PCG whose
+        recurrence runs in FP32 with the FP32 matrix-free operator, re-anchored to the
+        FP64 true residual each time it falls by ``reliable_delta``, to the same
+        tolerance (in place of the reference's ``_refined_solve``, :1220-1329); with
+        ``"mg"``, the FP64 CG preconditioned by the V-cycle run in FP32.  Implies
+        ``matrix_free_solves``.
     """
 
     def __init__(self, Vh, f=1.0, bc=None, bc0=None, is_fwd_linear=True, solver_tolerance=1e-12,
@@ -98,8 +100,6 @@ class PDEVariationalProblem:
         self.reliable_delta = float(reliable_delta)
         if preconditioner not in ("jacobi", "mg"):
             raise ValueError("preconditioner must be 'jacobi' or 'mg'")
-        if preconditioner == "mg" and solver_precision != "fp64":
-            raise ValueError("the multigrid preconditioner is for FP64 solves")
         self.preconditioner = preconditioner
         self.matrix_free_solves = (bool(matrix_free_solves) or solver_precision == "mixed"
                                    or preconditioner == "mg")
@@ -305,7 +305,9 @@ class PDEVariationalProblem:
 
     def _get_solver(self, A):
         if self.preconditioner == "mg":
-            return MGPCGSolver(A, rel_tolerance=self.solver_tolerance, max_iter=self.max_iter)
+            mgp = "fp32" if self.solver_precision == "mixed" else "fp64"
+            return MGPCGSolver(A, rel_tolerance=self.solver_tolerance, max_iter=self.max_iter,
+                               mg_precision=mgp)
         if self.solver_precision == "mixed":
             return MixedPCGSolver(A, self._jac_cache[2], rel_tolerance=self.solver_tolerance,
                                   reliable_delta=self.reliable_delta, max_iter=self.max_iter)

@@ -356,21 +356,55 @@ def default_smoothing_degree(mesh):
     return 1 if mesh.ndof >= 1_000_000 else 2
 
 
+MG_PRECISIONS = ("fp64", "fp32")
+
+
 class Multigrid:
     """The lattice Jacobian's geometric multigrid V-cycle (``hm_mg_*``): hierarchy and
     level storage on one workspace; ``setup`` loads a point's FP64 operator data (again
-    whenever the point changes); ``apply(r, z)`` is ``z = V(r)``."""
+    whenever the point changes); ``apply(r, z)`` is ``z = V(r)``.  ``precision="fp32"``
+    runs the cycle on single-precision copies of the level data (formed at every set-up;
+    ``r`` and ``z`` stay FP64): a preconditioner of the FP64 CG, which keeps the solve's
+    accuracy."""
 
-    def __init__(self, mesh, degree=None, coarse_degree=24):
+    def __init__(self, mesh, degree=None, coarse_degree=24, precision="fp64"):
         if degree is None:
             degree = default_smoothing_degree(mesh)
         self.mesh = mesh
         nbytes = lib.hm_mg_workspace_bytes(mesh.handle)
         self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=mesh.device)
+        self.work32 = None
+        self.precision = "fp64"
         self._mg = ctypes.c_void_p()
         check(lib.hm_mg_create(mesh.handle, ptr(self.work), int(degree), int(coarse_degree),
                                ctypes.byref(self._mg)), "hm_mg_create")
         self.levels = lib.hm_mg_levels(self._mg)
+        self.set_precision(precision)
+
+    @staticmethod
+    def workspace_bytes(mesh, precision="fp64"):
+        """Device bytes of a V-cycle's storage in ``precision``."""
+        nbytes = lib.hm_mg_workspace_bytes(mesh.handle)
+        if precision == "fp32":
+            nbytes += lib.hm_mg_single_workspace_bytes(mesh.handle)
+        return nbytes
+
+    def set_precision(self, precision, stream=None):
+        """The cycle in ``"fp64"`` or ``"fp32"``; after a set-up the FP32 copies are
+        formed at once (on ``stream``)."""
+        if precision not in MG_PRECISIONS:
+            raise ValueError("the multigrid precision must be one of %s" % (MG_PRECISIONS,))
+        if precision == "fp32":
+            if self.work32 is None:
+                nbytes = lib.hm_mg_single_workspace_bytes(self.mesh.handle)
+                self.work32 = torch.empty((nbytes + 3) // 4, dtype=torch.float32,
+                                          device=self.mesh.device)
+            check(lib.hm_mg_set_single(self._mg, ptr(self.work32), stream_ptr(stream)),
+                  "hm_mg_set_single")
+        else:
+            check(lib.hm_mg_set_single(self._mg, None, stream_ptr(stream)), "hm_mg_set_single")
+        self.precision = precision
+        return self
 
     def setup(self, jac64, ess, diag, stream=None):
         check(lib.hm_mg_setup(self._mg, ptr(jac64), ptr(ess), ptr(diag), stream_ptr(stream)),
@@ -410,10 +444,12 @@ class MGPCGSolver:
     hypre PCG (algorithms/linSolvers.py:243-828, 709).  It runs as a solve plan on the
     operator's own storage (``hm_pcg_plan_*`` with ``hm_pcg_plan_set_mg``): in a stream
     other than the legacy default stream every batch of iterations, V-cycles included,
-    replays a captured CUDA graph.  ``x`` is overwritten (the solve starts from zero)."""
+    replays a captured CUDA graph.  ``x`` is overwritten (the solve starts from zero).
+    ``mg_precision="fp32"`` runs the V-cycle in single precision; the CG recurrence, its
+    inner products and the stopping test stay FP64, so the tolerance means the same."""
 
     def __init__(self, operator, rel_tolerance=1e-12, max_iter=2000, check_every=4,
-                 degree=None, coarse_degree=24, raise_on_fail=True):
+                 degree=None, coarse_degree=24, raise_on_fail=True, mg_precision="fp64"):
         if not isinstance(operator, MatrixFreeJacobian) or operator.precision != _lib.HM_FP64:
             raise TypeError("the multigrid solve needs the FP64 matrix-free Jacobian")
         self.op = operator
@@ -421,7 +457,7 @@ class MGPCGSolver:
                            "check_every": int(check_every)}
         self.raise_on_fail = raise_on_fail
         mesh = operator.mesh
-        self.mg = Multigrid(mesh, degree, coarse_degree)
+        self.mg = Multigrid(mesh, degree, coarse_degree, precision=mg_precision)
         self.mg.setup(operator.jac, operator.ess, operator._diag)
         n = operator.nrow
         self.b = torch.zeros(n, dtype=torch.float64, device=mesh.device)

@@ -402,6 +402,17 @@ int hm_mg_set_tail_nodes(hm_mg* mg, int64_t max_nodes);
  * bit (fused = 1, the default).  fused = 0 launches the steps one by one.  Set it before
  * a plan's first solve, as the tail. */
 int hm_mg_set_fused(hm_mg* mg, int fused);
+/* The cycle in FP32 (d_work32 of hm_mg_single_workspace_bytes), or in FP64 again
+ * (d_work32 = NULL, the default).  The set-up stays FP64; each set-up (and this call,
+ * after one, on `stream`) rounds the point's D, the coarse coefficients, the reciprocal
+ * diagonals and the coarse inverse to FP32 copies.  r and z of hm_mg_apply stay FP64;
+ * with fused degree-1 smoothing inside the solves the level-0 passes read the FP64
+ * residual and write the FP64 result themselves.  A preconditioner of the FP64 CG
+ * (hm_pcg_mg, plans): the recurrence, its inner products and the stopping test are
+ * unchanged, so a solve meets the same tolerance.  Set it before a plan's first solve,
+ * as the tail. */
+int64_t hm_mg_single_workspace_bytes(const hm_lattice* lattice);
+int hm_mg_set_single(hm_mg* mg, void* d_work32, void* stream);
 int hm_mg_destroy(hm_mg* mg);
 int hm_pcg_mg(hm_mg* mg, const double* d_b, double* d_x, double rtol, int maxiter,
               int check_every, void* d_work, int* iterations, double* relres, void* stream);
