@@ -791,6 +791,7 @@ int hm_mg_vcycle(hm_mg* mg, const double* r, double* z, void* stream) {
   double* out = nullptr;
   return vcycle<double>(mg, 0, r, z, true, S_(stream), &out);
 }
+bool hm_mg_flexible(const hm_mg* mg) { return mg->single != 0; }
 const double* hm_mg_level0_diag(const hm_mg* mg) { return mg->lv[0].diag; }
 void* hm_mg_jac(const hm_mg* mg) { return mg->jac; }
 const uint8_t* hm_mg_ess(const hm_mg* mg) { return mg->ess; }

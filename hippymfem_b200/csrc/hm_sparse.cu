@@ -133,15 +133,17 @@ __global__ void k_pcg_alpha(const double* __restrict__ part, int64_t nparts, dou
   }
 }
 
-// beta = (r.z)_new / (r.z)_old, the convergence test and the iteration count (thread 0)
-__device__ __forceinline__ void beta_step(double rz, double rr, double* sc) {
+// beta = ((r.z)_new - rzc) / (r.z)_old, the convergence test and the iteration count
+// (thread 0).  rzc = 0: Fletcher-Reeves; rzc = r_new . z_old: Polak-Ribiere, the flexible
+// CG step (Notay 2000) for a preconditioner that is symmetric only to rounding.
+__device__ __forceinline__ void beta_step(double rz, double rr, double* sc, double rzc = 0.0) {
   const bool was = sc[SC_CONV] >= 0.0;
   if (!was) {
     const double it = sc[SC_IT] + 1.0;
     sc[SC_IT] = it;
     sc[SC_RR] = rr;
     if (rr <= sc[SC_TOL2] * sc[SC_BB]) sc[SC_CONV] = it;
-    const double beta = sc[SC_RZ] == 0.0 ? 0.0 : rz / sc[SC_RZ];
+    const double beta = sc[SC_RZ] == 0.0 ? 0.0 : (rz - rzc) / sc[SC_RZ];
     sc[SC_BETA] = isfinite(beta) ? beta : 0.0;
     sc[SC_RZ] = rz;
   }
@@ -210,28 +212,36 @@ __global__ void k_pcg_pupdate(int64_t n, const double* __restrict__ sc, const T*
 }
 
 // x += alpha p, r -= alpha q; partials of r.r (for a preconditioner applied after it)
+// and, given the last preconditioned residual zold, of r.zold (slot 2: the flexible step)
 __global__ void __launch_bounds__(kReduceThreads)
     k_pcg_update_rr(int64_t n, const double* __restrict__ sc, double* __restrict__ x,
                     double* __restrict__ r, const double* __restrict__ p,
-                    const double* __restrict__ q, double* __restrict__ part) {
+                    const double* __restrict__ q, double* __restrict__ part,
+                    const double* __restrict__ zold = nullptr) {
   __shared__ double sh[32];
   const double alpha = sc[SC_ALPHA];
-  double rr = 0.0;
+  double rr = 0.0, rzc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] = fma(alpha, p[i], x[i]);
     const double ri = fma(-alpha, q[i], r[i]);
     r[i] = ri;
     rr = fma(ri, ri, rr);
+    if (zold != nullptr) rzc = fma(ri, zold[i], rzc);
   }
   rr = block_sum(rr, sh);
   if (threadIdx.x == 0) part[kReduceBlocks + blockIdx.x] = rr;
+  if (zold != nullptr) {
+    rzc = block_sum(rzc, sh);
+    if (threadIdx.x == 0) part[2 * kReduceBlocks + blockIdx.x] = rzc;
+  }
 }
 
-// partials of r.z; the last block takes beta from them and the r.r partials
+// partials of r.z; the last block takes beta from them and the r.r partials (flex: and
+// the r.zold partials of k_pcg_update_rr, the flexible step)
 __global__ void __launch_bounds__(kReduceThreads)
     k_pcg_rz_beta(int64_t n, const double* __restrict__ r, const double* __restrict__ z,
                   double* __restrict__ part, unsigned* __restrict__ counter,
-                  double* __restrict__ sc) {
+                  double* __restrict__ sc, int flex = 0) {
   __shared__ double sh[32];
   double rz = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -239,15 +249,17 @@ __global__ void __launch_bounds__(kReduceThreads)
   rz = block_sum(rz, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = rz;
   if (last_block(counter)) {
-    double v0 = 0.0, v1 = 0.0;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
     for (int b = threadIdx.x; b < kReduceBlocks; b += blockDim.x) {
       v0 += __ldcg(part + b);
       v1 += __ldcg(part + kReduceBlocks + b);
+      if (flex) v2 += __ldcg(part + 2 * kReduceBlocks + b);
     }
     v0 = block_sum(v0, sh);
     v1 = block_sum(v1, sh);
+    if (flex) v2 = block_sum(v2, sh);
     if (threadIdx.x == 0) {
-      beta_step(v0, v1, sc);
+      beta_step(v0, v1, sc, v2);
       *counter = 0u;
     }
   }
@@ -595,6 +607,8 @@ extern "C" int hm_pcg_impl(int64_t n, const int32_t* indptr, const int32_t* indi
 }
 
 int hm_mg_vcycle(hm_mg* mg, const double* r, double* z, void* stream);
+// the V-cycle is symmetric only to rounding (FP32): its CG takes the flexible step
+bool hm_mg_flexible(const hm_mg* mg);
 const double* hm_mg_level0_diag(const hm_mg* mg);
 void* hm_mg_jac(const hm_mg* mg);
 const uint8_t* hm_mg_ess(const hm_mg* mg);
@@ -634,10 +648,25 @@ int pcg_mg_run(hm_mg* mg, const double* b, double* x, double rtol, int maxiter, 
     return HM_ERR_CUDA;
   double host[SC_N];
   int it = 0;
+  const int flex = hm_mg_flexible(mg) ? 1 : 0;
+  // with the FP32 cycle: r.r at each check; the solve stops (HM_ERR_NOCONV) once, past
+  // iteration 24, twelve iterations no longer halve the residual -- the cycle's rounding,
+  // relative to the smooth part of its correction, then swamps the rest (high contrast)
+  std::vector<double> hist;
+  const int back = (12 + check_every - 1) / check_every;
+  bool stalled = false;
   for (;;) {
     if (cudaMemcpyAsync(host, sc, sizeof(host), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HM_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return HM_ERR_CUDA;
     if (host[SC_CONV] >= 0.0 || it >= maxiter) break;
+    if (flex) {
+      hist.push_back(host[SC_RR]);
+      if (it >= 24 && (int)hist.size() > back &&
+          host[SC_RR] > 0.25 * hist[hist.size() - 1 - back]) {
+        stalled = true;
+        break;
+      }
+    }
     const int count = it + check_every < maxiter ? check_every : maxiter - it;
     rc = run_batch(graph, count == check_every, s, [&]() -> int {
       for (int j = 0; j < count; ++j) {
@@ -645,9 +674,10 @@ int pcg_mg_run(hm_mg* mg, const double* b, double* x, double rtol, int maxiter, 
         int e = op_apply(o, p, q, pq_part, &np, (void*)s, sc, cnt, &fused);
         if (e) return e;
         if (!fused) k_pcg_alpha<<<1, 1024, 0, s>>>(pq_part, np, sc);
-        k_pcg_update_rr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, p, q, part);
+        k_pcg_update_rr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, x, r, p, q, part,
+                                                                 flex ? z : nullptr);
         if ((e = hm_mg_vcycle(mg, r, z, (void*)s))) return e;
-        k_pcg_rz_beta<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, part, cnt + 1, sc);
+        k_pcg_rz_beta<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, r, z, part, cnt + 1, sc, flex);
         k_pcg_pupdate<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, sc, z, p);
       }
       return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
@@ -655,7 +685,7 @@ int pcg_mg_run(hm_mg* mg, const double* b, double* x, double rtol, int maxiter, 
     if (rc) return rc;
     it += count;
   }
-  const bool conv = host[SC_CONV] >= 0.0;
+  const bool conv = !stalled && host[SC_CONV] >= 0.0;
   if (iterations) *iterations = conv ? (int)host[SC_CONV] : it;
   if (relres) *relres = host[SC_BB] > 0.0 ? std::sqrt(host[SC_RR] / host[SC_BB]) : 0.0;
   return conv ? HM_OK : HM_ERR_NOCONV;
@@ -972,9 +1002,11 @@ int group_batch(hm_pcg_plan* pl, int count, cudaStream_t s) {
     int e = op_apply(o, B.p, B.q, B.pq_part, &np, (void*)s, B.sc, B.cnt, &fused);
     if (e) return e;
     if (!fused) k_pcg_alpha<<<1, 1024, 0, s>>>(B.pq_part, np, B.sc);
-    k_pcg_update_rr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.sc, pl->x, B.r, B.p, B.q, B.part);
+    const int flex = hm_mg_flexible(pl->mg) ? 1 : 0;
+    k_pcg_update_rr<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.sc, pl->x, B.r, B.p, B.q, B.part,
+                                                             flex ? B.z : nullptr);
     if ((e = hm_mg_vcycle(pl->mg, B.r, B.z, (void*)s))) return e;
-    k_pcg_rz_beta<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.r, B.z, B.part, B.cnt + 1, B.sc);
+    k_pcg_rz_beta<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.r, B.z, B.part, B.cnt + 1, B.sc, flex);
     k_pcg_pupdate<double><<<kReduceBlocks, kReduceThreads, 0, s>>>(n, B.sc, B.z, B.p);
   }
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;

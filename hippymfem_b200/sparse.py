@@ -446,7 +446,12 @@ class MGPCGSolver:
     other than the legacy default stream every batch of iterations, V-cycles included,
     replays a captured CUDA graph.  ``x`` is overwritten (the solve starts from zero).
     ``mg_precision="fp32"`` runs the V-cycle in single precision; the CG recurrence, its
-    inner products and the stopping test stay FP64, so the tolerance means the same."""
+    inner products and the stopping test stay FP64, so the tolerance means the same.  The
+    FP32 cycle's rounding is relative to the smooth part of its correction, so at high
+    contrast (condition numbers near 1e7) it can stop carrying the solve: a solve with it
+    that stalls, or whose FP64 true residual ends above ten times the tolerance, is solved
+    again with the FP64 cycle, which the solver keeps from then on (``fallbacks`` counts
+    them), as the reference finishes a refined solve in double (``_solve_in_double``)."""
 
     def __init__(self, operator, rel_tolerance=1e-12, max_iter=2000, check_every=4,
                  degree=None, coarse_degree=24, raise_on_fail=True, mg_precision="fp64"):
@@ -465,20 +470,53 @@ class MGPCGSolver:
         nbytes = lib.hm_pcg_workspace_bytes(n)
         self.work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device=mesh.device)
         self._plan = ctypes.c_void_p()
-        check(lib.hm_pcg_plan_create(mesh.handle, ptr(operator.jac), None, ptr(operator.ess),
-                                     ptr(operator._diag), ptr(self.b), ptr(self.x), ptr(self.work),
-                                     int(check_every), ctypes.byref(self._plan)), "hm_pcg_plan_create")
-        check(lib.hm_pcg_plan_set_mg(self._plan, self.mg._mg), "hm_pcg_plan_set_mg")
+        self._make_plan()
+        self._y = None
+        self.fallbacks = 0
         self.last = None
 
-    def solve(self, x, b, stream=None):
+    def _make_plan(self):
+        """A solve plan on the operator's storage with this solver's V-cycle (again after
+        the cycle's precision changes: a plan keeps the launches it captured)."""
+        if self._plan:
+            lib.hm_pcg_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+        op = self.op
+        check(lib.hm_pcg_plan_create(op.mesh.handle, ptr(op.jac), None, ptr(op.ess), ptr(op._diag),
+                                     ptr(self.b), ptr(self.x), ptr(self.work),
+                                     self.parameters["check_every"], ctypes.byref(self._plan)),
+              "hm_pcg_plan_create")
+        check(lib.hm_pcg_plan_set_mg(self._plan, self.mg._mg), "hm_pcg_plan_set_mg")
+
+    def _run(self, stream):
         prm = self.parameters
-        self.b.copy_(b)
         it, nup, rr = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         rc = lib.hm_pcg_plan_solve(self._plan, prm["rel_tolerance"], 0.1, 1, prm["max_iter"],
                                    ctypes.byref(it), ctypes.byref(nup), ctypes.byref(rr),
                                    stream_ptr(stream))
         self.last = PCGResult(it.value, rr.value, rc == _lib.HM_OK)
+        return rc
+
+    def _carried(self, stream):
+        """The FP64 true residual of the FP32-cycle solve within ten times the tolerance."""
+        if self._y is None:
+            self._y = torch.empty_like(self.x)
+        with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+            self.op.mult(self.x, self._y)
+            self._y.sub_(self.b)
+            tol = 10.0 * self.parameters["rel_tolerance"] * float(self.b.norm())
+            return float(self._y.norm()) <= tol
+
+    def solve(self, x, b, stream=None):
+        self.b.copy_(b)
+        rc = self._run(stream)
+        if self.mg.precision == "fp32" and rc in (_lib.HM_OK, _lib.HM_ERR_NOCONV) and (
+                rc != _lib.HM_OK or not self._carried(stream)):
+            self.mg.set_precision("fp64", stream)
+            self.mg.work32 = None
+            self._make_plan()
+            self.fallbacks += 1
+            rc = self._run(stream)
         if rc == _lib.HM_ERR_NOCONV and not self.raise_on_fail:
             x.copy_(self.x)
             return x
