@@ -359,6 +359,7 @@ __device__ __forceinline__ void axis_elems(int i, int nel, int& e0, int& a0, int
 //      c.r = b - y, c.x = d
 //   2  one smoothing step from c.x (the input): c.x += (b - y) c.diag / theta, in place,
 //      or into c.z (FP64) when given (this pass reads no x but the Dirichlet nodes' own)
+//   3  as 1 with d already in c.x (the input): c.r = b - y
 // c.r and c.x are in the vector type V (the updates are formed in FP64 and rounded once)
 template <typename V>
 struct ChebOutT {
@@ -448,6 +449,9 @@ __global__ void __launch_bounds__(256)
           const double y = fx ? (double)(vec)d : acc;
           c.r[nn] = (vec)(bn - y);
           c.x[nn] = (vec)d;
+        } else if constexpr (OUT == 3) {
+          const double y = fx ? (double)c.x[nn] : acc;
+          c.r[nn] = (vec)(bn - y);
         } else {
           const double xn = (double)c.x[nn];
           const double y = fx ? xn : acc;
@@ -629,16 +633,24 @@ int hm_launch_cheb1_from_x(const Lattice& L, void* jac, const uint8_t* ess, cons
 // single precision): the first direction d = b idiag / theta is formed in FP64 from the
 // FP64 right-hand side and rounded to FP32 on the fly; the post-smoothing result goes to
 // the FP64 z
+// d = b idiag / theta rounded to FP32, one thread per node (the FP64 product the FP64
+// element pass forms on the fly)
+__global__ void k_cheb_first32(int64_t n, const double* __restrict__ b, const double* __restrict__ idiag,
+                               const double* __restrict__ cheb, float* __restrict__ d) {
+  const double inv_theta = 1.0 / cheb[0];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = (float)__dmul_rn(inv_theta * b[i], idiag[i]);
+}
 int hm_launch_cheb1_from_zero32(const Lattice& L, void* jac32, const uint8_t* ess, const double* b,
                                 const double* idiag, const double* cheb, float* x, float* r,
                                 void* stream) {
   float* Dq = static_cast<float*>(jac32);
   float* Ye = Dq + L.ne * 27;
   const int64_t warps = (L.ne + 9) / 10;
-  k_elem_apply<float, double, false, true><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(
-      L, Dq, ess, b, Ye, idiag, cheb);
+  k_cheb_first32<<<grid1(L.ndof, 256), 256, 0, S_(stream)>>>(L.ndof, b, idiag, cheb, x);
+  k_elem_apply<float, float, false><<<grid1(warps * 32, 256), 256, 0, S_(stream)>>>(L, Dq, ess, x, Ye);
   ChebOutT<float> c{b, idiag, cheb, r, x, nullptr};
-  k_node_gather<float, float, 1><<<gather_blocks(L), 256, 0, S_(stream)>>>(
+  k_node_gather<float, float, 3><<<gather_blocks(L), 256, 0, S_(stream)>>>(
       L, Ye, ess, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c);
   return cudaGetLastError() == cudaSuccess ? HM_OK : HM_ERR_CUDA;
 }
