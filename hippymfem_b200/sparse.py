@@ -451,7 +451,8 @@ class MGPCGSolver:
     contrast (condition numbers near 1e7) it can stop carrying the solve: a solve with it
     that stalls, or whose FP64 true residual ends above ten times the tolerance, is solved
     again with the FP64 cycle, which the solver keeps from then on (``fallbacks`` counts
-    them), as the reference finishes a refined solve in double (``_solve_in_double``)."""
+    them), as the reference finishes a refined solve in double (``_solve_in_double``,
+    modeling/PDEVariationalProblem.py:1331)."""
 
     def __init__(self, operator, rel_tolerance=1e-12, max_iter=2000, check_every=4,
                  degree=None, coarse_degree=24, raise_on_fail=True, mg_precision="fp64"):
