@@ -723,6 +723,14 @@ int plan_levels(const Lattice& L, MGLevel* lv, int max_levels) {
   return nl;
 }
 
+// the coarsest level is solved exactly (through its inverse) when it is a Q1 level with
+// few interior nodes
+bool exact_coarsest(const hm_mg* mg, int l) {
+  if (mg->nlev < 2 || l != mg->nlev - 1) return false;
+  const int ni = interior_count(mg->lv[l]);
+  return ni >= 1 && ni <= kCoarseDirectMax;
+}
+
 // the FP32 copies of the level data on work32 (in floats; each piece starts on 128 bytes)
 int64_t layout_single(hm_mg* mg, float* work32) {
   float* w = work32;
@@ -748,7 +756,7 @@ int64_t layout_single(hm_mg* mg, float* work32) {
     f.idiag = take(d.nodes);
     f.x = take(d.nodes); f.b = take(d.nodes); f.r = take(d.nodes);
     f.d = take(d.nodes); f.t = take(d.nodes);
-    f.cinv = d.cinv ? take(kCoarseDirectMax * kCoarseDirectMax) : nullptr;
+    f.cinv = exact_coarsest(mg, l) ? take(kCoarseDirectMax * kCoarseDirectMax) : nullptr;
     f.cheb = d.cheb;
     f.degree = d.degree;
     if (work32) mg->lv32[l] = f;
@@ -844,11 +852,8 @@ extern "C" int hm_mg_create(const hm_lattice* h, void* work, int degree, int coa
   }
   z.cinv = nullptr;
   // an exact coarse solve when the coarsest Q1 level has few interior nodes
-  if (mg->nlev > 1) {
-    MGLevel& c = mg->lv[mg->nlev - 1];
-    const int ni = interior_count(c);
-    if (ni >= 1 && ni <= kCoarseDirectMax) c.cinv = take(kCoarseDirectMax * kCoarseDirectMax);
-  }
+  if (exact_coarsest(mg, mg->nlev - 1))
+    mg->lv[mg->nlev - 1].cinv = take(kCoarseDirectMax * kCoarseDirectMax);
   *out = mg;
   return HM_OK;
 }
@@ -928,12 +933,6 @@ extern "C" int64_t hm_mg_single_workspace_bytes(const hm_lattice* h) {
   hm_mg probe{};
   probe.L = *L;
   probe.nlev = plan_levels(*L, probe.lv, 16);
-  if (probe.nlev > 1) {
-    MGLevel& c = probe.lv[probe.nlev - 1];
-    const int ni = interior_count(c);
-    // a non-null marker: layout_single only asks whether the coarse inverse exists
-    if (ni >= 1 && ni <= kCoarseDirectMax) c.cinv = reinterpret_cast<double*>(&probe);
-  }
   return layout_single(&probe, nullptr) * (int64_t)sizeof(float);
 }
 
