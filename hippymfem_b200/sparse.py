@@ -505,8 +505,8 @@ class MGPCGSolver:
         with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
             self.op.mult(self.x, self._y)
             self._y.sub_(self.b)
-            tol = 10.0 * self.parameters["rel_tolerance"] * float(self.b.norm())
-            return float(self._y.norm()) <= tol
+            res, bnorm = torch.stack((self._y.norm(), self.b.norm())).tolist()   # one read
+        return res <= 10.0 * self.parameters["rel_tolerance"] * bnorm
 
     def solve(self, x, b, stream=None):
         self.b.copy_(b)
