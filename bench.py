@@ -59,6 +59,8 @@ def parse():
                     help="the Hessian action sharded over z-slabs of the 64^3 lattice across "
                          "the ranks (one per GPU; halo exchange by point-to-point messages, "
                          "plane-ordered dot products; Jacobi-PCG), H-applies/s, strong scaling")
+    ap.add_argument("--mg-precision", choices=("fp64", "fp32"), default="fp64",
+                    help="the V-cycle's precision in --config solve (the CG stays FP64)")
     ap.add_argument("--config", choices=("main", "precision", "differentiation", "solve"),
                     default="main",
                     help="precision: 128^3, FP32 contractions and mixed-precision Hessian "
@@ -879,8 +881,8 @@ def run_differentiation(a, n=32, ndir=16, h=1e-6):
 
 def run_solve(a):
     """One incremental solve A x = b at n^3 (the matrix-free FP64 Jacobian at the
-    benchmark field, multigrid-PCG to rtol 1e-12, graph-replayed in a side stream),
-    warm-up then --steps timed solves with CUDA events."""
+    benchmark field, multigrid-PCG to rtol 1e-12, graph-replayed in a side stream, the
+    V-cycle in --mg-precision), warm-up then --steps timed solves with CUDA events."""
     import torch
 
     from hippymfem_b200 import BoxMesh, DirichletBC, PDEVariationalProblem, Q2Space
@@ -897,7 +899,7 @@ def run_solve(a):
                         device=mesh.device).masked_fill_(prob.bc0.mask, 0.0)
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
-        solver = MGPCGSolver(A, rel_tolerance=1e-12)
+        solver = MGPCGSolver(A, rel_tolerance=1e-12, mg_precision=a.mg_precision)
         x = V.vector()
         for _ in range(max(a.warmup, 1)):
             solver.solve(x, b)
@@ -912,6 +914,7 @@ def run_solve(a):
     line = {"metric": "incremental solves/s (FP64 multigrid-PCG, rtol 1e-12)",
             "value": 1e3 / ms, "unit": "solves/s", "ms_per_solve": ms,
             "iterations": solver.last.iterations, "relres": solver.last.relres,
+            "mg_precision": solver.mg.precision, "fallbacks": solver.fallbacks,
             "steps": a.steps, "warmup": a.warmup,
             "config": {"workload": "Q2 hex %d^3 Jacobian solve at the benchmark field" % a.n,
                        "dofs": mesh.ndof},
