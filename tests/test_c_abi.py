@@ -146,3 +146,38 @@ def test_dof_permutation_from_a_caller_table():
             _lib.check(_lib.lib.hm_lattice_dof_permutation(h, hptr(big), hptr(local), hptr(out)))
     finally:
         _lib.lib.hm_lattice_destroy(h)
+
+
+def _mg_levels(n):
+    """The multigrid hierarchy's (elements, nodes) per level, restated: the Q2 lattice, Q1
+    on the same elements, then Q1 coarsened 2:1 while every axis stays even and >= 4."""
+    nx, ny, nz = n
+    lv = [(nx * ny * nz, (2 * nx + 1) * (2 * ny + 1) * (2 * nz + 1))]
+    if min(n) < 2:
+        return lv, 0
+    lv.append((nx * ny * nz, (nx + 1) * (ny + 1) * (nz + 1)))
+    while len(lv) < 16 and all(a % 2 == 0 and a >= 4 for a in (nx, ny, nz)):
+        nx, ny, nz = nx // 2, ny // 2, nz // 2
+        lv.append((nx * ny * nz, (nx + 1) * (ny + 1) * (nz + 1)))
+    return lv, (nx - 1) * (ny - 1) * (nz - 1)
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (16, 8, 12), (8, 8, 8), (24, 24, 24)])
+def test_single_cycle_workspace_matches_the_level_plan(n):
+    """hm_mg_single_workspace_bytes: the point's D and the element results (54 floats per
+    element), per level the coefficients (Q1 levels), reciprocal diagonal and five vectors,
+    the coarse inverse when the coarsest level has at most 64 interior nodes; every piece
+    rounded up to 32 floats."""
+    from hippymfem_b200 import _lib
+
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib.hm_lattice_create(*n, 1.0, 1.0, 1.0, ctypes.byref(h)))
+    levels, interior = _mg_levels(n)
+    up = lambda k: (k + 31) // 32 * 32                       # noqa: E731
+    floats = up(54 * levels[0][0])
+    for l, (ne, nodes) in enumerate(levels):
+        floats += (up(ne) if l >= 1 else 0) + 6 * up(nodes)
+    if len(levels) > 1 and 1 <= interior <= 64:
+        floats += up(64 * 64)
+    assert _lib.lib.hm_mg_single_workspace_bytes(h) == 4 * floats
+    _lib.lib.hm_lattice_destroy(h)
