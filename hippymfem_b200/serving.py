@@ -45,7 +45,7 @@ from ._lib import check, lib, ptr, stream_ptr
 from .mesh import BoxMesh, DirichletBC, Q2Space
 from .modeling import DiscreteStateObservation, PointwiseStateObservation
 from .problem import STATE
-from .sparse import SolveGroup, SolvePlan
+from .sparse import Multigrid, SolveGroup, SolvePlan
 from .synthetic import field_params, interior_points
 
 
@@ -98,7 +98,7 @@ class _MeshState:
     def footprint(self, precision, multigrid=False):
         """Bytes of one slot's workspace for this size."""
         nd, q = self.mesh.ndof, self.mesh.quad_bytes(_lib.HM_FP64)
-        mg = lib.hm_mg_workspace_bytes(self.mesh.handle) if multigrid else 0
+        mg = Multigrid.workspace_bytes(self.mesh) if multigrid else 0
         jac = lib.hm_lattice_jacobian_bytes(self.mesh.handle, _lib.HM_FP64)
         if precision == "mixed":
             jac += lib.hm_lattice_jacobian_bytes(self.mesh.handle, _lib.HM_FP32)
