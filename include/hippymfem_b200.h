@@ -409,8 +409,12 @@ int hm_mg_set_fused(hm_mg* mg, int fused);
  * with fused degree-1 smoothing inside the solves the level-0 passes read the FP64
  * residual and write the FP64 result themselves.  A preconditioner of the FP64 CG
  * (hm_pcg_mg, plans): the recurrence, its inner products and the stopping test are
- * unchanged, so a solve meets the same tolerance.  Set it before a plan's first solve,
- * as the tail. */
+ * unchanged, so a solve meets the same tolerance.  With it the CG takes the flexible
+ * (Polak-Ribiere) step, the cycle being symmetric only to FP32 rounding, and a solve
+ * returns HM_ERR_NOCONV as soon as, past iteration 24, twelve iterations no longer halve
+ * the residual: at high contrast (condition numbers near 1e7) FP32 rounding, relative to
+ * the smooth part of the cycle's correction, swamps the rest; the caller then solves with
+ * the FP64 cycle.  Set it before a plan's first solve, as the tail. */
 int64_t hm_mg_single_workspace_bytes(const hm_lattice* lattice);
 int hm_mg_set_single(hm_mg* mg, void* d_work32, void* stream);
 int hm_mg_destroy(hm_mg* mg);
