@@ -134,8 +134,10 @@ __global__ void k_pcg_alpha(const double* __restrict__ part, int64_t nparts, dou
 }
 
 // beta = ((r.z)_new - rzc) / (r.z)_old, the convergence test and the iteration count
-// (thread 0).  rzc = 0: Fletcher-Reeves; rzc = r_new . z_old: Polak-Ribiere, the flexible
-// CG step (Notay 2000) for a preconditioner that is symmetric only to rounding.
+// (thread 0).  rzc = 0: Fletcher-Reeves; rzc = r_new . z_old: a Polak-Ribiere-type step
+// for a preconditioner that is symmetric only to rounding.  The textbook flexible step
+// (Golub and Ye 1999) takes z_new . r_old instead; for a symmetric preconditioner the
+// two cross terms are equal, and both vanish in exact arithmetic.
 __device__ __forceinline__ void beta_step(double rz, double rr, double* sc, double rzc = 0.0) {
   const bool was = sc[SC_CONV] >= 0.0;
   if (!was) {

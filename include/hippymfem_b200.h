@@ -409,8 +409,9 @@ int hm_mg_set_fused(hm_mg* mg, int fused);
  * with fused degree-1 smoothing inside the solves the level-0 passes read the FP64
  * residual and write the FP64 result themselves.  A preconditioner of the FP64 CG
  * (hm_pcg_mg, plans): the recurrence, its inner products and the stopping test are
- * unchanged, so a solve meets the same tolerance.  With it the CG takes the flexible
- * (Polak-Ribiere) step, the cycle being symmetric only to FP32 rounding, and a solve
+ * unchanged, so a solve meets the same tolerance.  With it the CG takes a
+ * Polak-Ribiere-type step (beta = r+.(z+ - z) / r.z), the cycle being symmetric only to
+ * FP32 rounding, and a solve
  * returns HM_ERR_NOCONV as soon as, past iteration 24, twelve iterations no longer halve
  * the residual: at high contrast (condition numbers near 1e7) FP32 rounding, relative to
  * the smooth part of the cycle's correction, swamps the rest; the caller then solves with

@@ -116,7 +116,7 @@ def test_single_copies_follow_each_setup(cuda):
                                      ((48, 24, 32), 0.5), ((32, 32, 32), 1.0),
                                      ((48, 48, 48), 1.0)])
 def test_mg_pcg_with_the_single_cycle_meets_the_fp64_tolerance(cuda, n, sigma):
-    """The FP64 CG with the FP32 cycle (the flexible, Polak-Ribiere step) meets the FP64
+    """The FP64 CG with the FP32 cycle (a Polak-Ribiere-type step) meets the FP64
     tolerance: with the same iterations where the cycle is strong; where the contrast
     (sigma = 1: e^m over about e^-3..e^3) makes the FP32 cycle's rounding swamp its
     correction, the solve stalls or drifts, and the solver solves again with the FP64
