@@ -631,8 +631,9 @@ int hm_launch_cheb1_from_x(const Lattice& L, void* jac, const uint8_t* ess, cons
 
 // the same two steps with the FP32 operator and FP32 level vectors (the multigrid cycle in
 // single precision): the first direction d = b idiag / theta is formed in FP64 from the
-// FP64 right-hand side and rounded to FP32 on the fly; the post-smoothing result goes to
-// the FP64 z
+// FP64 right-hand side, once per node, and rounded to FP32 into x (k_cheb_first32); the
+// element pass and the gather then read it from there; the post-smoothing result goes
+// to the FP64 z
 // d = b idiag / theta rounded to FP32, one thread per node (the FP64 product the FP64
 // element pass forms on the fly)
 __global__ void k_cheb_first32(int64_t n, const double* __restrict__ b, const double* __restrict__ idiag,
