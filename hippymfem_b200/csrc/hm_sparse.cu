@@ -137,7 +137,8 @@ __global__ void k_pcg_alpha(const double* __restrict__ part, int64_t nparts, dou
 // (thread 0).  rzc = 0: Fletcher-Reeves; rzc = r_new . z_old: a Polak-Ribiere-type step
 // for a preconditioner that is symmetric only to rounding.  The textbook flexible step
 // (Golub and Ye 1999) takes z_new . r_old instead; for a symmetric preconditioner the
-// two cross terms are equal, and both vanish in exact arithmetic.
+// two cross terms are equal, and both vanish in exact arithmetic.  With the FP32 V-cycle
+// at high contrast the textbook step stalled on fields where this one converged.
 __device__ __forceinline__ void beta_step(double rz, double rr, double* sc, double rzc = 0.0) {
   const bool was = sc[SC_CONV] >= 0.0;
   if (!was) {
